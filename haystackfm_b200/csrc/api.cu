@@ -1,0 +1,651 @@
+// api.cu — the C ABI (include/hfm.h): device-resident index, query pipelines,
+// per-handle memory arenas and streams.
+//
+// A handle owns one CUDA stream and grow-only device buffers; calls on one handle are
+// serialised by its mutex, separate handles (e.g. one per GPU) run concurrently.  This
+// replaces the reference's process-wide wgpu context and its per-call index uploads
+// (src/gpu/context_cache.rs:11-19, src/gpu/locate.rs:69-111,
+// src/fm_index/bidir_index.rs:410-411).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dev_index.cuh"
+#include "hfm_internal.h"
+#include "resolve.cuh"
+#include "search.cuh"
+
+namespace hfm {
+
+static thread_local std::string g_err;
+
+int set_error(int status, const std::string& msg) {
+  g_err = msg;
+  return status;
+}
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t _e = (call);                                                                      \
+    if (_e != cudaSuccess)                                                                        \
+      return set_error(_e == cudaErrorMemoryAllocation ? HFM_E_OOM : HFM_E_CUDA,                  \
+                       std::string(#call) + ": " + cudaGetErrorString(_e));                       \
+  } while (0)
+
+#define RET(x) do { int _r = (x); if (_r != HFM_OK) return _r; } while (0)
+
+// compatible_symbols / ExactDna::compatible (src/alphabet.rs:174-193,286-294) as bit masks
+static void compat_masks(uint32_t tag, uint16_t out[16]) {
+  static const uint8_t iupac[16][15] = {
+      {0}, {1, 5, 6, 9, 11, 13, 14, 15}, {2, 5, 7, 8, 11, 12, 14, 15}, {3, 5, 6, 8, 10, 12, 13, 15},
+      {4, 5, 7, 9, 10, 12, 13, 14}, {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15},
+      {1, 3, 5, 6, 8, 9, 10, 11, 12, 13, 14, 15}, {2, 4, 5, 7, 8, 9, 10, 11, 12, 13, 14, 15},
+      {2, 3, 5, 6, 7, 8, 10, 11, 12, 13, 14, 15}, {1, 4, 5, 6, 7, 9, 10, 11, 12, 13, 14, 15},
+      {3, 4, 5, 6, 7, 8, 9, 10, 12, 13, 14, 15}, {1, 2, 5, 6, 7, 8, 9, 11, 12, 13, 14, 15},
+      {2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15}, {1, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15},
+      {1, 2, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15}, {1, 2, 3, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15}};
+  for (int c = 0; c < 16; c++) {
+    uint16_t m = 0;
+    if (tag == 1) { if (c >= 1 && c <= 4) m = (uint16_t)(1u << c); }
+    else for (int k = 0; k < 15; k++) if (iupac[c][k]) m |= (uint16_t)(1u << iupac[c][k]);
+    out[c] = m;
+  }
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  int ensure(size_t bytes) {
+    if (bytes <= cap) return HFM_OK;
+    if (p) cudaFree(p);
+    p = nullptr; cap = 0;
+    size_t want = std::max<size_t>(bytes + bytes / 4, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      e = cudaMalloc(&p, bytes);
+      if (e != cudaSuccess) { cudaGetLastError(); p = nullptr; return set_error(HFM_E_OOM, "cudaMalloc failed: " + std::to_string(bytes) + " bytes"); }
+      want = bytes;
+    }
+    cap = want;
+    return HFM_OK;
+  }
+  template <class T> T* as() const { return (T*)p; }
+  void release() { if (p) cudaFree(p); p = nullptr; cap = 0; }
+};
+
+struct Counters {                    // device-side counters, one block per handle
+  unsigned long long iv_used, hit_used, touches, steps;
+  uint32_t n_ovf, still_ovf, walk_err, _pad;
+};
+
+struct FmDev {
+  DevFm d{};
+  DevBuf occ, sbc, ssa, sa_vals, lut, bounds, compat;
+  uint32_t text_len = 0, num_seqs = 0, lookup_depth = 0, tag = 0, num_lanes = 0, encoding = 0, rate = 0;
+  std::vector<uint32_t> seq_boundaries;
+  size_t bytes() const { return occ.cap + sbc.cap + ssa.cap + sa_vals.cap + lut.cap + bounds.cap + compat.cap; }
+};
+
+}  // namespace hfm
+
+using namespace hfm;
+
+struct hfm_index {
+  int device = 0, kind = 0;
+  FmDev fwd, rev;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  bool count_work = false;
+  // per-call work buffers (grow-only)
+  DevBuf q, qoff, counts, nhits, niv, ivoff, status, ovf, ivpool, hitpool, seg_row, seg_off, pos_base, seg_base,
+      scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr;
+  uint64_t iv_cap = 0, hit_cap = 0;
+  Counters* h_ctr = nullptr;        // pinned
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  hfm_stats stats{};
+};
+
+namespace hfm {
+
+// ---------------------------------------------------------------------------
+// Device layout construction (host transform of the bincode records)
+// ---------------------------------------------------------------------------
+static int upload(DevBuf& b, const void* src, size_t bytes, cudaStream_t s) {
+  RET(b.ensure(std::max<size_t>(bytes, 16)));
+  if (bytes) CK(cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, s));
+  return HFM_OK;
+}
+
+static int build_device_fm(const HostFm& h, FmDev& f, cudaStream_t s) {
+  const uint32_t n = h.text_len, L = h.num_lanes;
+  const uint64_t nblk = ((uint64_t)n + 63) / 64, nsb = ((uint64_t)n + 4095) / 4096;
+  std::vector<uint32_t> occ(nblk * 16, 0), sbc(nsb * 16, 0);
+  std::vector<uint32_t> ssa(nblk * 4, 0);
+  uint32_t cur_sb[16] = {0};
+  const uint64_t width = h.encoding == 0 ? h.num_planes : L;
+  for (uint64_t b = 0; b < nblk; b++) {
+    const uint8_t* r = h.block_data + b * h.block_stride;
+    uint32_t cnt[16] = {0};
+    uint64_t words[16] = {0};
+    for (uint64_t w = 0; w < width; w++) std::memcpy(&words[w], r + L * 6 + w * 8, 8);
+    uint64_t planes[4] = {0, 0, 0, 0};
+    for (uint32_t l = 0; l < L; l++) {
+      uint32_t sbv; uint16_t dv;
+      std::memcpy(&sbv, r + l * 4, 4); std::memcpy(&dv, r + L * 4 + l * 2, 2);
+      uint32_t sym = h.l2s[l];
+      cnt[sym] = sbv + dv;
+      uint64_t m;
+      if (h.encoding == 1) m = words[l];
+      else if (h.num_planes == 0) m = ~0ull;
+      else { m = ~0ull; for (uint32_t p = 0; p < h.num_planes; p++) m &= ((l >> p) & 1) ? words[p] : ~words[p]; }
+      if (b == nblk - 1 && (n & 63)) m &= (1ull << (n & 63)) - 1;   // rows past the text
+      for (int p = 0; p < 4; p++) if ((sym >> p) & 1) planes[p] |= m;
+    }
+    if (b % 64 == 0) { std::memcpy(cur_sb, cnt, 64); std::memcpy(&sbc[(b / 64) * 16], cnt, 64); }
+    uint16_t deltas[16];
+    for (int sy = 0; sy < 16; sy++) deltas[sy] = (uint16_t)(cnt[sy] - cur_sb[sy]);
+    std::memcpy(&occ[b * 16], deltas, 32);
+    std::memcpy(&occ[b * 16 + 8], planes, 32);
+    // sampled-SA record: bits + rank before (validated equal to the stored sb + delta)
+    uint64_t word; uint32_t sb; uint16_t d;
+    std::memcpy(&word, h.ssa_words + b * 14, 8); std::memcpy(&sb, h.ssa_words + b * 14 + 8, 4);
+    std::memcpy(&d, h.ssa_words + b * 14 + 12, 2);
+    if (b == nblk - 1 && (n & 63)) word &= (1ull << (n & 63)) - 1;
+    ssa[b * 4 + 0] = (uint32_t)word; ssa[b * 4 + 1] = (uint32_t)(word >> 32); ssa[b * 4 + 2] = sb + d;
+  }
+  // symbols absent from the lane map are absent from the text
+  uint16_t sym_mask = 0;
+  for (int sy = 0; sy < 16; sy++) if (h.s2l[sy] != 0xFF) sym_mask |= (uint16_t)(1u << sy);
+  RET(upload(f.occ, occ.data(), occ.size() * 4, s));
+  RET(upload(f.sbc, sbc.data(), sbc.size() * 4, s));
+  RET(upload(f.ssa, ssa.data(), ssa.size() * 4, s));
+  RET(upload(f.sa_vals, h.sa_vals, h.n_sa_vals * 4, s));
+  RET(upload(f.bounds, h.seq_boundaries.data(), h.seq_boundaries.size() * 4, s));
+  if (h.has_lookup) RET(upload(f.lut, h.lookup_intervals, h.n_lookup * 8, s));
+  uint16_t cm[16];
+  compat_masks(h.tag, cm);
+  RET(upload(f.compat, cm, sizeof(cm), s));
+  CK(cudaStreamSynchronize(s));      // host vectors die at return
+  DevFm& d = f.d;
+  d.occ = f.occ.as<uint4>(); d.sbc = f.sbc.as<uint4>(); d.ssa = f.ssa.as<uint4>();
+  d.sa_vals = f.sa_vals.as<uint32_t>(); d.seq_bounds = f.bounds.as<uint32_t>();
+  d.lut = h.has_lookup ? f.lut.as<uint2>() : nullptr;
+  d.text_len = n; d.num_seqs = (uint32_t)h.seq_boundaries.size(); d.sample_rate = h.sample_rate;
+  d.lut_depth = h.has_lookup ? h.lookup_depth : 0; d.tag = h.tag;
+  d.lut_radix = (uint32_t)h.lookup_core.size(); d.num_blocks = (uint32_t)nblk;
+  std::memcpy(d.C, h.C, 64); std::memcpy(d.s2l, h.s2l, 16); std::memcpy(d.l2s, h.l2s, 16);
+  std::memset(d.lut_digit, 0xFF, 16);
+  for (size_t k = h.lookup_core.size(); k-- > 0;) if (h.lookup_core[k] < 16) d.lut_digit[h.lookup_core[k]] = (uint8_t)k;
+  d.sym_mask = sym_mask;
+  f.text_len = n; f.num_seqs = h.num_sequences; f.lookup_depth = d.lut_depth; f.tag = h.tag;
+  f.num_lanes = L; f.encoding = h.encoding; f.rate = h.sample_rate; f.seq_boundaries = h.seq_boundaries;
+  return HFM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Scan helper: out[0..n] = exclusive scan of in (stride in elements), out[n] = total.
+// ---------------------------------------------------------------------------
+template <class T>
+static int scan(hfm_index* x, const T* in, uint32_t stride, uint64_t n, uint64_t* out, uint32_t& launches) {
+  if (n == 0) { CK(cudaMemsetAsync(out, 0, 8, x->stream)); return HFM_OK; }
+  uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  RET(x->scan_tmp.ensure((tiles + 1) * 8));
+  uint64_t* sums = x->scan_tmp.as<uint64_t>();
+  k_scan_tiles<T><<<(unsigned)tiles, SCAN_T, 0, x->stream>>>(in, stride, n, out, sums);
+  k_scan_sums<<<1, 1024, 0, x->stream>>>(sums, (uint32_t)tiles);
+  k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, x->stream>>>(out, n, sums, (uint32_t)tiles);
+  launches += 3;
+  CK(cudaGetLastError());
+  return HFM_OK;
+}
+
+static int read_ctr(hfm_index* x) {
+  CK(cudaMemcpyAsync(x->h_ctr, x->ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  return HFM_OK;
+}
+
+static Counters* dctr(hfm_index* x) { return x->ctr.as<Counters>(); }
+
+static int read_u64(hfm_index* x, const uint64_t* dsrc, uint64_t& v) {
+  CK(cudaMemcpyAsync(&x->h_ctr->steps, dsrc, 8, cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  v = x->h_ctr->steps;
+  return HFM_OK;
+}
+
+static constexpr int BS_K = 16;        // fast-path interval-set capacity (backward search)
+static constexpr int MEM_K = 32;       // fast-path interval-set capacity (SMEM / MEM)
+static constexpr int MEM_KC = 32;      // fast-path candidate capacity
+
+// Backward search for a batch.  with_ivs = false: counts only.
+static int run_bsearch(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t cap,
+                       bool with_ivs, uint32_t* d_counts, uint32_t& launches) {
+  const FmDev& F = x->fwd;
+  RET(x->nhits.ensure((size_t)nq * 8 + 8)); RET(x->niv.ensure((size_t)nq * 4 + 4));
+  RET(x->ivoff.ensure((size_t)nq * 8 + 8)); RET(x->status.ensure((size_t)nq * 4 + 4));
+  RET(x->ovf.ensure((size_t)nq * 4 + 4));
+  if (with_ivs) {
+    if (x->iv_cap < (uint64_t)nq * 2 + 1024) x->iv_cap = (uint64_t)nq * 2 + 1024;
+    RET(x->ivpool.ensure(x->iv_cap * 8));
+    x->iv_cap = x->ivpool.cap / 8;
+  }
+  for (int attempt = 0; attempt < 8; attempt++) {
+    CK(cudaMemsetAsync(x->ctr.p, 0, sizeof(Counters), x->stream));
+    Pool pool{x->ivpool.p, &dctr(x)->iv_used, x->iv_cap};
+    BsOut o{d_counts, with_ivs ? x->nhits.as<uint64_t>() : nullptr, x->niv.as<uint32_t>(), x->ivoff.as<uint64_t>(),
+            x->status.as<uint32_t>(), x->ovf.as<uint32_t>(), &dctr(x)->n_ovf, &dctr(x)->touches};
+    if (nq) {
+      unsigned grid = (nq + 255) / 256;
+      if (x->count_work) k_bsearch<BS_K, true><<<grid, 256, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, nq, cap, pool, o);
+      else k_bsearch<BS_K, false><<<grid, 256, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, nq, cap, pool, o);
+      launches++;
+      CK(cudaGetLastError());
+    }
+    RET(read_ctr(x));
+    uint32_t n_ovf = x->h_ctr->n_ovf;
+    if (n_ovf) {
+      // fallback: large global-memory sets, doubling until every query fits
+      uint32_t set_cap = 4096;
+      while (true) {
+        uint32_t per = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n_ovf, (1ull << 30) / ((uint64_t)set_cap * 16)));
+        RET(x->work.ensure((size_t)per * set_cap * 16));
+        CK(cudaMemsetAsync(&dctr(x)->still_ovf, 0, 4, x->stream));
+        for (uint32_t b = 0; b < n_ovf; b += per) {
+          uint32_t cnt = std::min(per, n_ovf - b);
+          if (x->count_work) k_bsearch_big<true><<<(cnt + 127) / 128, 128, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>() + b, cnt, cap, x->work.as<uint2>(), set_cap, pool, o, &dctr(x)->still_ovf);
+          else k_bsearch_big<false><<<(cnt + 127) / 128, 128, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>() + b, cnt, cap, x->work.as<uint2>(), set_cap, pool, o, &dctr(x)->still_ovf);
+          launches++;
+          CK(cudaGetLastError());
+        }
+        RET(read_ctr(x));
+        x->stats.fallback_reads += n_ovf;
+        if (x->h_ctr->still_ovf == 0) break;
+        if (set_cap >= (1u << 24)) return set_error(HFM_E_OVERFLOW, "interval set exceeds 2^24 intervals");
+        set_cap *= 4;
+      }
+    }
+    if (!with_ivs || x->h_ctr->iv_used <= x->iv_cap) {
+      x->stats.occ_touches += x->h_ctr->touches;
+      return HFM_OK;
+    }
+    x->iv_cap = x->h_ctr->iv_used + x->h_ctr->iv_used / 2 + 1024;   // pool exhausted: grow, re-run
+    RET(x->ivpool.ensure(x->iv_cap * 8));
+    x->iv_cap = x->ivpool.cap / 8;
+  }
+  return set_error(HFM_E_OVERFLOW, "interval pool did not converge");
+}
+
+static int resolve(hfm_index* x, const FmDev& F, const uint32_t* seg_row, uint32_t stride, const uint64_t* seg_off,
+                   uint64_t nseg, uint64_t total, const uint32_t* d_bounds, uint32_t nb, uint32_t* out,
+                   uint32_t& launches) {
+  if (total == 0) return HFM_OK;
+  if (nseg >= 0xFFFFFFFFull) return set_error(HFM_E_ARG, "too many intervals in one call");
+  ResolveArgs A{seg_row, stride, seg_off, (uint32_t)nseg, total, d_bounds, nb,
+                F.rate ? F.rate : F.text_len, out, &dctr(x)->walk_err, &dctr(x)->steps};
+  uint64_t blocks = (total + RES_T - 1) / RES_T;
+  // grid.x limit 2^31-1 blocks covers 5e11 positions
+  if (x->count_work) k_resolve<true><<<(unsigned)blocks, RES_T, 0, x->stream>>>(F.d, A);
+  else k_resolve<false><<<(unsigned)blocks, RES_T, 0, x->stream>>>(F.d, A);
+  launches++;
+  CK(cudaGetLastError());
+  return HFM_OK;
+}
+
+static void begin_stats(hfm_index* x) {
+  x->stats = hfm_stats{};
+  cudaEventRecord(x->ev[0], x->stream);
+}
+static void end_stats(hfm_index* x) {
+  cudaEventRecord(x->ev[2], x->stream);
+  cudaEventSynchronize(x->ev[2]);
+  float a = 0, b = 0;
+  cudaEventElapsedTime(&a, x->ev[0], x->ev[1]);
+  cudaEventElapsedTime(&b, x->ev[1], x->ev[2]);
+  x->stats.ms_search = a; x->stats.ms_resolve = b; x->stats.ms_total = a + b;
+}
+
+// ---------------------------------------------------------------------------
+// Pipelines (device buffers in, device buffers out)
+// ---------------------------------------------------------------------------
+static int count_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t* d_counts) {
+  begin_stats(x);
+  uint32_t launches = 0;
+  RET(run_bsearch(x, d_q, d_qoff, nq, 0, false, d_counts, launches));
+  cudaEventRecord(x->ev[1], x->stream);
+  end_stats(x);
+  x->stats.search_launches = launches;
+  return HFM_OK;
+}
+
+static int locate_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t cap,
+                         hfm_dev_hits* out) {
+  begin_stats(x);
+  uint32_t launches = 0, other = 0;
+  RET(x->counts.ensure((size_t)nq * 4 + 4));
+  RET(run_bsearch(x, d_q, d_qoff, nq, cap, true, x->counts.as<uint32_t>(), launches));
+  RET(x->seg_base.ensure(((size_t)nq + 1) * 8));
+  RET(x->pos_base.ensure(((size_t)nq + 1) * 8));
+  RET(scan(x, x->niv.as<uint32_t>(), 1, nq, x->seg_base.as<uint64_t>(), other));
+  RET(scan(x, x->nhits.as<uint64_t>(), 1, nq, x->pos_base.as<uint64_t>(), other));
+  uint64_t nseg = 0, total = 0;
+  RET(read_u64(x, x->seg_base.as<uint64_t>() + nq, nseg));
+  RET(read_u64(x, x->pos_base.as<uint64_t>() + nq, total));
+  RET(x->seg_row.ensure(nseg * 4 + 4));
+  RET(x->seg_off.ensure((nseg + 1) * 8));
+  RET(x->out_pairs.ensure(total * 8 + 8));
+  if (nq) {
+    k_gather_locate<<<(nq + 255) / 256, 256, 0, x->stream>>>(x->ivpool.as<uint2>(), x->ivoff.as<uint64_t>(),
+                                                            x->niv.as<uint32_t>(), x->seg_base.as<uint64_t>(),
+                                                            x->pos_base.as<uint64_t>(), nq, cap,
+                                                            x->seg_row.as<uint32_t>(), x->seg_off.as<uint64_t>());
+    other++;
+    CK(cudaGetLastError());
+  }
+  CK(cudaMemcpyAsync(x->seg_off.as<uint64_t>() + nseg, &total, 8, cudaMemcpyHostToDevice, x->stream));
+  cudaEventRecord(x->ev[1], x->stream);
+  uint32_t rl = 0;
+  RET(resolve(x, x->fwd, x->seg_row.as<uint32_t>(), 1, x->seg_off.as<uint64_t>(), nseg, total,
+              x->fwd.bounds.as<uint32_t>(), (uint32_t)x->fwd.seq_boundaries.size(), x->out_pairs.as<uint32_t>(), rl));
+  RET(read_ctr(x));
+  end_stats(x);
+  x->stats.search_launches = launches; x->stats.resolve_launches = rl; x->stats.other_launches = other;
+  x->stats.rows_resolved = total; x->stats.lf_steps = x->h_ctr->steps;
+  if (x->h_ctr->walk_err) return set_error(HFM_E_WALK, "LF walk exceeded sample_rate steps: index inconsistent");
+  out->nq = nq; out->total = total;
+  out->d_offsets = x->pos_base.as<uint64_t>(); out->d_counts = x->counts.as<uint32_t>();
+  out->d_pairs = x->out_pairs.as<uint32_t>();
+  return HFM_OK;
+}
+
+static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t min_len,
+                       uint32_t mode, const uint32_t* h_bounds, uint32_t nb, uint32_t cap, hfm_dev_mems* out) {
+  if (x->kind != HFM_KIND_BIDIR) return set_error(HFM_E_ARG, "MEM/SMEM search needs a bidirectional index");
+  if (mode > 1) return set_error(HFM_E_ARG, "mode must be 0 (SMEM) or 1 (MEM)");
+  begin_stats(x);
+  uint32_t launches = 0, other = 0;
+  RET(x->ref_bounds.ensure((size_t)nb * 4 + 4));
+  if (nb) CK(cudaMemcpyAsync(x->ref_bounds.p, h_bounds, (size_t)nb * 4, cudaMemcpyHostToDevice, x->stream));
+  RET(x->hit_start.ensure((size_t)nq * 8 + 8)); RET(x->hit_count.ensure((size_t)nq * 4 + 4));
+  RET(x->status.ensure((size_t)nq * 4 + 4)); RET(x->ovf.ensure((size_t)nq * 4 + 4));
+  if (x->iv_cap < (uint64_t)nq * 24 + 4096) x->iv_cap = (uint64_t)nq * 24 + 4096;     // BIv = 16 B
+  if (x->hit_cap < (uint64_t)nq * 24 + 4096) x->hit_cap = (uint64_t)nq * 24 + 4096;   // hit = 32 B
+  MemsParams P{min_len, mode, cap, nb ? 1u : 0u};
+  const FmDev& Fw = x->fwd; const FmDev& Rv = x->rev;
+  bool done = false;
+  for (int attempt = 0; attempt < 8 && !done; attempt++) {
+    RET(x->ivpool.ensure(x->iv_cap * 16)); x->iv_cap = x->ivpool.cap / 16;
+    RET(x->hitpool.ensure(x->hit_cap * 32)); x->hit_cap = x->hitpool.cap / 32;
+    CK(cudaMemsetAsync(x->ctr.p, 0, sizeof(Counters), x->stream));
+    Pool ivp{x->ivpool.p, &dctr(x)->iv_used, x->iv_cap}, hp{x->hitpool.p, &dctr(x)->hit_used, x->hit_cap};
+    MemsOut o{x->hit_start.as<uint64_t>(), x->hit_count.as<uint32_t>(), x->status.as<uint32_t>(),
+              x->ovf.as<uint32_t>(), &dctr(x)->n_ovf, &dctr(x)->touches};
+    if (nq) {
+      unsigned grid = (nq + 127) / 128;
+      if (x->count_work) k_mems<MEM_K, MEM_KC, true><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, nq, P, ivp, hp, o);
+      else k_mems<MEM_K, MEM_KC, false><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, nq, P, ivp, hp, o);
+      launches++;
+      CK(cudaGetLastError());
+    }
+    RET(read_ctr(x));
+    uint32_t n_ovf = x->h_ctr->n_ovf;
+    if (n_ovf) {
+      uint32_t set_cap = 1024, cand_cap = 1024;
+      while (true) {
+        uint64_t per_thread = (uint64_t)set_cap * 4 * 16 + (uint64_t)cand_cap * sizeof(Cand);
+        uint32_t per = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n_ovf, (1ull << 30) / per_thread));
+        RET(x->work.ensure((size_t)per * set_cap * 4 * 16));
+        RET(x->cwork.ensure((size_t)per * cand_cap * sizeof(Cand)));
+        CK(cudaMemsetAsync(&dctr(x)->still_ovf, 0, 4, x->stream));
+        for (uint32_t b = 0; b < n_ovf; b += per) {
+          uint32_t cnt = std::min(per, n_ovf - b);
+          if (x->count_work) k_mems_big<true><<<(cnt + 63) / 64, 64, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>() + b, cnt, P, x->work.as<BIv>(), set_cap, x->cwork.as<Cand>(), cand_cap, ivp, hp, o, &dctr(x)->still_ovf);
+          else k_mems_big<false><<<(cnt + 63) / 64, 64, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>() + b, cnt, P, x->work.as<BIv>(), set_cap, x->cwork.as<Cand>(), cand_cap, ivp, hp, o, &dctr(x)->still_ovf);
+          launches++;
+          CK(cudaGetLastError());
+        }
+        RET(read_ctr(x));
+        x->stats.fallback_reads += n_ovf;
+        if (x->h_ctr->still_ovf == 0) break;
+        if (set_cap >= (1u << 22)) return set_error(HFM_E_OVERFLOW, "MEM interval set exceeds 2^22 intervals");
+        set_cap *= 4; cand_cap *= 4;
+      }
+    }
+    if (x->h_ctr->iv_used <= x->iv_cap && x->h_ctr->hit_used <= x->hit_cap) { done = true; break; }
+    x->iv_cap = std::max(x->iv_cap, (uint64_t)(x->h_ctr->iv_used * 3 / 2 + 4096));
+    x->hit_cap = std::max(x->hit_cap, (uint64_t)(x->h_ctr->hit_used * 3 / 2 + 4096));
+  }
+  if (!done) return set_error(HFM_E_OVERFLOW, "MEM pools did not converge");
+  x->stats.occ_touches += x->h_ctr->touches;
+  // CSR of hits, then positions
+  RET(x->hit_base.ensure(((size_t)nq + 1) * 8));
+  RET(scan(x, x->hit_count.as<uint32_t>(), 1, nq, x->hit_base.as<uint64_t>(), other));
+  uint64_t nh = 0;
+  RET(read_u64(x, x->hit_base.as<uint64_t>() + nq, nh));
+  RET(x->hits.ensure(nh * 32 + 32));
+  if (nq) {
+    k_gather_hits<<<(nq + 255) / 256, 256, 0, x->stream>>>(x->hitpool.as<uint4>(), x->hit_start.as<uint64_t>(),
+                                                          x->hit_count.as<uint32_t>(), x->hit_base.as<uint64_t>(), nq,
+                                                          x->hits.as<uint4>());
+    other++;
+    CK(cudaGetLastError());
+  }
+  RET(x->npos_scan.ensure((nh + 1) * 8));
+  RET(scan(x, x->hits.as<uint32_t>() + 5, 8, nh, x->npos_scan.as<uint64_t>(), other));
+  uint64_t npos = 0;
+  RET(read_u64(x, x->npos_scan.as<uint64_t>() + nh, npos));
+  if (nh) {
+    k_set_pos_off<<<(unsigned)((nh + 255) / 256), 256, 0, x->stream>>>(x->hits.as<uint32_t>(), x->npos_scan.as<uint64_t>(), nh);
+    other++;
+    CK(cudaGetLastError());
+  }
+  RET(x->out_pairs.ensure(npos * 8 + 8));
+  cudaEventRecord(x->ev[1], x->stream);
+  uint32_t rl = 0;
+  RET(resolve(x, Fw, x->hits.as<uint32_t>() + 4, 8, x->npos_scan.as<uint64_t>(), nh, npos,
+              x->ref_bounds.as<uint32_t>(), nb, x->out_pairs.as<uint32_t>(), rl));
+  RET(read_ctr(x));
+  end_stats(x);
+  x->stats.search_launches = launches; x->stats.resolve_launches = rl; x->stats.other_launches = other;
+  x->stats.rows_resolved = npos; x->stats.lf_steps = x->h_ctr->steps;
+  if (x->h_ctr->walk_err) return set_error(HFM_E_WALK, "LF walk exceeded sample_rate steps: index inconsistent");
+  out->nq = nq; out->n_hits = nh; out->n_positions = npos;
+  out->d_hit_offsets = x->hit_base.as<uint64_t>(); out->d_hits = x->hits.as<hfm_mem_hit>();
+  out->d_positions = x->out_pairs.as<uint32_t>();
+  return HFM_OK;
+}
+
+// H2D of a host query batch into the handle's buffers.
+static int stage_queries(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32_t nq) {
+  if (nq && (!q_off)) return set_error(HFM_E_ARG, "q_off is NULL");
+  uint64_t bytes = nq ? q_off[nq] : 0;
+  for (uint32_t i = 0; i < nq; i++) if (q_off[i + 1] < q_off[i]) return set_error(HFM_E_ARG, "q_off not ascending");
+  if (bytes && !q) return set_error(HFM_E_ARG, "q is NULL");
+  RET(x->q.ensure(bytes + 16));
+  RET(x->qoff.ensure(((size_t)nq + 1) * 8));
+  if (bytes) CK(cudaMemcpyAsync(x->q.p, q, bytes, cudaMemcpyHostToDevice, x->stream));
+  if (nq) CK(cudaMemcpyAsync(x->qoff.p, q_off, ((size_t)nq + 1) * 8, cudaMemcpyHostToDevice, x->stream));
+  return HFM_OK;
+}
+
+struct Guard {
+  hfm_index* x;
+  std::unique_lock<std::mutex> lk;
+  explicit Guard(hfm_index* i) : x(i), lk(i->mu) { cudaSetDevice(i->device); }
+};
+
+}  // namespace hfm
+
+// ===========================================================================
+// extern "C"
+// ===========================================================================
+extern "C" {
+
+const char* hfm_last_error(void) { return hfm::g_err.c_str(); }
+
+void hfm_free(void* p) { std::free(p); }
+
+int hfm_index_load(const uint8_t* bytes, size_t len, int kind, const hfm_opts* opts, hfm_index** out) {
+  if (!bytes || !out) return set_error(HFM_E_ARG, "NULL argument");
+  if (kind != HFM_KIND_FM && kind != HFM_KIND_BIDIR) return set_error(HFM_E_ARG, "kind must be 0 or 1");
+  *out = nullptr;
+  HostFm hf, hr;
+  if (kind == HFM_KIND_FM) RET(parse_fm(bytes, len, hf));
+  else {
+    // BidirFmIndex::from_bytes (src/fm_index/bidir_index.rs:195-210)
+    if (len < 4) return set_error(HFM_E_FORMAT, "truncated bidirectional index");
+    uint32_t fl; std::memcpy(&fl, bytes, 4);
+    if (len < 4ull + fl) return set_error(HFM_E_FORMAT, "truncated forward index");
+    RET(parse_fm(bytes + 4, fl, hf));
+    RET(parse_fm(bytes + 4 + fl, len - 4 - fl, hr));
+    if (hr.text_len != hf.text_len) return set_error(HFM_E_FORMAT, "forward and reverse text lengths differ");
+  }
+  int dev = opts ? opts->device : 0;
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (dev < 0 || dev >= ndev) return set_error(HFM_E_ARG, "device ordinal out of range");
+  CK(cudaSetDevice(dev));
+  std::unique_ptr<hfm_index> x(new hfm_index());
+  x->device = dev; x->kind = kind;
+  CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
+  for (auto& e : x->ev) CK(cudaEventCreate(&e));
+  CK(cudaMallocHost((void**)&x->h_ctr, sizeof(Counters)));
+  RET(x->ctr.ensure(sizeof(Counters)));
+  RET(build_device_fm(hf, x->fwd, x->stream));
+  if (kind == HFM_KIND_BIDIR) RET(build_device_fm(hr, x->rev, x->stream));
+  *out = x.release();
+  return HFM_OK;
+}
+
+void hfm_index_free(hfm_index* x) {
+  if (!x) return;
+  cudaSetDevice(x->device);
+  if (x->stream) cudaStreamSynchronize(x->stream);
+  for (DevBuf* b : {&x->fwd.occ, &x->fwd.sbc, &x->fwd.ssa, &x->fwd.sa_vals, &x->fwd.lut, &x->fwd.bounds,
+                    &x->fwd.compat, &x->rev.occ, &x->rev.sbc, &x->rev.ssa, &x->rev.sa_vals, &x->rev.lut,
+                    &x->rev.bounds, &x->rev.compat, &x->q, &x->qoff, &x->counts, &x->nhits, &x->niv, &x->ivoff,
+                    &x->status, &x->ovf, &x->ivpool, &x->hitpool, &x->seg_row, &x->seg_off, &x->pos_base,
+                    &x->seg_base, &x->scan_tmp, &x->out_pairs, &x->ref_bounds, &x->hit_start, &x->hit_count,
+                    &x->hit_base, &x->hits, &x->npos_scan, &x->work, &x->cwork, &x->ctr})
+    b->release();
+  for (auto& e : x->ev) if (e) cudaEventDestroy(e);
+  if (x->h_ctr) cudaFreeHost(x->h_ctr);
+  if (x->stream) cudaStreamDestroy(x->stream);
+  delete x;
+}
+
+int hfm_index_info_get(const hfm_index* x, hfm_index_info* o) {
+  if (!x || !o) return set_error(HFM_E_ARG, "NULL argument");
+  o->kind = x->kind; o->text_len = x->fwd.text_len; o->num_sequences = x->fwd.num_seqs;
+  o->sample_rate = x->fwd.rate; o->lookup_depth = x->fwd.lookup_depth; o->alphabet_tag = x->fwd.tag;
+  o->num_lanes = x->fwd.num_lanes; o->encoding = x->fwd.encoding;
+  o->device_bytes = x->fwd.bytes() + x->rev.bytes();
+  return HFM_OK;
+}
+
+void* hfm_index_stream(hfm_index* x) { return x ? (void*)x->stream : nullptr; }
+
+int hfm_last_stats(const hfm_index* x, hfm_stats* o) {
+  if (!x || !o) return set_error(HFM_E_ARG, "NULL argument");
+  *o = x->stats;
+  return HFM_OK;
+}
+
+int hfm_set_counters(hfm_index* x, int enable) {
+  if (!x) return set_error(HFM_E_ARG, "NULL argument");
+  x->count_work = enable != 0;
+  return HFM_OK;
+}
+
+int hfm_count_batch_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t* d_counts) {
+  if (!x || (nq && (!d_qoff || !d_counts))) return set_error(HFM_E_ARG, "NULL argument");
+  Guard g(x);
+  return count_device(x, d_q, d_qoff, nq, d_counts);
+}
+
+int hfm_locate_batch_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t cap,
+                            hfm_dev_hits* out) {
+  if (!x || !out || (nq && !d_qoff)) return set_error(HFM_E_ARG, "NULL argument");
+  Guard g(x);
+  return locate_device(x, d_q, d_qoff, nq, cap, out);
+}
+
+int hfm_mems_batch_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t min_len,
+                          uint32_t mode, const uint32_t* ref_bounds, uint32_t nb, uint32_t cap, hfm_dev_mems* out) {
+  if (!x || !out || (nq && !d_qoff) || (nb && !ref_bounds)) return set_error(HFM_E_ARG, "NULL argument");
+  Guard g(x);
+  return mems_device(x, d_q, d_qoff, nq, min_len, mode, ref_bounds, nb, cap, out);
+}
+
+int hfm_count_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32_t nq, uint32_t* counts_out) {
+  if (!x || (nq && !counts_out)) return set_error(HFM_E_ARG, "NULL argument");
+  Guard g(x);
+  RET(stage_queries(x, q, q_off, nq));
+  RET(x->counts.ensure((size_t)nq * 4 + 4));
+  RET(count_device(x, x->q.as<uint8_t>(), x->qoff.as<uint64_t>(), nq, x->counts.as<uint32_t>()));
+  if (nq) CK(cudaMemcpyAsync(counts_out, x->counts.p, (size_t)nq * 4, cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  return HFM_OK;
+}
+
+int hfm_locate_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32_t nq, uint32_t cap, hfm_hits** out) {
+  if (!x || !out) return set_error(HFM_E_ARG, "NULL argument");
+  *out = nullptr;
+  Guard g(x);
+  RET(stage_queries(x, q, q_off, nq));
+  hfm_dev_hits d{};
+  RET(locate_device(x, x->q.as<uint8_t>(), x->qoff.as<uint64_t>(), nq, cap, &d));
+  // one malloc block: struct | offsets | counts | pairs
+  size_t bytes = sizeof(hfm_hits) + ((size_t)nq + 1) * 8 + (size_t)nq * 4 + 4 + (size_t)d.total * 8;
+  uint8_t* blk = (uint8_t*)std::malloc(bytes);
+  if (!blk) return set_error(HFM_E_OOM, "host allocation failed");
+  hfm_hits* h = (hfm_hits*)blk;
+  h->nq = nq; h->_pad = 0; h->total = d.total;
+  h->offsets = (uint64_t*)(blk + sizeof(hfm_hits));
+  h->pairs = (uint32_t*)(h->offsets + nq + 1);
+  h->counts = h->pairs + d.total * 2;
+  CK(cudaMemcpyAsync(h->offsets, d.d_offsets, ((size_t)nq + 1) * 8, cudaMemcpyDeviceToHost, x->stream));
+  if (d.total) CK(cudaMemcpyAsync(h->pairs, d.d_pairs, (size_t)d.total * 8, cudaMemcpyDeviceToHost, x->stream));
+  if (nq) CK(cudaMemcpyAsync(h->counts, d.d_counts, (size_t)nq * 4, cudaMemcpyDeviceToHost, x->stream));
+  cudaError_t e = cudaStreamSynchronize(x->stream);
+  if (e != cudaSuccess) { std::free(blk); return set_error(HFM_E_CUDA, cudaGetErrorString(e)); }
+  *out = h;
+  return HFM_OK;
+}
+
+int hfm_mems_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32_t nq, uint32_t min_len, uint32_t mode,
+                   const uint32_t* ref_bounds, uint32_t nb, uint32_t cap, hfm_mem_out** out) {
+  if (!x || !out || (nb && !ref_bounds)) return set_error(HFM_E_ARG, "NULL argument");
+  *out = nullptr;
+  Guard g(x);
+  RET(stage_queries(x, q, q_off, nq));
+  hfm_dev_mems d{};
+  RET(mems_device(x, x->q.as<uint8_t>(), x->qoff.as<uint64_t>(), nq, min_len, mode, ref_bounds, nb, cap, &d));
+  size_t bytes = sizeof(hfm_mem_out) + ((size_t)nq + 1) * 8 + (size_t)d.n_hits * sizeof(hfm_mem_hit) +
+                 (size_t)d.n_positions * 8 + 8;
+  uint8_t* blk = (uint8_t*)std::malloc(bytes);
+  if (!blk) return set_error(HFM_E_OOM, "host allocation failed");
+  hfm_mem_out* m = (hfm_mem_out*)blk;
+  m->nq = nq; m->_pad = 0; m->n_hits = d.n_hits; m->n_positions = d.n_positions;
+  m->hit_offsets = (uint64_t*)(blk + sizeof(hfm_mem_out));
+  m->hits = (hfm_mem_hit*)(m->hit_offsets + nq + 1);
+  m->positions = (uint32_t*)(m->hits + d.n_hits);
+  CK(cudaMemcpyAsync(m->hit_offsets, d.d_hit_offsets, ((size_t)nq + 1) * 8, cudaMemcpyDeviceToHost, x->stream));
+  if (d.n_hits) CK(cudaMemcpyAsync(m->hits, d.d_hits, (size_t)d.n_hits * sizeof(hfm_mem_hit), cudaMemcpyDeviceToHost, x->stream));
+  if (d.n_positions) CK(cudaMemcpyAsync(m->positions, d.d_positions, (size_t)d.n_positions * 8, cudaMemcpyDeviceToHost, x->stream));
+  cudaError_t e = cudaStreamSynchronize(x->stream);
+  if (e != cudaSuccess) { std::free(blk); return set_error(HFM_E_CUDA, cudaGetErrorString(e)); }
+  *out = m;
+  return HFM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,194 @@
+// resolve.cuh — SA-position resolve (LF walk to a sampled row) fused with the reference
+// boundary map, plus the scan / gather kernels that lay results out per read.
+//
+// One thread per output position.  Positions are grouped in segments (one per SA
+// interval, rows lo .. lo+n); a block finds its segments once and every thread locates
+// its own segment in shared memory.  Replaces locate_resolve.wgsl:98-176,
+// mem_resolve.wgsl:101-136 and ref_map.wgsl:32-59 of the reference, with the CPU
+// resolve_sa / map_position semantics (src/fm_index/query.rs:282-357).
+#pragma once
+#include "dev_index.cuh"
+
+namespace hfm {
+
+struct ResolveArgs {
+  const uint32_t* seg_row;      // row of the segment's first position
+  uint32_t row_stride;          // in u32 units
+  const uint64_t* seg_off;      // nseg + 1 ascending position offsets
+  uint32_t nseg;
+  uint64_t total;
+  const uint32_t* bounds;       // map position -> (index, offset): partition_point(bounds <= p)
+  uint32_t nb;
+  uint32_t guard;               // max LF steps before the walk is declared broken
+  uint32_t* out;                // 2 * total u32
+  uint32_t* walk_err;
+  unsigned long long* steps;    // LF steps (nullptr: not counted)
+};
+
+constexpr int RES_T = 256;
+constexpr int RES_BOUNDS_SMEM = 2048;
+
+template <bool COUNT>
+__global__ void __launch_bounds__(RES_T) k_resolve(DevFm F, ResolveArgs A) {
+  __shared__ SmemFm S;
+  __shared__ uint64_t s_off[RES_T + 1];
+  __shared__ uint32_t s_row[RES_T];
+  __shared__ uint32_t s_b[RES_BOUNDS_SMEM];
+  __shared__ uint32_t s_first, s_cnt;
+  if (threadIdx.x < 16) { S.C[threadIdx.x] = F.C[threadIdx.x]; }
+  uint64_t p0 = (uint64_t)blockIdx.x * RES_T;
+  uint64_t p1 = min(p0 + RES_T, A.total);
+  if (threadIdx.x == 0) {
+    // segment containing p0 / p1-1: last k with seg_off[k] <= p
+    uint32_t lo = 0, hi = A.nseg;
+    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (A.seg_off[mid] <= p0) lo = mid; else hi = mid - 1; }
+    uint32_t first = lo;
+    hi = A.nseg;
+    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (A.seg_off[mid] <= p1 - 1) lo = mid; else hi = mid - 1; }
+    s_first = first; s_cnt = lo - first + 1;
+  }
+  bool smem_b = A.nb <= RES_BOUNDS_SMEM;
+  if (smem_b) for (uint32_t k = threadIdx.x; k < A.nb; k += RES_T) s_b[k] = A.bounds[k];
+  __syncthreads();
+  uint32_t first = s_first, cnt = s_cnt;
+  bool local = cnt <= RES_T;
+  if (local) {
+    for (uint32_t k = threadIdx.x; k <= cnt; k += RES_T) s_off[k] = A.seg_off[first + k];
+    for (uint32_t k = threadIdx.x; k < cnt; k += RES_T) s_row[k] = A.seg_row[(size_t)(first + k) * A.row_stride];
+  }
+  __syncthreads();
+  uint64_t p = p0 + threadIdx.x;
+  if (p >= p1) return;
+  uint32_t seg, row;
+  if (local) {
+    uint32_t lo = 0, hi = cnt - 1;
+    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (s_off[mid] <= p) lo = mid; else hi = mid - 1; }
+    seg = lo; row = s_row[lo] + (uint32_t)(p - s_off[lo]);
+  } else {
+    uint32_t lo = first, hi = A.nseg - 1;
+    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (A.seg_off[mid] <= p) lo = mid; else hi = mid - 1; }
+    seg = lo; row = A.seg_row[(size_t)lo * A.row_stride] + (uint32_t)(p - A.seg_off[lo]);
+  }
+  (void)seg;
+  // LF walk (resolve_sa, src/fm_index/query.rs:282-291)
+  uint32_t pos = row, steps = 0, val = 0, text;
+  bool ok = true;
+  for (;;) {
+    if (lf_or_sample(F, S, pos, val)) break;
+    if (++steps > A.guard) { ok = false; break; }
+  }
+  uint32_t r0, r1;
+  if (ok) {
+    text = val + steps;
+    uint32_t idx = smem_b ? upper_bound_u32(s_b, A.nb, text) : upper_bound_u32(A.bounds, A.nb, text);
+    uint32_t start = idx == 0 ? 0 : (smem_b ? s_b[idx - 1] : A.bounds[idx - 1]);
+    r0 = idx; r1 = text - start;
+  } else {
+    atomicAdd(A.walk_err, 1u);
+    r0 = 0xFFFFFFFFu; r1 = 0xFFFFFFFFu;
+  }
+  reinterpret_cast<uint2*>(A.out)[p] = make_uint2(r0, r1);
+  if (COUNT) atomicAdd(A.steps, (unsigned long long)(steps + 1));
+}
+
+// ---- exclusive scan (u32 or u64 input) -> u64 output with out[n] = total ----------
+constexpr int SCAN_T = 256, SCAN_ITEMS = 8, SCAN_TILE = SCAN_T * SCAN_ITEMS;
+
+template <class T>
+__global__ void __launch_bounds__(SCAN_T) k_scan_tiles(const T* __restrict__ in, uint32_t in_stride, uint64_t n,
+                                                      uint64_t* __restrict__ out, uint64_t* __restrict__ tile_sums) {
+  __shared__ uint64_t s[SCAN_T];
+  uint64_t base = (uint64_t)blockIdx.x * SCAN_TILE + (uint64_t)threadIdx.x * SCAN_ITEMS;
+  uint64_t v[SCAN_ITEMS], sum = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    uint64_t i = base + k;
+    v[k] = i < n ? (uint64_t)in[i * in_stride] : 0;
+    sum += v[k];
+  }
+  s[threadIdx.x] = sum;
+  __syncthreads();
+  for (int d = 1; d < SCAN_T; d <<= 1) {
+    uint64_t t = threadIdx.x >= d ? s[threadIdx.x - d] : 0;
+    __syncthreads();
+    s[threadIdx.x] += t;
+    __syncthreads();
+  }
+  uint64_t run = s[threadIdx.x] - sum;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    uint64_t i = base + k;
+    if (i < n) out[i] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == SCAN_T - 1) tile_sums[blockIdx.x] = s[SCAN_T - 1];
+}
+
+// Scans tile sums in place (single block, sequential chunks).
+__global__ void __launch_bounds__(1024) k_scan_sums(uint64_t* sums, uint32_t ntiles) {
+  __shared__ uint64_t s[1024];
+  __shared__ uint64_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < ntiles; base += 1024) {
+    uint32_t i = base + threadIdx.x;
+    uint64_t v = i < ntiles ? sums[i] : 0;
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int d = 1; d < 1024; d <<= 1) {
+      uint64_t t = threadIdx.x >= d ? s[threadIdx.x - d] : 0;
+      __syncthreads();
+      s[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < ntiles) sums[i] = carry + s[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += s[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sums[ntiles] = carry;
+}
+
+__global__ void k_scan_add(uint64_t* out, uint64_t n, const uint64_t* __restrict__ sums, uint32_t ntiles) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] += sums[i / SCAN_TILE];
+  if (i == 0) out[n] = sums[ntiles];
+}
+
+// ---- gathers ------------------------------------------------------------------
+// Locate: query intervals (pool) -> resolve segments in query order.
+__global__ void k_gather_locate(const uint2* __restrict__ ivpool, const uint64_t* __restrict__ ivoff,
+                                const uint32_t* __restrict__ niv, const uint64_t* __restrict__ seg_base,
+                                const uint64_t* __restrict__ pos_base, uint32_t nq, uint32_t cap,
+                                uint32_t* __restrict__ seg_row, uint64_t* __restrict__ seg_off) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  uint64_t sb = seg_base[i], run = pos_base[i];
+  const uint2* iv = ivpool + ivoff[i];
+  for (uint32_t k = 0; k < niv[i]; k++) {
+    uint2 v = iv[k];
+    uint32_t sz = v.y - v.x;
+    seg_row[sb + k] = v.x; seg_off[sb + k] = run;
+    run += (cap && sz > cap) ? cap : sz;
+  }
+}
+
+// Mems: per-read hits (pool) -> CSR hit array.
+__global__ void k_gather_hits(const uint4* __restrict__ hitpool, const uint64_t* __restrict__ hit_start,
+                              const uint32_t* __restrict__ hit_count, const uint64_t* __restrict__ hit_base,
+                              uint32_t nq, uint4* __restrict__ hits) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  const uint4* src = hitpool + hit_start[i] * 2;
+  uint4* dst = hits + hit_base[i] * 2;
+  for (uint32_t k = 0; k < hit_count[i] * 2; k++) dst[k] = src[k];
+}
+
+__global__ void k_set_pos_off(uint32_t* __restrict__ hits, const uint64_t* __restrict__ pos_off, uint64_t nh) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nh) return;
+  uint64_t o = pos_off[i];
+  hits[i * 8 + 6] = (uint32_t)o; hits[i * 8 + 7] = (uint32_t)(o >> 32);
+}
+
+}  // namespace hfm

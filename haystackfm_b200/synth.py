@@ -1,0 +1,102 @@
+"""Seeded synthetic references and reads for the benchmark workloads.
+
+No public dataset is named for this path, so every input is generated here with the
+shapes and value distributions of the two workloads:
+
+* exact_dna_workload — one uniform ACGT reference (1 Mbp by default), ExactDna; 32-mer
+  queries, 90% substrings at uniform positions and 10% uniform random ACGT.
+* iupac_workload — contigs with lognormal lengths (mu=13, sigma=1) rescaled to the total
+  (100 Mbp, 200 contigs by default); uniform ACGT, N runs covering 2% of the bases
+  (geometric run lengths, mean 500) and 0.5% single ambiguity codes (R..V uniform).  Reads
+  (150 bp) are drawn from either strand of the unmasked ACGT sequence — the N runs and
+  ambiguity codes mask only the reference — with 1% substitutions and 0.1% N.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+A, C, G, T, N = 1, 2, 3, 4, 5
+
+
+@dataclass
+class Reference:
+    contigs: list           # list of np.uint8 code arrays (masked reference)
+    truth: list             # unmasked ACGT arrays (reads come from these)
+    seed: int
+
+
+def exact_dna_workload(ref_len=1_000_000, n_queries=10_000, qlen=32, substr_frac=0.9, seed=1):
+    rng = np.random.default_rng(seed)
+    ref = rng.integers(1, 5, size=ref_len, dtype=np.uint8)
+    n_sub = int(round(n_queries * substr_frac))
+    starts = rng.integers(0, ref_len - qlen + 1, size=n_sub)
+    subs = ref[starts[:, None] + np.arange(qlen)[None, :]]
+    rand = rng.integers(1, 5, size=(n_queries - n_sub, qlen), dtype=np.uint8)
+    q = np.concatenate([subs, rand]).astype(np.uint8)
+    q = q[rng.permutation(n_queries)]
+    return ref, q
+
+
+def _lognormal_lengths(rng, n, total, mu=13.0, sigma=1.0, min_len=1000):
+    raw = rng.lognormal(mu, sigma, size=n)
+    lens = np.maximum(np.floor(raw / raw.sum() * total).astype(np.int64), min_len)
+    diff = total - int(lens.sum())
+    lens[int(np.argmax(lens))] += diff          # exact total
+    return lens
+
+
+def iupac_reference(total=100_000_000, n_contigs=200, n_frac=0.02, n_run_mean=500, iupac_frac=0.005,
+                    seed=2) -> Reference:
+    rng = np.random.default_rng(seed)
+    lens = _lognormal_lengths(rng, n_contigs, total, min_len=max(1000, total // (n_contigs * 50)))
+    truth_all = rng.integers(1, 5, size=total, dtype=np.uint8)
+    masked = truth_all.copy()
+    # N runs: geometric lengths with the given mean, uniform starts, until 2% is covered
+    target = int(total * n_frac)
+    n_runs = max(1, target // n_run_mean)
+    run_len = rng.geometric(1.0 / n_run_mean, size=n_runs * 2)
+    run_len = run_len[np.cumsum(run_len) <= target] if run_len.sum() > target else run_len
+    starts = rng.integers(0, total, size=len(run_len))
+    for s, l in zip(starts, run_len):
+        masked[s:s + l] = N
+    # single ambiguity codes R..V (6..15) at uniform positions
+    k = int(total * iupac_frac)
+    pos = rng.integers(0, total, size=k)
+    masked[pos] = rng.integers(6, 16, size=k, dtype=np.uint8)
+    bounds = np.concatenate([[0], np.cumsum(lens)])
+    contigs = [masked[bounds[i]:bounds[i + 1]] for i in range(n_contigs)]
+    truth = [truth_all[bounds[i]:bounds[i + 1]] for i in range(n_contigs)]
+    return Reference(contigs, truth, seed)
+
+
+def sample_reads(ref: Reference, n_reads=1_000_000, read_len=150, sub_rate=0.01, n_rate=0.001, seed=3):
+    """Reads from either strand of the unmasked sequence with substitutions and Ns."""
+    rng = np.random.default_rng(seed)
+    lens = np.array([len(t) for t in ref.truth])
+    ok = np.nonzero(lens >= read_len)[0]
+    w = (lens[ok] - read_len + 1).astype(np.float64)
+    cid = ok[rng.choice(len(ok), size=n_reads, p=w / w.sum())]
+    starts = (rng.random(n_reads) * (lens[cid] - read_len + 1)).astype(np.int64)
+    reads = np.empty((n_reads, read_len), dtype=np.uint8)
+    for c in np.unique(cid):
+        sel = np.nonzero(cid == c)[0]
+        reads[sel] = ref.truth[c][starts[sel, None] + np.arange(read_len)[None, :]]
+    rc = rng.random(n_reads) < 0.5
+    reads[rc] = (5 - reads[rc])[:, ::-1]
+    sub = rng.random(reads.shape) < sub_rate
+    shift = rng.integers(1, 4, size=reads.shape, dtype=np.uint8)
+    reads = np.where(sub, ((reads - 1 + shift) % 4) + 1, reads).astype(np.uint8)
+    reads[rng.random(reads.shape) < n_rate] = N
+    return reads
+
+
+def pack_rows(rows: np.ndarray, width=None):
+    """Fixed-length reads (n, L) -> (flat codes, u64 offsets) of the first `width` codes."""
+    if width is not None:
+        rows = rows[:, :width]
+    rows = np.ascontiguousarray(rows, dtype=np.uint8)
+    n, l = rows.shape
+    off = (np.arange(n + 1, dtype=np.uint64) * np.uint64(l))
+    return rows.reshape(-1), off

@@ -1,0 +1,170 @@
+/*
+ * hfm.h — C ABI of haystackfm_b200, the B200 (sm_100a) engine for haystackfm's
+ * batched query path: IUPAC backward search with sampled-SA locate, and the
+ * bidirectional SMEM/MEM pipeline (find intervals, resolve SA positions, map to
+ * reference boundaries).
+ *
+ * Plain C types only.  Every entry point returns an hfm status (0 = OK, < 0 =
+ * error; message via hfm_last_error()).  Queries are encoded IUPAC codes 0..15
+ * (src/alphabet.rs:3-52 of the reference), concatenated, with nq+1 u64 offsets.
+ *
+ * Each declaration names the reference interface it replaces (file:line in
+ * sriram98v/haystackfm).  Results are bit-exact with the reference CPU
+ * count / locate / find_smems / find_mems on the same index bytes.
+ */
+#ifndef HFM_H
+#define HFM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define HFM_OK 0
+#define HFM_E_CUDA (-1)     /* CUDA runtime error (maps to FmIndexError::GpuError)          */
+#define HFM_E_OOM (-2)      /* device or host allocation failed                             */
+#define HFM_E_FORMAT (-3)   /* bad bincode / alphabet tag / inconsistent index (DeserializeError) */
+#define HFM_E_ARG (-4)      /* invalid argument                                             */
+#define HFM_E_TIMEOUT (-5)  /* device watchdog expired                                      */
+#define HFM_E_OVERFLOW (-6) /* a per-read work set outgrew the largest fallback capacity     */
+#define HFM_E_WALK (-7)     /* an LF walk exceeded sample_rate steps (index inconsistent)   */
+
+#define HFM_KIND_FM 0       /* FmIndex bytes        (src/fm_index/serialize.rs:13-52)       */
+#define HFM_KIND_BIDIR 1    /* BidirFmIndex bytes   (src/fm_index/bidir_index.rs:183-210)   */
+
+#define HFM_MODE_SMEM 0     /* src/gpu/mem_find.rs:9 */
+#define HFM_MODE_MEM 1      /* src/gpu/mem_find.rs:10 */
+
+typedef struct hfm_index hfm_index;   /* device-resident index, opaque */
+
+typedef struct hfm_opts {
+  int32_t device;          /* CUDA device ordinal (one index per GPU; replicate for multi-GPU) */
+  uint32_t flags;          /* reserved, 0 */
+} hfm_opts;
+
+typedef struct hfm_index_info {
+  uint32_t kind, text_len, num_sequences, sample_rate;
+  uint32_t lookup_depth, alphabet_tag, num_lanes, encoding;
+  uint64_t device_bytes;   /* HBM held by the device layout */
+} hfm_index_info;
+
+/* Locate result: per-query CSR of (seq_idx, pos_in_seq) pairs in the reference CPU
+ * order (merged SA intervals ascending, rows ascending; src/fm_index/query.rs:22-39). */
+typedef struct hfm_hits {
+  uint32_t nq;
+  uint32_t _pad;
+  uint64_t total;          /* number of pairs                                   */
+  uint64_t* offsets;       /* nq + 1                                            */
+  uint32_t* counts;        /* exact FmIndex::count per query (uncapped)         */
+  uint32_t* pairs;         /* 2 * total: seq_idx, pos_in_seq                    */
+} hfm_hits;
+
+/* One hit per SA interval of a MEM, as the reference GPU MemHit
+ * (src/gpu/mem_hit.rs:6-19, src/fm_index/bidir_index.rs:452-468).  Hits of one MEM
+ * are in ascending fwd_lo order; MEMs in ascending (query_start, query_end). */
+typedef struct hfm_mem_hit {
+  uint32_t query_start, query_end;
+  uint32_t match_count;    /* SA interval size                                  */
+  uint32_t truncated;      /* match_count > max_hits                            */
+  uint32_t fwd_lo;         /* forward SA interval start                         */
+  uint32_t n_pos;          /* positions resolved: min(match_count, max_hits), 0 without bounds */
+  uint64_t pos_off;        /* first (ref_id, offset) pair in positions          */
+} hfm_mem_hit;
+
+typedef struct hfm_mem_out {
+  uint32_t nq;
+  uint32_t _pad;
+  uint64_t n_hits, n_positions;
+  uint64_t* hit_offsets;   /* nq + 1                                            */
+  hfm_mem_hit* hits;       /* n_hits                                            */
+  uint32_t* positions;     /* 2 * n_positions: ref_id, offset_within_ref        */
+} hfm_mem_out;
+
+/* Per-call device timings and work counters of the last query on a handle. */
+typedef struct hfm_stats {
+  float ms_search, ms_resolve, ms_total;   /* CUDA-event times of the kernel phases */
+  uint32_t search_launches, resolve_launches, other_launches, fallback_reads;
+  uint64_t occ_touches, ssa_touches, lf_steps, rows_resolved;
+  uint64_t bytes_alg;                      /* algorithmic bytes of the search+resolve kernels */
+} hfm_stats;
+
+/* ---- index construction (replaces FmIndex::build_cpu_with + to_bytes,
+ *      src/fm_index/mod.rs:95-195, src/fm_index/bidir_index.rs:53-80,
+ *      src/fm_index/serialize.rs:13-26) ------------------------------------- */
+typedef struct hfm_build_opts {
+  uint32_t sa_sample_rate;   /* FmIndexConfig::sa_sample_rate (default 32)            */
+  uint32_t lookup_depth;     /* FmIndexConfig::lookup_depth (reverse index always 0)  */
+  uint32_t alphabet_tag;     /* 0 IupacDna, 1 ExactDna                                */
+  uint32_t occ_encoding;     /* 0 Bitplane, 1 OneHot                                  */
+  uint32_t threads;          /* host threads for construction (0 = all)               */
+} hfm_build_opts;
+
+/* codes: concatenated sequences (codes 1..15), seq_off[nseq+1]; headers: nseq C strings
+ * or NULL ("seq_{i}" defaults).  Writes malloc'd bincode bytes (free with hfm_free). */
+int hfm_build_index(const uint8_t* codes, const uint64_t* seq_off, uint32_t nseq,
+                    const char* const* headers, const hfm_build_opts* opts, int kind,
+                    uint8_t** bytes_out, size_t* len_out);
+
+/* ---- index load / free (replaces FmIndex::from_bytes / BidirFmIndex::from_bytes,
+ *      src/fm_index/serialize.rs:32-52, src/fm_index/bidir_index.rs:195-210, and the
+ *      per-call uploads of src/gpu/locate.rs:69-111, src/gpu/mem_find.rs:56-102,
+ *      src/gpu/mem_resolve.rs:44-85) ---------------------------------------- */
+int hfm_index_load(const uint8_t* bincode, size_t len, int kind, const hfm_opts* opts, hfm_index** out);
+void hfm_index_free(hfm_index* idx);
+int hfm_index_info_get(const hfm_index* idx, hfm_index_info* out);
+
+/* ---- queries, host buffers (the drop-in boundary) ------------------------ */
+
+/* FmIndex::count over a batch (src/fm_index/query.rs:9-14). */
+int hfm_count_batch(hfm_index* idx, const uint8_t* q, const uint64_t* q_off, uint32_t nq,
+                    uint32_t* counts_out);
+
+/* locate_batch_gpu (src/gpu/locate.rs:52-277) with the CPU semantics of
+ * FmIndex::locate (src/fm_index/query.rs:22-39, lookup seeding and unbounded IUPAC
+ * interval sets included).  max_hits > 0 keeps the first max_hits rows of every merged
+ * interval (an extension: the reference locate has no cap); 0 = all rows. */
+int hfm_locate_batch(hfm_index* idx, const uint8_t* q, const uint64_t* q_off, uint32_t nq,
+                     uint32_t max_hits, hfm_hits** out);
+
+/* BidirFmIndex::find_smems_gpu / find_mems_gpu (src/fm_index/bidir_index.rs:225-276,
+ * 391-514) with the CPU find_smems / find_mems semantics (src/fm_index/smem.rs:71-124).
+ * ref_bounds: exclusive end of each reference in the concatenated text (n_bounds = 0
+ * skips position resolution, as the reference does). */
+int hfm_mems_batch(hfm_index* idx, const uint8_t* q, const uint64_t* q_off, uint32_t nq,
+                   uint32_t min_len, uint32_t mode, const uint32_t* ref_bounds, uint32_t n_bounds,
+                   uint32_t max_hits, hfm_mem_out** out);
+
+/* ---- queries, device buffers (reads already resident in HBM) -------------
+ * Same semantics as above.  d_q / d_q_off are device pointers; results are written to
+ * device memory owned by the handle and stay valid until the next call on it. */
+typedef struct hfm_dev_hits {
+  uint32_t nq; uint32_t _pad; uint64_t total;
+  uint64_t* d_offsets; uint32_t* d_counts; uint32_t* d_pairs;
+} hfm_dev_hits;
+typedef struct hfm_dev_mems {
+  uint32_t nq; uint32_t _pad; uint64_t n_hits, n_positions;
+  uint64_t* d_hit_offsets; hfm_mem_hit* d_hits; uint32_t* d_positions;
+} hfm_dev_mems;
+
+int hfm_count_batch_device(hfm_index* idx, const uint8_t* d_q, const uint64_t* d_q_off, uint32_t nq,
+                           uint32_t* d_counts_out);
+int hfm_locate_batch_device(hfm_index* idx, const uint8_t* d_q, const uint64_t* d_q_off, uint32_t nq,
+                            uint32_t max_hits, hfm_dev_hits* out);
+int hfm_mems_batch_device(hfm_index* idx, const uint8_t* d_q, const uint64_t* d_q_off, uint32_t nq,
+                          uint32_t min_len, uint32_t mode, const uint32_t* ref_bounds, uint32_t n_bounds,
+                          uint32_t max_hits, hfm_dev_mems* out);
+
+/* ---- misc ----------------------------------------------------------------- */
+void hfm_free(void* p);                    /* frees hfm_hits*, hfm_mem_out*, build bytes */
+const char* hfm_last_error(void);          /* thread-local message of the last failure   */
+void* hfm_index_stream(hfm_index* idx);    /* the handle's cudaStream_t (for event timing) */
+int hfm_last_stats(const hfm_index* idx, hfm_stats* out);
+int hfm_set_counters(hfm_index* idx, int enable);  /* per-read work counters on/off (default off) */
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HFM_H */

@@ -1,0 +1,97 @@
+"""CPU-side checks of the C ABI: the library loads, exports every declared symbol, the
+native index builder reproduces the oracle's bytes, and malformed bincode is rejected
+before any device work (so these run without a GPU)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import random
+import re
+
+import numpy as np
+import pytest
+
+from haystackfm_b200 import _lib as L
+from haystackfm_b200 import alphabet as al
+from haystackfm_b200.errors import HFM_E_FORMAT, HFM_E_ARG
+from haystackfm_b200.fm_index import FmIndexConfig, _build, KIND_FM, KIND_BIDIR
+from tests.helpers import concat, seqs_codes
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "hfm.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(hfm_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = L.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(lib, s), s
+    assert set(syms) <= set(L.SIGNATURES), set(syms) - set(L.SIGNATURES)
+
+
+def _seqs(rng, n, alphabet, lo, hi):
+    return ["".join(rng.choice(alphabet) for _ in range(rng.randint(lo, hi))) for _ in range(n)]
+
+
+def product_bytes(seqs, rate=32, lookup=0, tag=0, enc=0, kind=0):
+    sq = [al.DnaSequence(c) for c in seqs_codes(seqs)]
+    return _build(sq, FmIndexConfig(sa_sample_rate=rate, lookup_depth=lookup, occ_encoding=enc, build_threads=2),
+                  tag, kind)
+
+
+def test_builder_matches_oracle_bytes(oracle):
+    rng = random.Random(5)
+    cases = [(["ACGT"], 1, 0, 0, 0, 0), (["ACGTNACGT"], 4, 3, 1, 0, 0), (["ACGT", "TGCA"], 2, 0, 0, 1, 1)]
+    for _ in range(40):
+        seqs = _seqs(rng, rng.randint(1, 4), rng.choice(["ACGT", "ACGTN", "ACGTNRYSWKMBDHV"]), 1, 300)
+        cases.append((seqs, rng.choice([1, 2, 7, 32]), rng.choice([0, 0, 2, 4]), rng.choice([0, 1]),
+                      rng.choice([0, 1]), rng.choice([0, 1])))
+    for seqs, rate, lookup, tag, enc, kind in cases:
+        want = oracle.build_index_bytes(seqs_codes(seqs), rate=rate, lookup_depth=lookup if kind == 0 or True else 0,
+                                        tag=tag, encoding=enc, kind=kind)
+        got = product_bytes(seqs, rate, lookup, tag, enc, kind)
+        assert got == want, (seqs, rate, lookup, tag, enc, kind)
+
+
+def test_suffix_array_matches_naive(oracle):
+    rng = random.Random(9)
+    lib = L.lib()
+    for _ in range(60):
+        seqs = _seqs(rng, rng.randint(1, 5), rng.choice(["A", "AC", "ACGT", "ACGTN"]), 1, 400)
+        text, _ = concat(seqs)
+        want = oracle.suffix_array(text)
+        got = np.zeros(len(text), dtype=np.uint32)
+        t = np.ascontiguousarray(text, dtype=np.uint8)
+        assert lib.hfm_suffix_array(L.ptr(t, L.u8p), len(t), L.ptr(got, L.u32p)) == 0
+        assert np.array_equal(got, want)
+
+
+def _load_status(data: bytes, kind: int):
+    buf = np.frombuffer(data, dtype=np.uint8).copy() if data else np.zeros(1, np.uint8)
+    h = C.c_void_p()
+    return L.lib().hfm_index_load(L.ptr(buf, L.u8p), len(data), kind, None, C.byref(h))
+
+
+def test_malformed_bincode_rejected_before_device_work():
+    good = product_bytes(["ACGTACGT"], rate=4)
+    assert _load_status(good[:-1] + b"\xff", KIND_FM) == HFM_E_FORMAT       # unknown alphabet tag
+    assert _load_status(good[:50], KIND_FM) == HFM_E_FORMAT                 # truncated
+    bad_c = bytearray(good); bad_c[4] ^= 1                                   # C array inconsistent
+    assert _load_status(bytes(bad_c), KIND_FM) == HFM_E_FORMAT
+    bidir = product_bytes(["ACGT", "TTGA"], kind=1)
+    assert _load_status(bidir[:3], KIND_BIDIR) == HFM_E_FORMAT
+    assert _load_status(bidir[:200], KIND_BIDIR) == HFM_E_FORMAT
+    assert _load_status(good, 7) == HFM_E_ARG
+
+
+def test_build_rejects_bad_input():
+    with pytest.raises(Exception):
+        _build([], FmIndexConfig(), 0, KIND_FM)
+    with pytest.raises(Exception):
+        _build([al.DnaSequence(np.array([1, 0, 2], np.uint8))], FmIndexConfig(), 0, KIND_FM)
