@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""SMEM+locate reads/s on one B200 — the IUPAC batch locate + SMEM workload.
+
+Workload (one step): 1,000,000 reads of 150 bp against a 100 Mbp synthetic reference of
+200 contigs (lognormal lengths mu=13 sigma=1; uniform ACGT, N runs over 2% with geometric
+lengths of mean 500, 0.5% single ambiguity codes); reads from either strand with 1%
+substitutions and 0.1% N; IupacDna, sa_sample_rate 32, lookup_depth 10.  Per read: locate
+of its first 32-mer (max 1024 positions per merged interval) and find_smems with
+min_len 19 and max_hits_per_mem 1024, positions mapped to the reference boundaries.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--reads R]
+
+`value` is device-resident throughput (reads in HBM before the timed region, results left
+in HBM); `e2e` goes through the C ABI with host buffers (H2D of the reads from pinned
+memory and D2H of every result inside the timed region).  --impl reference times the
+CPU restatement of the reference path on the host cores (the Rust reference cannot be
+built here).  Multi-GPU: one process per GPU, each with its own index replica and its own
+1M reads (weak scaling, no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import hashlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SMEM+locate reads/s on 1 B200, learned-binned vs plain (bit-exact); p99 latency"
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--reads", type=int, default=1_000_000)
+    ap.add_argument("--ref-len", type=int, default=100_000_000)
+    ap.add_argument("--contigs", type=int, default=200)
+    ap.add_argument("--e2e-chunk", type=int, default=250_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    return ap.parse_args()
+
+
+def workload(args, rank=0):
+    from haystackfm_b200 import alphabet as al, synth
+    from haystackfm_b200.fm_index import FmIndexConfig, KIND_BIDIR, _build
+    key = hashlib.sha1(f"iupac-v1-{args.ref_len}-{args.contigs}-2-rate32-lut10".encode()).hexdigest()[:16]
+    cache_dir = os.path.join(tempfile.gettempdir(), "hfm_bench_cache")
+    os.makedirs(cache_dir, exist_ok=True)
+    path = os.path.join(cache_dir, key + ".bin")
+    ref = synth.iupac_reference(total=args.ref_len, n_contigs=args.contigs, seed=2)
+    t0 = time.time()
+    if os.path.exists(path):
+        data = open(path, "rb").read()
+        built = False
+    else:
+        data = _build([al.DnaSequence(c) for c in ref.contigs],
+                      FmIndexConfig(sa_sample_rate=32, lookup_depth=10, build_threads=2), 0, KIND_BIDIR)
+        tmp = path + f".{os.getpid()}"
+        with open(tmp, "wb") as f:
+            f.write(data)
+        os.replace(tmp, path)
+        built = True
+    build_s = time.time() - t0
+    reads = synth.sample_reads(ref, n_reads=args.reads, seed=3 + rank)
+    return ref, data, reads, build_s, built
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.f = None
+
+    def start(self):
+        try:
+            self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, nm in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_reference(args, data, reads, bounds, seconds, threads):
+    """Oracle (C++ restatement of the reference CPU path) on a bounded read sample."""
+    from haystackfm_b200 import synth
+    from oracle import oracle as orc
+    orc.build()
+    o = orc.OracleIndex(data, 1)
+    n = 256
+    while True:
+        sub = reads[:n]
+        t0 = time.perf_counter()
+        f32, o32 = synth.pack_rows(sub, 32)
+        o.locate_packed(f32, o32, 1024, threads)
+        fr, orr = synth.pack_rows(sub)
+        o.mems_packed(fr, orr, 19, 0, bounds, 1024, threads)
+        dt = time.perf_counter() - t0
+        if dt >= seconds * 0.5 or n >= len(reads):
+            return n / dt, n, dt
+        n = min(len(reads), int(n * max(2.0, seconds * 0.6 / max(dt, 1e-3))))
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    _, data, reads, _, _ = workload(args)
+    from haystackfm_b200.fm_index import _header_fields
+    bounds = _header_fields(data, 4)[2]
+    threads = os.cpu_count() or 1
+    per_step = max(2.0, args.cpu_seconds / max(1, args.steps))
+    for _ in range(args.warmup):
+        cpu_reference(args, data, reads, bounds, per_step / 4, threads)
+    vals = []
+    for _ in range(args.steps):
+        v, n, dt = cpu_reference(args, data, reads, bounds, per_step, threads)
+        vals.append((v, n, dt))
+    tot_n = sum(x[1] for x in vals)
+    tot_t = sum(x[2] for x in vals)
+    value = tot_n / tot_t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * tot_t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
+        "config": {"workload": "iupac_batch_locate_smem", "reads_per_step": args.reads, "read_len": 150,
+                   "ref_len": args.ref_len, "contigs": args.contigs, "sa_sample_rate": 32, "lookup_depth": 10,
+                   "min_len": 19, "max_hits_per_mem": 1024, "locate_kmer": 32, "path": "cpu_reference"},
+        "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads, "kind": "port",
+                         "sample": f"{vals[-1][1]} reads of the 1M-read workload per step, oracle/hfm_oracle.cpp "
+                                   f"(Rust reference not buildable here), {threads} threads"},
+        "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(minutes=20),
+                                device_id=torch.device("cuda", local))
+    from haystackfm_b200 import synth
+    from haystackfm_b200.fm_index import BidirFmIndex
+
+    if dist and rank != 0:
+        dist.barrier()          # rank 0 builds (or finds) the cached index first
+    ref, data, reads, build_s, built = workload(args, rank)
+    if dist and rank == 0:
+        dist.barrier()
+    idx = BidirFmIndex.from_bytes(data, device=local)
+    h = idx.handle
+    lib = __import__("haystackfm_b200._lib", fromlist=["lib"]).lib()
+    from haystackfm_b200 import _lib as L
+    bounds = np.ascontiguousarray(idx.seq_boundaries(), dtype=np.uint32)
+    nb = len(bounds)
+    n = args.reads
+
+    # device-resident inputs
+    dev = torch.device("cuda", local)
+    reads_d = torch.from_numpy(reads.reshape(-1)).to(dev)
+    off_d = torch.arange(0, (n + 1) * 150, 150, dtype=torch.int64, device=dev)
+    k32_d = torch.from_numpy(np.ascontiguousarray(reads[:, :32]).reshape(-1)).to(dev)
+    off32_d = torch.arange(0, (n + 1) * 32, 32, dtype=torch.int64, device=dev)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(h.stream(), device=dev)
+
+    def step(stats_out=None):
+        dh = L.HfmDevHits()
+        L.check(lib.hfm_locate_batch_device(h.h, k32_d.data_ptr(), off32_d.data_ptr(), n, 1024, C.byref(dh)))
+        s1 = h.stats()
+        dm = L.HfmDevMems()
+        L.check(lib.hfm_mems_batch_device(h.h, reads_d.data_ptr(), off_d.data_ptr(), n, 19, 0,
+                                          L.ptr(bounds, L.u32p), nb, 1024, C.byref(dm)))
+        s2 = h.stats()
+        if stats_out is not None:
+            stats_out.append((s1, s2, dh.total, dm.n_hits, dm.n_positions))
+
+    # work counters (one untimed pass): algorithmic bytes per launch
+    h.set_counters(True)
+    cnt = []
+    step(cnt)
+    h.set_counters(False)
+    c_loc, c_mem, loc_total, n_hits, n_pos = cnt[0]
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    per = []
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(per)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    if dist:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n * args.steps / (ms / 1000.0)
+    launches = sum(s1.search_launches + s1.resolve_launches + s1.other_launches + s2.search_launches +
+                   s2.resolve_launches + s2.other_launches for s1, s2, *_ in per)
+    # kernel times (CUDA events around each launch, recorded by the library on its stream)
+    k_mems_ms = statistics.mean(s2.ms_search_kernel for _, s2, *_ in per)
+    k_res_mem_ms = statistics.mean(s2.ms_resolve_kernel for _, s2, *_ in per)
+    k_bs_ms = statistics.mean(s1.ms_search_kernel for s1, *_ in per)
+    k_res_loc_ms = statistics.mean(s1.ms_resolve_kernel for s1, *_ in per)
+    # algorithmic bytes (32 B per random Occ / SA-marker / sa_vals / lookup touch, read bytes,
+    # 8 B per output position, 16 B per MEM hit header)
+    b_mems = 32 * c_mem.occ_touches + 150 * n + 16 * c_mem.hits_out
+    b_res_mem = 32 * (2 * c_mem.lf_calls + c_mem.rows_resolved) + 8 * c_mem.rows_resolved
+    b_bs = 32 * c_loc.occ_touches + 32 * n
+    b_res_loc = 32 * (2 * c_loc.lf_calls + c_loc.rows_resolved) + 8 * c_loc.rows_resolved
+    kern = {"k_mems": (k_mems_ms, b_mems, c_mem.occ_touches, "Occ touches"),
+            "k_resolve(smem)": (k_res_mem_ms, b_res_mem, c_mem.lf_calls, "LF steps"),
+            "k_bsearch": (k_bs_ms, b_bs, c_loc.occ_touches, "Occ touches"),
+            "k_resolve(locate)": (k_res_loc_ms, b_res_loc, c_loc.lf_calls, "LF steps")}
+    dom = max(kern, key=lambda k: kern[k][0])
+    kms, kbytes, units, unit_name = kern[dom]
+    try:
+        peaks = json.load(open(MEASURED_PEAKS))
+        peak, peak_src = float(peaks["hbm_gbs"]), "measured"
+    except Exception:
+        peak, peak_src = FALLBACK_HBM_GBS, "fallback"
+    achieved = kbytes / (kms / 1000.0) / 1e9 if kms > 0 else 0.0
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_per_unit.json")
+    if os.path.exists(tpath):
+        tj = json.load(open(tpath))
+        if dom in tj:
+            traffic = tj[dom]["dram_bytes_per_unit"] * units
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                "kernel_ms": kms, "alg_bytes": kbytes, "units": units, "unit_name": unit_name,
+                "kernels_ms": {k: v[0] for k, v in kern.items()},
+                "kernels_gbs": {k: (v[1] / (v[0] / 1000) / 1e9 if v[0] > 0 else None) for k, v in kern.items()}}
+
+    # end to end through the host-buffer C ABI (pinned reads in, every result out)
+    reads_pin = torch.empty(n * 150, dtype=torch.uint8, pin_memory=True)
+    reads_pin.numpy()[:] = reads.reshape(-1)
+    k32_pin = torch.empty(n * 32, dtype=torch.uint8, pin_memory=True)
+    k32_pin.numpy()[:] = np.ascontiguousarray(reads[:, :32]).reshape(-1)
+    rp, kp = reads_pin.numpy(), k32_pin.numpy()
+    ch = min(args.e2e_chunk, n)
+
+    def e2e_step():
+        h2d = d2h = 0
+        for a in range(0, n, ch):
+            b = min(n, a + ch)
+            m = b - a
+            off150 = np.arange(0, (m + 1) * 150, 150, dtype=np.uint64)
+            off32 = np.arange(0, (m + 1) * 32, 32, dtype=np.uint64)
+            res = C.POINTER(L.HfmHits)()
+            L.check(lib.hfm_locate_batch(h.h, L.ptr(kp[a * 32:], L.u8p), L.ptr(off32, L.u64p), m, 1024, C.byref(res)))
+            d2h += (m + 1) * 8 + m * 4 + res.contents.total * 8
+            lib.hfm_free(res)
+            mo = C.POINTER(L.HfmMemOut)()
+            L.check(lib.hfm_mems_batch(h.h, L.ptr(rp[a * 150:], L.u8p), L.ptr(off150, L.u64p), m, 19, 0,
+                                       L.ptr(bounds, L.u32p), nb, 1024, C.byref(mo)))
+            d2h += (m + 1) * 8 + mo.contents.n_hits * 32 + mo.contents.n_positions * 8
+            lib.hfm_free(mo)
+            h2d += m * 32 + (m + 1) * 8 + m * 150 + (m + 1) * 8 + nb * 4
+        return h2d, d2h
+
+    e2e_step()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        h2d, d2h = e2e_step()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * n * args.steps / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": int(h2d),
+           "d2h_bytes_per_step": int(d2h), "chunk_reads": ch}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, ns, dt = cpu_reference(args, data, reads, bounds, args.cpu_seconds, threads)
+        cpu = {"value": v, "unit": "reads/s", "cores": threads, "kind": "port",
+               "sample": f"first {ns} reads of the workload ({dt:.1f} s): locate of the 32-mer + find_smems, "
+                         f"oracle/hfm_oracle.cpp, {threads} threads"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generators, haystackfm_b200/synth.py)",
+            "config": {"workload": "iupac_batch_locate_smem", "reads_per_step_per_gpu": n, "read_len": 150,
+                       "ref_len": args.ref_len, "contigs": args.contigs, "sa_sample_rate": 32, "lookup_depth": 10,
+                       "min_len": 19, "max_hits_per_mem": 1024, "locate_kmer": 32, "path": "plain",
+                       "l2": "no flush: index (0.7 GB device layout) + reads (150 MB) + outputs exceed the 126 MB L2",
+                       "index_build_s": round(build_s, 1), "index_cached": not built,
+                       "locate_positions": int(loc_total), "mem_hits": int(n_hits), "mem_positions": int(n_pos),
+                       "parallelism": f"replicas{world}" if world > 1 else "single"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -59,10 +59,11 @@ class HfmDevMems(C.Structure):
 
 class HfmStats(C.Structure):
     _fields_ = [("ms_search", C.c_float), ("ms_resolve", C.c_float), ("ms_total", C.c_float),
+                ("ms_search_kernel", C.c_float), ("ms_resolve_kernel", C.c_float),
                 ("search_launches", C.c_uint32), ("resolve_launches", C.c_uint32),
                 ("other_launches", C.c_uint32), ("fallback_reads", C.c_uint32),
-                ("occ_touches", C.c_uint64), ("ssa_touches", C.c_uint64), ("lf_steps", C.c_uint64),
-                ("rows_resolved", C.c_uint64), ("bytes_alg", C.c_uint64)]
+                ("occ_touches", C.c_uint64), ("lf_calls", C.c_uint64), ("rows_resolved", C.c_uint64),
+                ("hits_out", C.c_uint64)]
 
 
 class HfmBuildOpts(C.Structure):

@@ -111,6 +111,8 @@ struct hfm_index {
   uint64_t iv_cap = 0, hit_cap = 0;
   Counters* h_ctr = nullptr;        // pinned
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t evk[4] = {nullptr, nullptr, nullptr, nullptr};   // main search kernel, resolve kernel
+  bool k_search_rec = false, k_resolve_rec = false;
   hfm_stats stats{};
 };
 
@@ -246,8 +248,11 @@ static int run_bsearch(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
             x->status.as<uint32_t>(), x->ovf.as<uint32_t>(), &dctr(x)->n_ovf, &dctr(x)->touches};
     if (nq) {
       unsigned grid = (nq + 255) / 256;
+      cudaEventRecord(x->evk[0], x->stream);
       if (x->count_work) k_bsearch<BS_K, true><<<grid, 256, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, nq, cap, pool, o);
       else k_bsearch<BS_K, false><<<grid, 256, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, nq, cap, pool, o);
+      cudaEventRecord(x->evk[1], x->stream);
+      x->k_search_rec = true;
       launches++;
       CK(cudaGetLastError());
     }
@@ -294,8 +299,11 @@ static int resolve(hfm_index* x, const FmDev& F, const uint32_t* seg_row, uint32
                 F.rate ? F.rate : F.text_len, out, &dctr(x)->walk_err, &dctr(x)->steps};
   uint64_t blocks = (total + RES_T - 1) / RES_T;
   // grid.x limit 2^31-1 blocks covers 5e11 positions
+  cudaEventRecord(x->evk[2], x->stream);
   if (x->count_work) k_resolve<true><<<(unsigned)blocks, RES_T, 0, x->stream>>>(F.d, A);
   else k_resolve<false><<<(unsigned)blocks, RES_T, 0, x->stream>>>(F.d, A);
+  cudaEventRecord(x->evk[3], x->stream);
+  x->k_resolve_rec = true;
   launches++;
   CK(cudaGetLastError());
   return HFM_OK;
@@ -303,6 +311,7 @@ static int resolve(hfm_index* x, const FmDev& F, const uint32_t* seg_row, uint32
 
 static void begin_stats(hfm_index* x) {
   x->stats = hfm_stats{};
+  x->k_search_rec = x->k_resolve_rec = false;
   cudaEventRecord(x->ev[0], x->stream);
 }
 static void end_stats(hfm_index* x) {
@@ -312,6 +321,10 @@ static void end_stats(hfm_index* x) {
   cudaEventElapsedTime(&a, x->ev[0], x->ev[1]);
   cudaEventElapsedTime(&b, x->ev[1], x->ev[2]);
   x->stats.ms_search = a; x->stats.ms_resolve = b; x->stats.ms_total = a + b;
+  float ks = 0, kr = 0;
+  if (x->k_search_rec) cudaEventElapsedTime(&ks, x->evk[0], x->evk[1]);
+  if (x->k_resolve_rec) cudaEventElapsedTime(&kr, x->evk[2], x->evk[3]);
+  x->stats.ms_search_kernel = ks; x->stats.ms_resolve_kernel = kr;
 }
 
 // ---------------------------------------------------------------------------
@@ -359,7 +372,7 @@ static int locate_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qof
   RET(read_ctr(x));
   end_stats(x);
   x->stats.search_launches = launches; x->stats.resolve_launches = rl; x->stats.other_launches = other;
-  x->stats.rows_resolved = total; x->stats.lf_steps = x->h_ctr->steps;
+  x->stats.rows_resolved = total; x->stats.lf_calls = x->h_ctr->steps;
   if (x->h_ctr->walk_err) return set_error(HFM_E_WALK, "LF walk exceeded sample_rate steps: index inconsistent");
   out->nq = nq; out->total = total;
   out->d_offsets = x->pos_base.as<uint64_t>(); out->d_counts = x->counts.as<uint32_t>();
@@ -391,8 +404,11 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
               x->ovf.as<uint32_t>(), &dctr(x)->n_ovf, &dctr(x)->touches};
     if (nq) {
       unsigned grid = (nq + 127) / 128;
+      cudaEventRecord(x->evk[0], x->stream);
       if (x->count_work) k_mems<MEM_K, MEM_KC, true><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, nq, P, ivp, hp, o);
       else k_mems<MEM_K, MEM_KC, false><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, nq, P, ivp, hp, o);
+      cudaEventRecord(x->evk[1], x->stream);
+      x->k_search_rec = true;
       launches++;
       CK(cudaGetLastError());
     }
@@ -456,7 +472,7 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   RET(read_ctr(x));
   end_stats(x);
   x->stats.search_launches = launches; x->stats.resolve_launches = rl; x->stats.other_launches = other;
-  x->stats.rows_resolved = npos; x->stats.lf_steps = x->h_ctr->steps;
+  x->stats.rows_resolved = npos; x->stats.lf_calls = x->h_ctr->steps; x->stats.hits_out = nh;
   if (x->h_ctr->walk_err) return set_error(HFM_E_WALK, "LF walk exceeded sample_rate steps: index inconsistent");
   out->nq = nq; out->n_hits = nh; out->n_positions = npos;
   out->d_hit_offsets = x->hit_base.as<uint64_t>(); out->d_hits = x->hits.as<hfm_mem_hit>();
@@ -518,6 +534,7 @@ int hfm_index_load(const uint8_t* bytes, size_t len, int kind, const hfm_opts* o
   x->device = dev; x->kind = kind;
   CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
   for (auto& e : x->ev) CK(cudaEventCreate(&e));
+  for (auto& e : x->evk) CK(cudaEventCreate(&e));
   CK(cudaMallocHost((void**)&x->h_ctr, sizeof(Counters)));
   RET(x->ctr.ensure(sizeof(Counters)));
   RET(build_device_fm(hf, x->fwd, x->stream));
@@ -538,6 +555,7 @@ void hfm_index_free(hfm_index* x) {
                     &x->hit_base, &x->hits, &x->npos_scan, &x->work, &x->cwork, &x->ctr})
     b->release();
   for (auto& e : x->ev) if (e) cudaEventDestroy(e);
+  for (auto& e : x->evk) if (e) cudaEventDestroy(e);
   if (x->h_ctr) cudaFreeHost(x->h_ctr);
   if (x->stream) cudaStreamDestroy(x->stream);
   delete x;

@@ -84,8 +84,9 @@ def _build(sequences: Sequence[DnaSequence], config: FmIndexConfig, tag: int, ki
     codes = [s.as_slice() for s in sequences]
     flat, off = L.pack_queries(codes)
     hdr = (C.c_char_p * len(sequences))(*[s.header().encode() for s in sequences])
+    # build_threads 0 or 1 -> single-threaded, as FmIndexConfig::build_threads (src/fm_index/mod.rs:33-36)
     opts = L.HfmBuildOpts(config.sa_sample_rate, config.lookup_depth, tag, config.occ_encoding,
-                          max(0, int(config.build_threads)) if config.build_threads > 1 else 1)
+                          max(1, int(config.build_threads)))
     out = L.u8p()
     n = C.c_size_t()
     L.check(L.lib().hfm_build_index(L.ptr(flat, L.u8p), L.ptr(off, L.u64p), len(sequences), hdr, C.byref(opts),

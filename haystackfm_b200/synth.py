@@ -61,10 +61,11 @@ def iupac_reference(total=100_000_000, n_contigs=200, n_frac=0.02, n_run_mean=50
     starts = rng.integers(0, total, size=len(run_len))
     for s, l in zip(starts, run_len):
         masked[s:s + l] = N
-    # single ambiguity codes R..V (6..15) at uniform positions
+    # single ambiguity codes R..V (6..15) at uniform positions outside the N runs
     k = int(total * iupac_frac)
-    pos = rng.integers(0, total, size=k)
-    masked[pos] = rng.integers(6, 16, size=k, dtype=np.uint8)
+    free = np.flatnonzero(masked != N)
+    pos = free[rng.choice(len(free), size=min(k, len(free)), replace=False)] if k else free[:0]
+    masked[pos] = rng.integers(6, 16, size=len(pos), dtype=np.uint8)
     bounds = np.concatenate([[0], np.cumsum(lens)])
     contigs = [masked[bounds[i]:bounds[i + 1]] for i in range(n_contigs)]
     truth = [truth_all[bounds[i]:bounds[i + 1]] for i in range(n_contigs)]

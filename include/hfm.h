@@ -83,12 +83,18 @@ typedef struct hfm_mem_out {
   uint32_t* positions;     /* 2 * n_positions: ref_id, offset_within_ref        */
 } hfm_mem_out;
 
-/* Per-call device timings and work counters of the last query on a handle. */
+/* Per-call device timings and work counters of the last query on a handle.  Times are
+ * CUDA events recorded on the handle's stream around the phases and around the main
+ * search kernel and the resolve kernel alone.  Work counters are filled only while
+ * hfm_set_counters(idx, 1) is on (they slow the kernels). */
 typedef struct hfm_stats {
-  float ms_search, ms_resolve, ms_total;   /* CUDA-event times of the kernel phases */
+  float ms_search, ms_resolve, ms_total;
+  float ms_search_kernel, ms_resolve_kernel;
   uint32_t search_launches, resolve_launches, other_launches, fallback_reads;
-  uint64_t occ_touches, ssa_touches, lf_steps, rows_resolved;
-  uint64_t bytes_alg;                      /* algorithmic bytes of the search+resolve kernels */
+  uint64_t occ_touches;      /* Occ record touches of the search kernels (incl. lookup reads) */
+  uint64_t lf_calls;         /* LF-walk iterations of the resolve kernel (Occ + SA-marker touch each) */
+  uint64_t rows_resolved;    /* positions resolved (one sa_vals read and one output pair each) */
+  uint64_t hits_out;         /* MEM hit records written                                   */
 } hfm_stats;
 
 /* ---- index construction (replaces FmIndex::build_cpu_with + to_bytes,
