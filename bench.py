@@ -276,6 +276,12 @@ def main():
             "k_resolve(smem)": (k_res_mem_ms, b_res_mem, c_mem.lf_calls, "LF steps"),
             "k_bsearch": (k_bs_ms, b_bs, c_loc.occ_touches, "Occ touches"),
             "k_resolve(locate)": (k_res_loc_ms, b_res_loc, c_loc.lf_calls, "LF steps")}
+    for k, v in kern.items():
+        print(f"[bench] {k}: {v[0]:.3f} ms/launch, alg {v[1] / 1e9:.3f} GB, {v[2]} {v[3]}", file=sys.stderr)
+    s1, s2 = per[-1][0], per[-1][1]
+    print(f"[bench] locate phases {s1.ms_search:.2f}+{s1.ms_resolve:.2f} ms, mems phases {s2.ms_search:.2f}+"
+          f"{s2.ms_resolve:.2f} ms, fallback reads {s1.fallback_reads}/{s2.fallback_reads}, step {ms / args.steps:.1f} ms",
+          file=sys.stderr)
     dom = max(kern, key=lambda k: kern[k][0])
     kms, kbytes, units, unit_name = kern[dom]
     try:

@@ -84,7 +84,7 @@ struct DevBuf {
 
 struct Counters {                    // device-side counters, one block per handle
   unsigned long long iv_used, hit_used, touches, steps;
-  uint32_t n_ovf, still_ovf, walk_err, _pad;
+  uint32_t n_ovf, still_ovf, walk_err, queue, queue2, _pad[3];
 };
 
 struct FmDev {
@@ -107,8 +107,10 @@ struct hfm_index {
   bool count_work = false;
   // per-call work buffers (grow-only)
   DevBuf q, qoff, counts, nhits, niv, ivoff, status, ovf, ivpool, hitpool, seg_row, seg_off, pos_base, seg_base,
-      scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr;
-  uint64_t iv_cap = 0, hit_cap = 0;
+      scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr,
+      mivpool, bswork, memwork;
+  int num_sms = 0;
+  uint64_t iv_cap = 0, miv_cap = 0, hit_cap = 0;   // pool capacities in elements (uint2 / BIv / hit)
   Counters* h_ctr = nullptr;        // pinned
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t evk[4] = {nullptr, nullptr, nullptr, nullptr};   // main search kernel, resolve kernel
@@ -225,9 +227,9 @@ static int read_u64(hfm_index* x, const uint64_t* dsrc, uint64_t& v) {
   return HFM_OK;
 }
 
-static constexpr int BS_K = 16;        // fast-path interval-set capacity (backward search)
-static constexpr int MEM_K = 32;       // fast-path interval-set capacity (SMEM / MEM)
-static constexpr int MEM_KC = 32;      // fast-path candidate capacity
+static constexpr uint32_t BS_SET_CAP = 256;    // fast-path interval-set capacity (backward search)
+static constexpr uint32_t MEM_SET_CAP = 768;   // fast-path interval-set capacity (SMEM / MEM)
+static constexpr int MEM_KC = 32;              // fast-path candidate capacity (thread-local)
 
 // Backward search for a batch.  with_ivs = false: counts only.
 static int run_bsearch(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t cap,
@@ -241,16 +243,28 @@ static int run_bsearch(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
     RET(x->ivpool.ensure(x->iv_cap * 8));
     x->iv_cap = x->ivpool.cap / 8;
   }
+  // persistent fast pass: one wave of resident threads, BS_SET_CAP intervals per set
+  int bpsm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_bsearch<false, 32>, 256, 0));
+  uint64_t threads = (uint64_t)std::max(1, bpsm) * x->num_sms * 256;
+  threads = std::min<uint64_t>(threads, ((uint64_t)nq + 255) / 256 * 256);
+  RET(x->bswork.ensure(std::max<uint64_t>(threads, 32) * 2 * BS_SET_CAP * 8));
   for (int attempt = 0; attempt < 8; attempt++) {
     CK(cudaMemsetAsync(x->ctr.p, 0, sizeof(Counters), x->stream));
     Pool pool{x->ivpool.p, &dctr(x)->iv_used, x->iv_cap};
     BsOut o{d_counts, with_ivs ? x->nhits.as<uint64_t>() : nullptr, x->niv.as<uint32_t>(), x->ivoff.as<uint64_t>(),
             x->status.as<uint32_t>(), x->ovf.as<uint32_t>(), &dctr(x)->n_ovf, &dctr(x)->touches};
     if (nq) {
-      unsigned grid = (nq + 255) / 256;
+      unsigned grid = (unsigned)(threads / 256);
       cudaEventRecord(x->evk[0], x->stream);
-      if (x->count_work) k_bsearch<BS_K, true><<<grid, 256, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, nq, cap, pool, o);
-      else k_bsearch<BS_K, false><<<grid, 256, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, nq, cap, pool, o);
+      if (x->count_work)
+        k_bsearch<true, 32><<<grid, 256, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, nullptr, nq, cap,
+                                                        x->bswork.as<uint2>(), BS_SET_CAP, &dctr(x)->queue, pool, o,
+                                                        &dctr(x)->still_ovf);
+      else
+        k_bsearch<false, 32><<<grid, 256, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, nullptr, nq, cap,
+                                                         x->bswork.as<uint2>(), BS_SET_CAP, &dctr(x)->queue, pool, o,
+                                                         &dctr(x)->still_ovf);
       cudaEventRecord(x->evk[1], x->stream);
       x->k_search_rec = true;
       launches++;
@@ -259,19 +273,27 @@ static int run_bsearch(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
     RET(read_ctr(x));
     uint32_t n_ovf = x->h_ctr->n_ovf;
     if (n_ovf) {
-      // fallback: large global-memory sets, doubling until every query fits
-      uint32_t set_cap = 4096;
+      // fallback pass over the overflowed queries: contiguous per-thread sets, 16x larger,
+      // growing 4x until every query fits
+      uint32_t set_cap = BS_SET_CAP * 16;
       while (true) {
-        uint32_t per = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n_ovf, (1ull << 30) / ((uint64_t)set_cap * 16)));
-        RET(x->work.ensure((size_t)per * set_cap * 16));
+        uint64_t per_thread = (uint64_t)set_cap * 2 * 8;
+        uint32_t nthr = (uint32_t)std::max<uint64_t>(32, std::min<uint64_t>((uint64_t)n_ovf, (2ull << 30) / per_thread));
+        nthr = std::min<uint32_t>((nthr + 31) / 32 * 32, (uint32_t)threads);
+        RET(x->work.ensure((size_t)nthr * per_thread));
         CK(cudaMemsetAsync(&dctr(x)->still_ovf, 0, 4, x->stream));
-        for (uint32_t b = 0; b < n_ovf; b += per) {
-          uint32_t cnt = std::min(per, n_ovf - b);
-          if (x->count_work) k_bsearch_big<true><<<(cnt + 127) / 128, 128, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>() + b, cnt, cap, x->work.as<uint2>(), set_cap, pool, o, &dctr(x)->still_ovf);
-          else k_bsearch_big<false><<<(cnt + 127) / 128, 128, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>() + b, cnt, cap, x->work.as<uint2>(), set_cap, pool, o, &dctr(x)->still_ovf);
-          launches++;
-          CK(cudaGetLastError());
-        }
+        CK(cudaMemsetAsync(&dctr(x)->queue2, 0, 4, x->stream));
+        unsigned grid = (nthr + 127) / 128;
+        if (x->count_work)
+          k_bsearch<true, 1><<<grid, 128, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>(),
+                                                         n_ovf, cap, x->work.as<uint2>(), set_cap, &dctr(x)->queue2, pool,
+                                                         o, &dctr(x)->still_ovf);
+        else
+          k_bsearch<false, 1><<<grid, 128, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>(),
+                                                          n_ovf, cap, x->work.as<uint2>(), set_cap, &dctr(x)->queue2, pool,
+                                                          o, &dctr(x)->still_ovf);
+        launches++;
+        CK(cudaGetLastError());
         RET(read_ctr(x));
         x->stats.fallback_reads += n_ovf;
         if (x->h_ctr->still_ovf == 0) break;
@@ -390,23 +412,34 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   if (nb) CK(cudaMemcpyAsync(x->ref_bounds.p, h_bounds, (size_t)nb * 4, cudaMemcpyHostToDevice, x->stream));
   RET(x->hit_start.ensure((size_t)nq * 8 + 8)); RET(x->hit_count.ensure((size_t)nq * 4 + 4));
   RET(x->status.ensure((size_t)nq * 4 + 4)); RET(x->ovf.ensure((size_t)nq * 4 + 4));
-  if (x->iv_cap < (uint64_t)nq * 24 + 4096) x->iv_cap = (uint64_t)nq * 24 + 4096;     // BIv = 16 B
+  if (x->miv_cap < (uint64_t)nq * 24 + 4096) x->miv_cap = (uint64_t)nq * 24 + 4096;     // BIv = 16 B
   if (x->hit_cap < (uint64_t)nq * 24 + 4096) x->hit_cap = (uint64_t)nq * 24 + 4096;   // hit = 32 B
   MemsParams P{min_len, mode, cap, nb ? 1u : 0u};
   const FmDev& Fw = x->fwd; const FmDev& Rv = x->rev;
+  // persistent fast pass: one wave of resident threads, MEM_SET_CAP intervals per set
+  int bpsm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC>, 128, 0));
+  uint64_t threads = (uint64_t)std::max(1, bpsm) * x->num_sms * 128;
+  threads = std::min<uint64_t>(threads, ((uint64_t)nq + 127) / 128 * 128);
+  RET(x->memwork.ensure(std::max<uint64_t>(threads, 32) * 4 * MEM_SET_CAP * 16));
   bool done = false;
   for (int attempt = 0; attempt < 8 && !done; attempt++) {
-    RET(x->ivpool.ensure(x->iv_cap * 16)); x->iv_cap = x->ivpool.cap / 16;
+    RET(x->mivpool.ensure(x->miv_cap * 16)); x->miv_cap = x->mivpool.cap / 16;
     RET(x->hitpool.ensure(x->hit_cap * 32)); x->hit_cap = x->hitpool.cap / 32;
     CK(cudaMemsetAsync(x->ctr.p, 0, sizeof(Counters), x->stream));
-    Pool ivp{x->ivpool.p, &dctr(x)->iv_used, x->iv_cap}, hp{x->hitpool.p, &dctr(x)->hit_used, x->hit_cap};
+    Pool ivp{x->mivpool.p, &dctr(x)->iv_used, x->miv_cap}, hp{x->hitpool.p, &dctr(x)->hit_used, x->hit_cap};
     MemsOut o{x->hit_start.as<uint64_t>(), x->hit_count.as<uint32_t>(), x->status.as<uint32_t>(),
               x->ovf.as<uint32_t>(), &dctr(x)->n_ovf, &dctr(x)->touches};
     if (nq) {
-      unsigned grid = (nq + 127) / 128;
+      MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, nullptr, 0, &dctr(x)->queue, nullptr, nq, &dctr(x)->still_ovf};
+      unsigned grid = (unsigned)(threads / 128);
       cudaEventRecord(x->evk[0], x->stream);
-      if (x->count_work) k_mems<MEM_K, MEM_KC, true><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, nq, P, ivp, hp, o);
-      else k_mems<MEM_K, MEM_KC, false><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, nq, P, ivp, hp, o);
+      if (x->count_work)
+        k_mems<true, 32, MEM_KC><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                             d_q, d_qoff, P, ivp, hp, o, W);
+      else
+        k_mems<false, 32, MEM_KC><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                              d_q, d_qoff, P, ivp, hp, o, W);
       cudaEventRecord(x->evk[1], x->stream);
       x->k_search_rec = true;
       launches++;
@@ -415,20 +448,27 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
     RET(read_ctr(x));
     uint32_t n_ovf = x->h_ctr->n_ovf;
     if (n_ovf) {
-      uint32_t set_cap = 1024, cand_cap = 1024;
+      // fallback pass: contiguous per-thread sets and candidate lists, growing 4x
+      uint32_t set_cap = MEM_SET_CAP * 8, cand_cap = 256;
       while (true) {
         uint64_t per_thread = (uint64_t)set_cap * 4 * 16 + (uint64_t)cand_cap * sizeof(Cand);
-        uint32_t per = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n_ovf, (1ull << 30) / per_thread));
-        RET(x->work.ensure((size_t)per * set_cap * 4 * 16));
-        RET(x->cwork.ensure((size_t)per * cand_cap * sizeof(Cand)));
+        uint32_t nthr = (uint32_t)std::max<uint64_t>(32, std::min<uint64_t>((uint64_t)n_ovf, (2ull << 30) / per_thread));
+        nthr = (uint32_t)std::min<uint64_t>((nthr + 31) / 32 * 32, threads);
+        RET(x->work.ensure((size_t)nthr * set_cap * 4 * 16));
+        RET(x->cwork.ensure((size_t)nthr * cand_cap * sizeof(Cand)));
         CK(cudaMemsetAsync(&dctr(x)->still_ovf, 0, 4, x->stream));
-        for (uint32_t b = 0; b < n_ovf; b += per) {
-          uint32_t cnt = std::min(per, n_ovf - b);
-          if (x->count_work) k_mems_big<true><<<(cnt + 63) / 64, 64, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>() + b, cnt, P, x->work.as<BIv>(), set_cap, x->cwork.as<Cand>(), cand_cap, ivp, hp, o, &dctr(x)->still_ovf);
-          else k_mems_big<false><<<(cnt + 63) / 64, 64, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>() + b, cnt, P, x->work.as<BIv>(), set_cap, x->cwork.as<Cand>(), cand_cap, ivp, hp, o, &dctr(x)->still_ovf);
-          launches++;
-          CK(cudaGetLastError());
-        }
+        CK(cudaMemsetAsync(&dctr(x)->queue2, 0, 4, x->stream));
+        MemsWork W{x->work.as<BIv>(), set_cap, x->cwork.as<Cand>(), cand_cap, &dctr(x)->queue2, x->ovf.as<uint32_t>(),
+                   n_ovf, &dctr(x)->still_ovf};
+        unsigned grid = (nthr + 127) / 128;
+        if (x->count_work)
+          k_mems<true, 1, 0><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                         d_q, d_qoff, P, ivp, hp, o, W);
+        else
+          k_mems<false, 1, 0><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                          d_q, d_qoff, P, ivp, hp, o, W);
+        launches++;
+        CK(cudaGetLastError());
         RET(read_ctr(x));
         x->stats.fallback_reads += n_ovf;
         if (x->h_ctr->still_ovf == 0) break;
@@ -436,8 +476,8 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
         set_cap *= 4; cand_cap *= 4;
       }
     }
-    if (x->h_ctr->iv_used <= x->iv_cap && x->h_ctr->hit_used <= x->hit_cap) { done = true; break; }
-    x->iv_cap = std::max(x->iv_cap, (uint64_t)(x->h_ctr->iv_used * 3 / 2 + 4096));
+    if (x->h_ctr->iv_used <= x->miv_cap && x->h_ctr->hit_used <= x->hit_cap) { done = true; break; }
+    x->miv_cap = std::max(x->miv_cap, (uint64_t)(x->h_ctr->iv_used * 3 / 2 + 4096));
     x->hit_cap = std::max(x->hit_cap, (uint64_t)(x->h_ctr->hit_used * 3 / 2 + 4096));
   }
   if (!done) return set_error(HFM_E_OVERFLOW, "MEM pools did not converge");
@@ -532,6 +572,7 @@ int hfm_index_load(const uint8_t* bytes, size_t len, int kind, const hfm_opts* o
   CK(cudaSetDevice(dev));
   std::unique_ptr<hfm_index> x(new hfm_index());
   x->device = dev; x->kind = kind;
+  CK(cudaDeviceGetAttribute(&x->num_sms, cudaDevAttrMultiProcessorCount, dev));
   CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
   for (auto& e : x->ev) CK(cudaEventCreate(&e));
   for (auto& e : x->evk) CK(cudaEventCreate(&e));
@@ -552,7 +593,7 @@ void hfm_index_free(hfm_index* x) {
                     &x->rev.bounds, &x->rev.compat, &x->q, &x->qoff, &x->counts, &x->nhits, &x->niv, &x->ivoff,
                     &x->status, &x->ovf, &x->ivpool, &x->hitpool, &x->seg_row, &x->seg_off, &x->pos_base,
                     &x->seg_base, &x->scan_tmp, &x->out_pairs, &x->ref_bounds, &x->hit_start, &x->hit_count,
-                    &x->hit_base, &x->hits, &x->npos_scan, &x->work, &x->cwork, &x->ctr})
+                    &x->hit_base, &x->hits, &x->npos_scan, &x->work, &x->cwork, &x->ctr, &x->mivpool, &x->bswork, &x->memwork})
     b->release();
   for (auto& e : x->ev) if (e) cudaEventDestroy(e);
   for (auto& e : x->evk) if (e) cudaEventDestroy(e);

@@ -1,11 +1,15 @@
 // search.cuh — per-read search kernels: IUPAC backward search (count / locate
 // intervals) and the bidirectional SMEM / MEM candidate search.
 //
-// One thread owns one read; its interval sets live in thread-private arrays of a fixed
-// capacity (local memory, L1-cached) on the fast path.  A read whose set, candidate list
-// or output outgrows them is flagged and re-run by the same code with large global-memory
-// work areas (fallback launch), so there is no cap on interval-set size, as in the
-// reference CPU (src/fm_index/query.rs:248-274, src/fm_index/smem.rs:332-357).
+// Execution model: persistent grids (one wave of resident threads) pull reads from a
+// device work queue; one thread owns one read at a time.  A read's path is a chain of
+// ~|read| dependent rank steps, so throughput comes from keeping ~10^5 reads in flight,
+// not from spreading one read over a warp.  Interval sets live in per-thread slices of a
+// global work area, interleaved across the 32 lanes of a warp (element i of every lane is
+// one 512-byte run) with a fixed capacity; a read whose set, candidate list or output
+// outgrows it is queued for a fallback pass with much larger per-thread slices.  There is
+// therefore no cap on interval-set size, as in the reference CPU
+// (src/fm_index/query.rs:248-274, src/fm_index/smem.rs:332-357).
 #pragma once
 #include "dev_index.cuh"
 
@@ -18,23 +22,6 @@ struct Pool {
   uint64_t cap;               // elements
 };
 
-// Warp-aggregated bump allocation: every lane of the warp must call it (n may be 0).
-// Returns this lane's offset, or ~0ull when the pool is exhausted.
-__device__ __forceinline__ uint64_t warp_reserve(Pool& p, uint32_t n) {
-  const unsigned full = 0xFFFFFFFFu;
-  int lane = threadIdx.x & 31;
-  uint32_t incl = n;
-#pragma unroll
-  for (int d = 1; d < 32; d <<= 1) { uint32_t v = __shfl_up_sync(full, incl, d); if (lane >= d) incl += v; }
-  uint32_t total = __shfl_sync(full, incl, 31);
-  unsigned long long base = 0;
-  if (lane == 31 && total) base = atomicAdd(p.used, (unsigned long long)total);
-  base = __shfl_sync(full, base, 31);
-  uint64_t off = base + incl - n;
-  if (total == 0) return 0;
-  return (off + n <= p.cap) ? off : ~0ull;
-}
-
 __device__ __forceinline__ uint64_t thread_reserve(Pool& p, uint32_t n) {
   if (n == 0) return 0;
   unsigned long long off = atomicAdd(p.used, (unsigned long long)n);
@@ -44,19 +31,46 @@ __device__ __forceinline__ uint64_t thread_reserve(Pool& p, uint32_t n) {
 // Status bits per read.
 enum : uint32_t { ST_OK = 0, ST_SET_OVF = 1, ST_CAND_OVF = 2, ST_POOL_OVF = 4 };
 
+// A thread's interval set: element i at p[i * STRIDE].
+template <class T, int STRIDE>
+struct SetRef {
+  T* p;
+  __device__ __forceinline__ T& operator[](uint32_t i) const { return p[(size_t)i * STRIDE]; }
+};
+
+// Set s (of NS) of the calling thread inside `work`, `cap` elements each.
+// STRIDE 32: warp-interleaved slices (fast path); STRIDE 1: contiguous per-thread slices.
+template <class T, int STRIDE>
+__device__ __forceinline__ SetRef<T, STRIDE> thread_set(T* work, uint32_t cap, int NS, int s) {
+  uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (STRIDE == 32) {
+    uint64_t warp = tid >> 5, lane = tid & 31;
+    return SetRef<T, STRIDE>{work + ((warp * NS + s) * cap) * 32 + lane};
+  }
+  return SetRef<T, STRIDE>{work + (tid * NS + s) * cap};
+}
+
+// Next read from the device queue: reads are ids[k] (or k itself when ids is null).
+__device__ __forceinline__ bool next_read(unsigned int* ctr, uint32_t n, const uint32_t* ids, uint32_t& i) {
+  uint32_t k = atomicAdd(ctr, 1u);
+  if (k >= n) return false;
+  i = ids ? ids[k] : k;
+  return true;
+}
+
 // =====================================================================================
 // Backward search (FmIndex::backward_search, src/fm_index/query.rs:219-277)
 // =====================================================================================
 
 // Insert a non-empty interval into a sorted, coalesced set (the effect of
 // merge_intervals_inplace, src/fm_index/query.rs:390-407, applied incrementally).
-__device__ __forceinline__ bool iv_insert(uint2* a, uint32_t& n, uint32_t cap, uint32_t lo, uint32_t hi) {
+template <class SR>
+__device__ __forceinline__ bool iv_insert(const SR& a, uint32_t& n, uint32_t cap, uint32_t lo, uint32_t hi) {
   uint32_t j = n;
   while (j > 0 && a[j - 1].x > lo) j--;
   if (j > 0 && a[j - 1].y >= lo) { j--; lo = a[j].x; hi = max(hi, a[j].y); }
   uint32_t e = j;
   while (e < n && a[e].x <= hi) { hi = max(hi, a[e].y); e++; }
-  // replace a[j..e) by (lo, hi)
   uint32_t removed = e - j;
   if (removed == 0) {
     if (n >= cap) return false;
@@ -78,18 +92,17 @@ struct BsOut {
   uint32_t* status;      // per-query status bits
   uint32_t* ovf_list;    // queries to re-run with large sets
   uint32_t* n_ovf;
-  unsigned long long* touches;  // Occ record touches (nullptr: not counted)
+  unsigned long long* touches;  // Occ record touches (counted only with COUNT_TOUCH)
 };
 
-// Returns the final number of intervals in *cur (0 = no match), or ~0u on set overflow.
-template <bool COUNT_TOUCH>
+// Returns the final number of intervals in cur (0 = no match), or ~0u on set overflow.
+template <bool COUNT_TOUCH, class SR>
 __device__ __forceinline__ uint32_t backward_search_one(const DevFm& F, const SmemFm& S, const uint8_t* p,
-                                                        uint32_t m, uint2*& cur, uint2*& nxt, uint32_t cap,
+                                                        uint32_t m, SR& cur, SR& nxt, uint32_t cap,
                                                         uint64_t& touches) {
-  uint32_t n = 0;
-  if (m == 0) { cur[0] = make_uint2(0, F.text_len); return 1; }
-  uint32_t start = m;
-  cur[0] = make_uint2(0, F.text_len); n = 1;
+  cur[0] = make_uint2(0, F.text_len);
+  if (m == 0) return 1;
+  uint32_t n = 1, start = m;
   if (F.lut && m >= F.lut_depth) {
     // LookupTable::get (src/fm_index/lookup.rs:101-111): rightmost code is the most
     // significant digit of the base-radix index.
@@ -123,91 +136,58 @@ __device__ __forceinline__ uint32_t backward_search_one(const DevFm& F, const Sm
       for (int r = 0; r < 16; r++) {
         if (!((mask >> r) & 1)) continue;
         uint32_t nl = S.C[r] + rl[r], nh = S.C[r] + rh[r];
-        if (nl < nh) {
-          if (!iv_insert(nxt, nn, cap, nl, nh)) return ~0u;
-        }
+        if (nl < nh && !iv_insert(nxt, nn, cap, nl, nh)) return ~0u;
       }
     }
     if (nn == 0) return 0;
-    uint2* t = cur; cur = nxt; nxt = t; n = nn;
+    SR t = cur; cur = nxt; nxt = t; n = nn;
   }
   return n;
 }
 
-template <int K, bool COUNT_TOUCH>
+// Persistent backward search.  ids == nullptr: every query 0..n-1; otherwise the listed
+// queries (fallback pass; reads that overflow there bump *still_ovf).
+template <bool COUNT_TOUCH, int STRIDE>
 __global__ void __launch_bounds__(256) k_bsearch(DevFm F, const uint16_t* __restrict__ compat_masks,
                                                 const uint8_t* __restrict__ q, const uint64_t* __restrict__ qoff,
-                                                uint32_t nq, uint32_t cap, Pool pool, BsOut out) {
+                                                const uint32_t* __restrict__ ids, uint32_t n, uint32_t hit_cap,
+                                                uint2* work, uint32_t set_cap, unsigned int* queue, Pool pool,
+                                                BsOut out, uint32_t* still_ovf) {
   __shared__ SmemFm S;
   smem_fm_init(S, F, compat_masks);
   __syncthreads();
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool active = i < nq;
-  uint2 a[K], b[K];
-  uint2* cur = a; uint2* nxt = b;
-  uint32_t n = 0, st = ST_OK;
+  SetRef<uint2, STRIDE> A = thread_set<uint2, STRIDE>(work, set_cap, 2, 0);
+  SetRef<uint2, STRIDE> B = thread_set<uint2, STRIDE>(work, set_cap, 2, 1);
   uint64_t touches = 0;
-  if (active) {
+  uint32_t i;
+  while (next_read(queue, n, ids, i)) {
+    SetRef<uint2, STRIDE> cur = A, nxt = B;
     uint64_t o = qoff[i];
-    n = backward_search_one<COUNT_TOUCH>(F, S, q + o, (uint32_t)(qoff[i + 1] - o), cur, nxt, K, touches);
-    if (n == ~0u) { st = ST_SET_OVF; n = 0; }
-  }
-  uint32_t cnt = 0; uint64_t hits = 0;
-  for (uint32_t k = 0; k < n; k++) {
-    uint32_t sz = cur[k].y - cur[k].x;
-    cnt += sz; hits += (cap && sz > cap) ? cap : sz;
-  }
-  uint64_t off = 0;
-  if (out.nhits) {
-    off = warp_reserve(pool, n);
-    if (off == ~0ull) { st |= ST_POOL_OVF; }
-    else {
-      uint2* dst = (uint2*)pool.base + off;
-      for (uint32_t k = 0; k < n; k++) dst[k] = cur[k];
+    uint32_t niv = backward_search_one<COUNT_TOUCH>(F, S, q + o, (uint32_t)(qoff[i + 1] - o), cur, nxt, set_cap,
+                                                    touches);
+    uint32_t st = ST_OK;
+    if (niv == ~0u) { st = ST_SET_OVF; niv = 0; }
+    uint32_t cnt = 0; uint64_t hits = 0;
+    for (uint32_t k = 0; k < niv; k++) {
+      uint2 v = cur[k];
+      uint32_t sz = v.y - v.x;
+      cnt += sz; hits += (hit_cap && sz > hit_cap) ? hit_cap : sz;
+    }
+    uint64_t off = 0;
+    if (out.nhits && niv) {
+      off = thread_reserve(pool, niv);
+      if (off == ~0ull) st |= ST_POOL_OVF;
+      else { uint2* dst = (uint2*)pool.base + off; for (uint32_t k = 0; k < niv; k++) dst[k] = cur[k]; }
+    }
+    out.counts[i] = cnt;
+    if (out.nhits) { out.nhits[i] = hits; out.niv[i] = niv; out.ivoff[i] = off; }
+    out.status[i] = st;
+    if (st & ST_SET_OVF) {
+      if (ids) atomicAdd(still_ovf, 1u);
+      else out.ovf_list[atomicAdd(out.n_ovf, 1u)] = i;
     }
   }
   if (COUNT_TOUCH && touches) atomicAdd(out.touches, (unsigned long long)touches);
-  if (!active) return;
-  out.counts[i] = cnt;
-  if (out.nhits) { out.nhits[i] = hits; out.niv[i] = n; out.ivoff[i] = off; }
-  out.status[i] = st;
-  if (st & ST_SET_OVF) out.ovf_list[atomicAdd(out.n_ovf, 1u)] = i;
-}
-
-// Fallback: one thread per flagged query, interval sets in global memory (`cap` each).
-template <bool COUNT_TOUCH>
-__global__ void __launch_bounds__(128) k_bsearch_big(DevFm F, const uint16_t* __restrict__ compat_masks,
-                                                    const uint8_t* __restrict__ q, const uint64_t* __restrict__ qoff,
-                                                    const uint32_t* __restrict__ ids, uint32_t nids, uint32_t hit_cap,
-                                                    uint2* work, uint32_t set_cap, Pool pool, BsOut out,
-                                                    uint32_t* still_ovf) {
-  __shared__ SmemFm S;
-  smem_fm_init(S, F, compat_masks);
-  __syncthreads();
-  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nids) return;
-  uint32_t i = ids[t];
-  uint2* cur = work + (size_t)t * 2 * set_cap;
-  uint2* nxt = cur + set_cap;
-  uint64_t touches = 0, o = qoff[i];
-  uint32_t n = backward_search_one<COUNT_TOUCH>(F, S, q + o, (uint32_t)(qoff[i + 1] - o), cur, nxt, set_cap, touches);
-  if (n == ~0u) { atomicAdd(still_ovf, 1u); out.status[i] = ST_SET_OVF; return; }
-  uint32_t cnt = 0; uint64_t hits = 0;
-  for (uint32_t k = 0; k < n; k++) {
-    uint32_t sz = cur[k].y - cur[k].x;
-    cnt += sz; hits += (hit_cap && sz > hit_cap) ? hit_cap : sz;
-  }
-  uint32_t st = ST_OK;
-  uint64_t off = 0;
-  if (out.nhits) {
-    off = thread_reserve(pool, n);
-    if (off == ~0ull) st = ST_POOL_OVF;
-    else { uint2* dst = (uint2*)pool.base + off; for (uint32_t k = 0; k < n; k++) dst[k] = cur[k]; }
-  }
-  if (COUNT_TOUCH && touches) atomicAdd(out.touches, (unsigned long long)touches);
-  out.counts[i] = cnt;
-  if (out.nhits) { out.nhits[i] = hits; out.niv[i] = n; out.ivoff[i] = off; }
-  out.status[i] = st;
 }
 
 // =====================================================================================
@@ -218,11 +198,11 @@ __global__ void __launch_bounds__(128) k_bsearch_big(DevFm F, const uint16_t* __
 // emitted in ascending fwd_lo order at the end.
 // =====================================================================================
 
-// dir 0 = right (ranks on the reverse index), 1 = left (ranks on the forward index).
-template <int DIR, bool COUNT_TOUCH>
-__device__ __forceinline__ uint32_t extend_set(const DevFm& X, const SmemFm& S, uint32_t mask,
-                                               const BIv* in, uint32_t nin, BIv* out, uint32_t cap,
-                                               uint32_t& cov, bool& ovf, uint64_t& touches) {
+// DIR 0 = right (ranks on the reverse index), 1 = left (ranks on the forward index).
+template <int DIR, bool COUNT_TOUCH, class SRI, class SRO>
+__device__ __forceinline__ uint32_t extend_set(const DevFm& X, const SmemFm& S, uint32_t mask, const SRI& in,
+                                               uint32_t nin, const SRO& out, uint32_t cap, uint32_t& cov,
+                                               bool& ovf, uint64_t& touches) {
   uint32_t nout = 0; cov = 0;
   for (uint32_t i = 0; i < nin; i++) {
     BIv iv = in[i];
@@ -251,8 +231,8 @@ __device__ __forceinline__ uint32_t extend_set(const DevFm& X, const SmemFm& S, 
 }
 
 // Does any interval of the set extend by a compatible symbol?
-template <int DIR, bool COUNT_TOUCH>
-__device__ __forceinline__ bool any_extend(const DevFm& X, const SmemFm& S, uint32_t mask, const BIv* in,
+template <int DIR, bool COUNT_TOUCH, class SR>
+__device__ __forceinline__ bool any_extend(const DevFm& X, const SmemFm& S, uint32_t mask, const SR& in,
                                            uint32_t nin, uint64_t& touches) {
   for (uint32_t i = 0; i < nin; i++) {
     BIv iv = in[i];
@@ -294,17 +274,17 @@ __device__ __forceinline__ void sort_by_flo(BIv* a, uint32_t n) {
 
 // Candidate search for one read.  Returns the number of candidates, or ~0u on overflow
 // of a set, the candidate list or the interval pool (flags in st).
-template <bool COUNT_TOUCH>
+template <bool COUNT_TOUCH, class SR>
 __device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf, const SmemFm& Sr,
-                             const uint8_t* q, uint32_t n, const MemsParams& P, BIv* curr, BIv* nxt, BIv* wa,
-                             BIv* wb, uint32_t set_cap, Cand* cands, uint32_t cand_cap, Pool& ivpool,
-                             uint32_t& st, uint64_t& touches) {
+                             const uint8_t* q, uint32_t n, const MemsParams& P, const SR& curr, const SR& nxt,
+                             const SR& wa, const SR& wb, uint32_t set_cap, Cand* cands, uint32_t cand_cap,
+                             Pool& ivpool, uint32_t& st, uint64_t& touches) {
   uint32_t nc = 0;
   if (n == 0 || P.min_len == 0) return 0;
   const BIv full = {0, Fw.text_len, 0, Fw.text_len};
   bool ovf = false;
   auto qmask = [&](const SmemFm& S, uint8_t c) -> uint32_t { return c < 16 ? S.compat_mask[c] : 0u; };
-  auto emit = [&](uint32_t qs, uint32_t qe, uint32_t count, const BIv* ivs, uint32_t niv) -> bool {
+  auto emit = [&](uint32_t qs, uint32_t qe, uint32_t count, const SR& ivs, uint32_t niv) -> bool {
     if (nc >= cand_cap) { st |= ST_CAND_OVF; return false; }
     uint64_t off = thread_reserve(ivpool, niv);
     if (off == ~0ull) { st |= ST_POOL_OVF; return false; }
@@ -316,7 +296,7 @@ __device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf,
   if (P.mode == 1) {
     // find_mems: raw_mem_from(i) for every start (src/fm_index/smem.rs:250-295)
     for (uint32_t i = 0; i < n; i++) {
-      BIv* c = curr; BIv* x = nxt;
+      SR c = curr, x = nxt;
       c[0] = full;
       uint32_t ncur = 1, cov = 0, j = i;
       bool matched = false;
@@ -325,7 +305,7 @@ __device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf,
         uint32_t nn = extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, ncur, x, set_cap, ncov, ovf, touches);
         if (ovf) { st |= ST_SET_OVF; return ~0u; }
         if (nn == 0) break;
-        BIv* t = c; c = x; x = t; ncur = nn; cov = ncov; j++; matched = true;
+        SR t = c; c = x; x = t; ncur = nn; cov = ncov; j++; matched = true;
       }
       if (!matched || j - i < P.min_len) continue;
       bool lmax = i == 0 || !any_extend<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[i - 1]), c, ncur, touches);
@@ -337,16 +317,16 @@ __device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf,
   // find_smems: collect_smem_candidates (src/fm_index/smem.rs:154-222)
   uint32_t pivot = 0;
   while (pivot < n) {
-    BIv* c = curr; BIv* x = nxt;
+    SR c = curr, x = nxt;
+    x[0] = full;
     uint32_t cov;
-    uint32_t ncur = extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[pivot]), &full, 1, c, set_cap, cov, ovf, touches);
+    uint32_t ncur = extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[pivot]), x, 1, c, set_cap, cov, ovf, touches);
     if (ovf) { st |= ST_SET_OVF; return ~0u; }
     if (ncur == 0) { pivot++; continue; }
     uint32_t j = pivot + 1, reach = pivot + 1;
     for (;;) {
-      uint32_t end; bool next_empty;
-      uint32_t nn = 0, ncov = 0;
-      bool record;
+      uint32_t end, nn = 0, ncov = 0;
+      bool next_empty, record;
       if (j == n) { end = n; next_empty = true; record = true; }
       else {
         nn = extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, ncur, x, set_cap, ncov, ovf, touches);
@@ -356,24 +336,27 @@ __device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf,
       if (record) {
         // right-maximal prefix [pivot, end): extend_left_maximally (smem.rs:227-243)
         reach = end;
-        const BIv* b = c; uint32_t nb = ncur, start = pivot;
-        BIv* bufs[2] = {wa, wb}; int t = 0;
-        uint32_t bcov = cov;
+        SR b = c;
+        uint32_t nb = ncur, start = pivot, bcov = cov;
+        SR bufs[2] = {wa, wb};
+        int t = 0;
         while (start > 0) {
           uint32_t lcov;
-          uint32_t nl = extend_set<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[start - 1]), b, nb, bufs[t], set_cap, lcov, ovf, touches);
+          uint32_t nl = extend_set<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[start - 1]), b, nb, bufs[t], set_cap, lcov,
+                                                   ovf, touches);
           if (ovf) { st |= ST_SET_OVF; return ~0u; }
           if (nl == 0) break;
           b = bufs[t]; nb = nl; bcov = lcov; t ^= 1; start--;
         }
         if (end - start >= P.min_len) {
+          // right-maximality (smem.rs:202-207); with no left extension it is next_empty
           bool rmax = end == n ||
                       (start == pivot ? next_empty : !any_extend<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[end]), b, nb, touches));
           if (rmax && !emit(start, end, bcov, b, nb)) return ~0u;
         }
       }
       if (j == n || nn == 0) break;
-      BIv* tt = c; c = x; x = tt; ncur = nn; cov = ncov; j++;
+      SR tt = c; c = x; x = tt; ncur = nn; cov = ncov; j++;
     }
     pivot = max(reach, pivot + 1);
   }
@@ -398,7 +381,6 @@ __device__ __forceinline__ uint32_t finalize_smems(Cand* c, uint32_t n) {
       if (j != i && c[j].qs <= c[i].qs && c[i].qe <= c[j].qe) contained = true;   // distinct after dedup
     if (!contained) c[w++] = c[i];
   }
-  // survivors keep sorted order; compaction in place is safe because w <= i
   return w;
 }
 
@@ -420,73 +402,63 @@ __device__ __forceinline__ bool write_hits(Cand* c, uint32_t n, const MemsParams
     for (uint32_t t = 0; t < c[k].nivs; t++) {
       uint32_t sz = ivs[t].fhi - ivs[t].flo;
       uint32_t eff = P.resolve ? min(sz, P.max_hits) : 0u;
-      h[0] = c[k].qs; h[1] = c[k].qe; h[2] = sz; h[3] = sz > P.max_hits ? 1u : 0u;
-      h[4] = ivs[t].flo; h[5] = eff; h[6] = 0; h[7] = 0;
+      uint4 a = make_uint4(c[k].qs, c[k].qe, sz, sz > P.max_hits ? 1u : 0u);
+      uint4 b = make_uint4(ivs[t].flo, eff, 0u, 0u);
+      reinterpret_cast<uint4*>(h)[0] = a; reinterpret_cast<uint4*>(h)[1] = b;
       h += 8;
     }
   }
   return true;
 }
 
-template <int K, int KC, bool COUNT_TOUCH>
+struct MemsWork {
+  BIv* sets; uint32_t set_cap;        // 4 sets per thread
+  Cand* cands; uint32_t cand_cap;     // contiguous per thread (fallback pass); nullptr: local
+  unsigned int* queue;
+  const uint32_t* ids; uint32_t n;    // reads to process (ids == nullptr: 0..n-1)
+  uint32_t* still_ovf;
+};
+
+template <bool COUNT_TOUCH, int STRIDE, int KC>
 __global__ void __launch_bounds__(128) k_mems(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
                                              const uint16_t* __restrict__ compat_rv, const uint8_t* __restrict__ q,
-                                             const uint64_t* __restrict__ qoff, uint32_t nq, MemsParams P,
-                                             Pool ivpool, Pool hitpool, MemsOut out) {
+                                             const uint64_t* __restrict__ qoff, MemsParams P, Pool ivpool,
+                                             Pool hitpool, MemsOut out, MemsWork W) {
   __shared__ SmemFm Sf, Sr;
   smem_fm_init(Sf, Fw, compat_fw);
   smem_fm_init(Sr, Rv, compat_rv);
   __syncthreads();
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nq) return;
-  BIv curr[K], nxt[K], wa[K], wb[K];
-  Cand cands[KC];
-  uint32_t st = ST_OK;
-  uint64_t touches = 0, o = qoff[i];
-  uint32_t nc = mems_one<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, (uint32_t)(qoff[i + 1] - o), P, curr, nxt, wa, wb, K,
-                                      cands, KC, ivpool, st, touches);
-  uint64_t hs = 0; uint32_t hc = 0;
-  if (nc != ~0u) {
-    if (P.mode == 0) nc = finalize_smems(cands, nc);
-    if (!write_hits(cands, nc, P, ivpool, hitpool, hs, hc)) st |= ST_POOL_OVF;
+  using SR = SetRef<BIv, STRIDE>;
+  SR s0 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 0), s1 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 1);
+  SR s2 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 2), s3 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 3);
+  Cand local_c[KC > 0 ? KC : 1];
+  Cand* cands = local_c;
+  uint32_t cand_cap = KC;
+  if (KC == 0) {
+    uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    cands = W.cands + tid * W.cand_cap;
+    cand_cap = W.cand_cap;
+  }
+  uint64_t touches = 0;
+  uint32_t i;
+  while (next_read(W.queue, W.n, W.ids, i)) {
+    uint32_t st = ST_OK;
+    uint64_t o = qoff[i];
+    uint32_t nc = mems_one<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, (uint32_t)(qoff[i + 1] - o), P, s0, s1, s2, s3,
+                                        W.set_cap, cands, cand_cap, ivpool, st, touches);
+    uint64_t hs = 0; uint32_t hc = 0;
+    if (nc != ~0u) {
+      if (P.mode == 0) nc = finalize_smems(cands, nc);
+      if (!write_hits(cands, nc, P, ivpool, hitpool, hs, hc)) st |= ST_POOL_OVF;
+    }
+    if (st) { hs = 0; hc = 0; }
+    out.hit_start[i] = hs; out.hit_count[i] = hc; out.status[i] = st;
+    if (st & (ST_SET_OVF | ST_CAND_OVF)) {
+      if (W.ids) atomicAdd(W.still_ovf, 1u);
+      else out.ovf_list[atomicAdd(out.n_ovf, 1u)] = i;
+    }
   }
   if (COUNT_TOUCH && touches) atomicAdd(out.touches, (unsigned long long)touches);
-  if (st) { hs = 0; hc = 0; }
-  out.hit_start[i] = hs; out.hit_count[i] = hc; out.status[i] = st;
-  if (st & (ST_SET_OVF | ST_CAND_OVF)) out.ovf_list[atomicAdd(out.n_ovf, 1u)] = i;
-}
-
-// Fallback for reads whose sets or candidate lists overflowed: global work areas.
-template <bool COUNT_TOUCH>
-__global__ void __launch_bounds__(64) k_mems_big(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
-                                                const uint16_t* __restrict__ compat_rv, const uint8_t* __restrict__ q,
-                                                const uint64_t* __restrict__ qoff, const uint32_t* __restrict__ ids,
-                                                uint32_t nids, MemsParams P, BIv* work, uint32_t set_cap,
-                                                Cand* cwork, uint32_t cand_cap, Pool ivpool, Pool hitpool,
-                                                MemsOut out, uint32_t* still_ovf) {
-  __shared__ SmemFm Sf, Sr;
-  smem_fm_init(Sf, Fw, compat_fw);
-  smem_fm_init(Sr, Rv, compat_rv);
-  __syncthreads();
-  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nids) return;
-  uint32_t i = ids[t];
-  BIv* base = work + (size_t)t * 4 * set_cap;
-  Cand* cands = cwork + (size_t)t * cand_cap;
-  uint32_t st = ST_OK;
-  uint64_t touches = 0, o = qoff[i];
-  uint32_t nc = mems_one<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, (uint32_t)(qoff[i + 1] - o), P, base, base + set_cap,
-                                      base + 2 * set_cap, base + 3 * set_cap, set_cap, cands, cand_cap, ivpool, st,
-                                      touches);
-  uint64_t hs = 0; uint32_t hc = 0;
-  if (nc != ~0u) {
-    if (P.mode == 0) nc = finalize_smems(cands, nc);
-    if (!write_hits(cands, nc, P, ivpool, hitpool, hs, hc)) st |= ST_POOL_OVF;
-  }
-  if (COUNT_TOUCH && touches) atomicAdd(out.touches, (unsigned long long)touches);
-  if (st) { hs = 0; hc = 0; }
-  if (st & (ST_SET_OVF | ST_CAND_OVF)) atomicAdd(still_ovf, 1u);
-  out.hit_start[i] = hs; out.hit_count[i] = hc; out.status[i] = st;
 }
 
 }  // namespace hfm
