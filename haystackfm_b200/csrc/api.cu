@@ -256,6 +256,7 @@ static int run_bsearch(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
             x->status.as<uint32_t>(), x->ovf.as<uint32_t>(), &dctr(x)->n_ovf, &dctr(x)->touches};
     if (nq) {
       unsigned grid = (unsigned)(threads / 256);
+      if (x->bswork.cap < (size_t)grid * 256 * 2 * BS_SET_CAP * 8) return set_error(HFM_E_ARG, "internal: work area too small");
       cudaEventRecord(x->evk[0], x->stream);
       if (x->count_work)
         k_bsearch<true, 32><<<grid, 256, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, nullptr, nq, cap,
@@ -279,11 +280,13 @@ static int run_bsearch(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       while (true) {
         uint64_t per_thread = (uint64_t)set_cap * 2 * 8;
         uint32_t nthr = (uint32_t)std::max<uint64_t>(32, std::min<uint64_t>((uint64_t)n_ovf, (2ull << 30) / per_thread));
-        nthr = std::min<uint32_t>((nthr + 31) / 32 * 32, (uint32_t)threads);
+        // every launched thread may take a read from the queue: size for the whole grid
+        nthr = (uint32_t)std::min<uint64_t>((nthr + 127) / 128 * 128, std::max<uint64_t>(threads, 128));
         RET(x->work.ensure((size_t)nthr * per_thread));
         CK(cudaMemsetAsync(&dctr(x)->still_ovf, 0, 4, x->stream));
         CK(cudaMemsetAsync(&dctr(x)->queue2, 0, 4, x->stream));
         unsigned grid = (nthr + 127) / 128;
+        if (x->work.cap < (size_t)grid * 128 * per_thread) return set_error(HFM_E_ARG, "internal: fallback work area too small");
         if (x->count_work)
           k_bsearch<true, 1><<<grid, 128, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>(),
                                                          n_ovf, cap, x->work.as<uint2>(), set_cap, &dctr(x)->queue2, pool,
@@ -433,6 +436,7 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
     if (nq) {
       MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, nullptr, 0, &dctr(x)->queue, nullptr, nq, &dctr(x)->still_ovf};
       unsigned grid = (unsigned)(threads / 128);
+      if (x->memwork.cap < (size_t)grid * 128 * 4 * MEM_SET_CAP * 16) return set_error(HFM_E_ARG, "internal: work area too small");
       cudaEventRecord(x->evk[0], x->stream);
       if (x->count_work)
         k_mems<true, 32, MEM_KC><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
@@ -453,7 +457,8 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       while (true) {
         uint64_t per_thread = (uint64_t)set_cap * 4 * 16 + (uint64_t)cand_cap * sizeof(Cand);
         uint32_t nthr = (uint32_t)std::max<uint64_t>(32, std::min<uint64_t>((uint64_t)n_ovf, (2ull << 30) / per_thread));
-        nthr = (uint32_t)std::min<uint64_t>((nthr + 31) / 32 * 32, threads);
+        // every launched thread may take a read from the queue: size for the whole grid
+        nthr = (uint32_t)std::min<uint64_t>((nthr + 127) / 128 * 128, std::max<uint64_t>(threads, 128));
         RET(x->work.ensure((size_t)nthr * set_cap * 4 * 16));
         RET(x->cwork.ensure((size_t)nthr * cand_cap * sizeof(Cand)));
         CK(cudaMemsetAsync(&dctr(x)->still_ovf, 0, 4, x->stream));
@@ -461,6 +466,8 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
         MemsWork W{x->work.as<BIv>(), set_cap, x->cwork.as<Cand>(), cand_cap, &dctr(x)->queue2, x->ovf.as<uint32_t>(),
                    n_ovf, &dctr(x)->still_ovf};
         unsigned grid = (nthr + 127) / 128;
+        if (x->work.cap < (size_t)grid * 128 * set_cap * 4 * 16 || x->cwork.cap < (size_t)grid * 128 * cand_cap * sizeof(Cand))
+          return set_error(HFM_E_ARG, "internal: fallback work area too small");
         if (x->count_work)
           k_mems<true, 1, 0><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                          d_q, d_qoff, P, ivp, hp, o, W);
