@@ -16,6 +16,9 @@ from .errors import FmIndexError
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libhfm.so")
 
+HFM_FLAG_DEDUP_ALWAYS = 1
+HFM_FLAG_DEDUP_NEVER = 2
+
 u8p = C.POINTER(C.c_uint8)
 u32p = C.POINTER(C.c_uint32)
 u64p = C.POINTER(C.c_uint64)
@@ -63,7 +66,7 @@ class HfmStats(C.Structure):
                 ("search_launches", C.c_uint32), ("resolve_launches", C.c_uint32),
                 ("other_launches", C.c_uint32), ("fallback_reads", C.c_uint32),
                 ("occ_touches", C.c_uint64), ("lf_calls", C.c_uint64), ("rows_resolved", C.c_uint64),
-                ("hits_out", C.c_uint64)]
+                ("hits_out", C.c_uint64), ("rows_unique", C.c_uint64)]
 
 
 class HfmBuildOpts(C.Structure):

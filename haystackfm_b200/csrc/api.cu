@@ -13,8 +13,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <mutex>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -108,7 +110,8 @@ struct hfm_index {
   // per-call work buffers (grow-only)
   DevBuf q, qoff, counts, nhits, niv, ivoff, status, ovf, ivpool, hitpool, seg_row, seg_off, pos_base, seg_base,
       scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr,
-      mivpool, bswork, memwork;
+      mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout;
+  uint32_t flags = 0;
   int num_sms = 0;
   uint64_t iv_cap = 0, miv_cap = 0, hit_cap = 0;   // pool capacities in elements (uint2 / BIv / hit)
   Counters* h_ctr = nullptr;        // pinned
@@ -334,6 +337,50 @@ static int resolve(hfm_index* x, const FmDev& F, const uint32_t* seg_row, uint32
   return HFM_OK;
 }
 
+// Resolve with deduplication of identical segments (see k_dedup_*): each distinct
+// (first row, length) is walked once and copied to every hit that has it.
+static int resolve_segments(hfm_index* x, const FmDev& F, const uint32_t* seg_row, uint32_t stride,
+                            const uint64_t* seg_off, uint64_t nseg, uint64_t total, const uint32_t* d_bounds,
+                            uint32_t nb, uint32_t* out, uint32_t& launches, uint32_t& other) {
+  if (total == 0) return HFM_OK;
+  bool dedup = (x->flags & HFM_FLAG_DEDUP_ALWAYS) || (!(x->flags & HFM_FLAG_DEDUP_NEVER) && total >= 4 * nseg);
+  if (!dedup || nseg < 2) return resolve(x, F, seg_row, stride, seg_off, nseg, total, d_bounds, nb, out, launches);
+  uint64_t size = 1024;
+  while (size < 2 * nseg) size <<= 1;
+  RET(x->hkeys.ensure(size * 8)); RET(x->hslot.ensure(nseg * 4 + 4));
+  RET(x->hflags.ensure(size * 4)); RET(x->huid.ensure((size + 1) * 8));
+  CK(cudaMemsetAsync(x->hkeys.p, 0xFF, size * 8, x->stream));
+  k_dedup_insert<<<(unsigned)((nseg + 255) / 256), 256, 0, x->stream>>>(seg_row, stride, seg_off, (uint32_t)nseg,
+                                                                      x->hkeys.as<unsigned long long>(), size - 1,
+                                                                      x->hslot.as<uint32_t>());
+  k_dedup_flags<<<(unsigned)((size + 255) / 256), 256, 0, x->stream>>>(x->hkeys.as<unsigned long long>(), size,
+                                                                     x->hflags.as<uint32_t>());
+  other += 2;
+  CK(cudaGetLastError());
+  RET(scan(x, x->hflags.as<uint32_t>(), 1, size, x->huid.as<uint64_t>(), other));
+  uint64_t nuniq = 0;
+  RET(read_u64(x, x->huid.as<uint64_t>() + size, nuniq));
+  RET(x->urow.ensure(nuniq * 4 + 4)); RET(x->ulen.ensure(nuniq * 4 + 4)); RET(x->uoff.ensure((nuniq + 1) * 8));
+  k_dedup_compact<<<(unsigned)((size + 255) / 256), 256, 0, x->stream>>>(x->hkeys.as<unsigned long long>(), size,
+                                                                       x->huid.as<uint64_t>(), x->urow.as<uint32_t>(),
+                                                                       x->ulen.as<uint32_t>());
+  other++;
+  CK(cudaGetLastError());
+  RET(scan(x, x->ulen.as<uint32_t>(), 1, nuniq, x->uoff.as<uint64_t>(), other));
+  uint64_t utotal = 0;
+  RET(read_u64(x, x->uoff.as<uint64_t>() + nuniq, utotal));
+  RET(x->uout.ensure(utotal * 8 + 8));
+  RET(resolve(x, F, x->urow.as<uint32_t>(), 1, x->uoff.as<uint64_t>(), nuniq, utotal, d_bounds, nb,
+              x->uout.as<uint32_t>(), launches));
+  k_dedup_expand<<<(unsigned)((total + EXP_T - 1) / EXP_T), EXP_T, 0, x->stream>>>(
+      seg_off, (uint32_t)nseg, total, x->hslot.as<uint32_t>(), x->huid.as<uint64_t>(), x->uoff.as<uint64_t>(),
+      x->uout.as<uint2>(), reinterpret_cast<uint2*>(out));
+  other++;
+  CK(cudaGetLastError());
+  x->stats.rows_unique += utotal;
+  return HFM_OK;
+}
+
 static void begin_stats(hfm_index* x) {
   x->stats = hfm_stats{};
   x->k_search_rec = x->k_resolve_rec = false;
@@ -392,8 +439,8 @@ static int locate_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qof
   CK(cudaMemcpyAsync(x->seg_off.as<uint64_t>() + nseg, &total, 8, cudaMemcpyHostToDevice, x->stream));
   cudaEventRecord(x->ev[1], x->stream);
   uint32_t rl = 0;
-  RET(resolve(x, x->fwd, x->seg_row.as<uint32_t>(), 1, x->seg_off.as<uint64_t>(), nseg, total,
-              x->fwd.bounds.as<uint32_t>(), (uint32_t)x->fwd.seq_boundaries.size(), x->out_pairs.as<uint32_t>(), rl));
+  RET(resolve_segments(x, x->fwd, x->seg_row.as<uint32_t>(), 1, x->seg_off.as<uint64_t>(), nseg, total,
+              x->fwd.bounds.as<uint32_t>(), (uint32_t)x->fwd.seq_boundaries.size(), x->out_pairs.as<uint32_t>(), rl, other));
   RET(read_ctr(x));
   end_stats(x);
   x->stats.search_launches = launches; x->stats.resolve_launches = rl; x->stats.other_launches = other;
@@ -514,8 +561,8 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   RET(x->out_pairs.ensure(npos * 8 + 8));
   cudaEventRecord(x->ev[1], x->stream);
   uint32_t rl = 0;
-  RET(resolve(x, Fw, x->hits.as<uint32_t>() + 4, 8, x->npos_scan.as<uint64_t>(), nh, npos,
-              x->ref_bounds.as<uint32_t>(), nb, x->out_pairs.as<uint32_t>(), rl));
+  RET(resolve_segments(x, Fw, x->hits.as<uint32_t>() + 4, 8, x->npos_scan.as<uint64_t>(), nh, npos,
+              x->ref_bounds.as<uint32_t>(), nb, x->out_pairs.as<uint32_t>(), rl, other));
   RET(read_ctr(x));
   end_stats(x);
   x->stats.search_launches = launches; x->stats.resolve_launches = rl; x->stats.other_launches = other;
@@ -540,6 +587,48 @@ static int stage_queries(hfm_index* x, const uint8_t* q, const uint64_t* q_off, 
   return HFM_OK;
 }
 
+// Result blocks of the host-buffer entry points come from a process-wide cache of
+// pinned host memory: the device-to-host copy of a result runs at link speed and a
+// block released by hfm_free is reused by the next call instead of being re-pinned.
+struct PinnedCache {
+  std::mutex mu;
+  std::multimap<size_t, void*> free_blocks;
+  std::unordered_map<void*, size_t> owned;
+  size_t cached_bytes = 0;
+};
+static PinnedCache& pinned_cache() { static PinnedCache* c = new PinnedCache(); return *c; }
+static constexpr size_t PINNED_CACHE_MAX = 48ull << 30;
+
+static void* host_result_alloc(size_t bytes) {
+  PinnedCache& P = pinned_cache();
+  std::lock_guard<std::mutex> lk(P.mu);
+  auto it = P.free_blocks.lower_bound(bytes);
+  if (it != P.free_blocks.end() && it->first <= 2 * bytes + (64ull << 20)) {
+    void* p = it->second;
+    P.cached_bytes -= it->first;
+    P.free_blocks.erase(it);
+    return p;
+  }
+  size_t sz = (bytes + (2ull << 20) - 1) & ~((2ull << 20) - 1);
+  void* p = nullptr;
+  if (cudaHostAlloc(&p, sz, cudaHostAllocDefault) != cudaSuccess) {
+    cudaGetLastError();
+    return std::malloc(bytes);          // pageable fallback, released by std::free
+  }
+  P.owned[p] = sz;
+  return p;
+}
+
+static void host_result_free(void* p) {
+  PinnedCache& P = pinned_cache();
+  std::lock_guard<std::mutex> lk(P.mu);
+  auto it = P.owned.find(p);
+  if (it == P.owned.end()) { std::free(p); return; }
+  if (P.cached_bytes + it->second > PINNED_CACHE_MAX) { cudaFreeHost(p); P.owned.erase(it); return; }
+  P.free_blocks.insert({it->second, p});
+  P.cached_bytes += it->second;
+}
+
 struct Guard {
   hfm_index* x;
   std::unique_lock<std::mutex> lk;
@@ -555,7 +644,9 @@ extern "C" {
 
 const char* hfm_last_error(void) { return hfm::g_err.c_str(); }
 
-void hfm_free(void* p) { std::free(p); }
+void hfm_free(void* p) {
+  if (p) host_result_free(p);
+}
 
 int hfm_index_load(const uint8_t* bytes, size_t len, int kind, const hfm_opts* opts, hfm_index** out) {
   if (!bytes || !out) return set_error(HFM_E_ARG, "NULL argument");
@@ -578,7 +669,7 @@ int hfm_index_load(const uint8_t* bytes, size_t len, int kind, const hfm_opts* o
   if (dev < 0 || dev >= ndev) return set_error(HFM_E_ARG, "device ordinal out of range");
   CK(cudaSetDevice(dev));
   std::unique_ptr<hfm_index> x(new hfm_index());
-  x->device = dev; x->kind = kind;
+  x->device = dev; x->kind = kind; x->flags = opts ? opts->flags : 0;
   CK(cudaDeviceGetAttribute(&x->num_sms, cudaDevAttrMultiProcessorCount, dev));
   CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
   for (auto& e : x->ev) CK(cudaEventCreate(&e));
@@ -600,7 +691,8 @@ void hfm_index_free(hfm_index* x) {
                     &x->rev.bounds, &x->rev.compat, &x->q, &x->qoff, &x->counts, &x->nhits, &x->niv, &x->ivoff,
                     &x->status, &x->ovf, &x->ivpool, &x->hitpool, &x->seg_row, &x->seg_off, &x->pos_base,
                     &x->seg_base, &x->scan_tmp, &x->out_pairs, &x->ref_bounds, &x->hit_start, &x->hit_count,
-                    &x->hit_base, &x->hits, &x->npos_scan, &x->work, &x->cwork, &x->ctr, &x->mivpool, &x->bswork, &x->memwork})
+                    &x->hit_base, &x->hits, &x->npos_scan, &x->work, &x->cwork, &x->ctr, &x->mivpool, &x->bswork, &x->memwork,
+                    &x->hkeys, &x->hslot, &x->hflags, &x->huid, &x->urow, &x->ulen, &x->uoff, &x->uout})
     b->release();
   for (auto& e : x->ev) if (e) cudaEventDestroy(e);
   for (auto& e : x->evk) if (e) cudaEventDestroy(e);
@@ -672,7 +764,7 @@ int hfm_locate_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint
   RET(locate_device(x, x->q.as<uint8_t>(), x->qoff.as<uint64_t>(), nq, cap, &d));
   // one malloc block: struct | offsets | counts | pairs
   size_t bytes = sizeof(hfm_hits) + ((size_t)nq + 1) * 8 + (size_t)nq * 4 + 4 + (size_t)d.total * 8;
-  uint8_t* blk = (uint8_t*)std::malloc(bytes);
+  uint8_t* blk = (uint8_t*)host_result_alloc(bytes);
   if (!blk) return set_error(HFM_E_OOM, "host allocation failed");
   hfm_hits* h = (hfm_hits*)blk;
   h->nq = nq; h->_pad = 0; h->total = d.total;
@@ -683,7 +775,7 @@ int hfm_locate_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint
   if (d.total) CK(cudaMemcpyAsync(h->pairs, d.d_pairs, (size_t)d.total * 8, cudaMemcpyDeviceToHost, x->stream));
   if (nq) CK(cudaMemcpyAsync(h->counts, d.d_counts, (size_t)nq * 4, cudaMemcpyDeviceToHost, x->stream));
   cudaError_t e = cudaStreamSynchronize(x->stream);
-  if (e != cudaSuccess) { std::free(blk); return set_error(HFM_E_CUDA, cudaGetErrorString(e)); }
+  if (e != cudaSuccess) { host_result_free(blk); return set_error(HFM_E_CUDA, cudaGetErrorString(e)); }
   *out = h;
   return HFM_OK;
 }
@@ -698,7 +790,7 @@ int hfm_mems_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32
   RET(mems_device(x, x->q.as<uint8_t>(), x->qoff.as<uint64_t>(), nq, min_len, mode, ref_bounds, nb, cap, &d));
   size_t bytes = sizeof(hfm_mem_out) + ((size_t)nq + 1) * 8 + (size_t)d.n_hits * sizeof(hfm_mem_hit) +
                  (size_t)d.n_positions * 8 + 8;
-  uint8_t* blk = (uint8_t*)std::malloc(bytes);
+  uint8_t* blk = (uint8_t*)host_result_alloc(bytes);
   if (!blk) return set_error(HFM_E_OOM, "host allocation failed");
   hfm_mem_out* m = (hfm_mem_out*)blk;
   m->nq = nq; m->_pad = 0; m->n_hits = d.n_hits; m->n_positions = d.n_positions;
@@ -709,7 +801,7 @@ int hfm_mems_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32
   if (d.n_hits) CK(cudaMemcpyAsync(m->hits, d.d_hits, (size_t)d.n_hits * sizeof(hfm_mem_hit), cudaMemcpyDeviceToHost, x->stream));
   if (d.n_positions) CK(cudaMemcpyAsync(m->positions, d.d_positions, (size_t)d.n_positions * 8, cudaMemcpyDeviceToHost, x->stream));
   cudaError_t e = cudaStreamSynchronize(x->stream);
-  if (e != cudaSuccess) { std::free(blk); return set_error(HFM_E_CUDA, cudaGetErrorString(e)); }
+  if (e != cudaSuccess) { host_result_free(blk); return set_error(HFM_E_CUDA, cudaGetErrorString(e)); }
   *out = m;
   return HFM_OK;
 }

@@ -91,6 +91,99 @@ __global__ void __launch_bounds__(RES_T) k_resolve(DevFm F, ResolveArgs A) {
   if (COUNT) atomicAdd(A.steps, (unsigned long long)(steps + 1));
 }
 
+// ---- resolve deduplication ----------------------------------------------------------
+// Segments with the same (first row, length) resolve to the same positions: across a
+// batch, hits on repeated strings (N runs, repeat copies) share their SA interval.  The
+// segments are hashed, each distinct one is resolved once, and every hit copies its
+// positions from it.  Output is identical to resolving every row.
+
+constexpr unsigned long long HASH_EMPTY = ~0ull;
+
+__device__ __forceinline__ uint64_t mix64(uint64_t k) {      // splitmix64 finaliser
+  k ^= k >> 30; k *= 0xbf58476d1ce4e5b9ull; k ^= k >> 27; k *= 0x94d049bb133111ebull; k ^= k >> 31;
+  return k;
+}
+
+__global__ void k_dedup_insert(const uint32_t* __restrict__ seg_row, uint32_t stride, const uint64_t* __restrict__ seg_off,
+                               uint32_t nseg, unsigned long long* __restrict__ keys, uint64_t mask,
+                               uint32_t* __restrict__ seg_slot) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  uint64_t n = seg_off[s + 1] - seg_off[s];
+  if (n == 0) { seg_slot[s] = 0xFFFFFFFFu; return; }
+  unsigned long long key = ((unsigned long long)seg_row[(size_t)s * stride] << 32) | (uint32_t)n;
+  uint64_t h = mix64(key) & mask;
+  // the table has at least twice as many slots as segments: an empty slot is always found
+  for (uint64_t probe = 0; probe <= mask; probe++) {
+    unsigned long long prev = atomicCAS(keys + h, HASH_EMPTY, key);
+    if (prev == HASH_EMPTY || prev == key) { seg_slot[s] = (uint32_t)h; return; }
+    h = (h + 1) & mask;
+  }
+  seg_slot[s] = 0xFFFFFFFFu;    // unreachable with a half-empty table
+}
+
+__global__ void k_dedup_flags(const unsigned long long* __restrict__ keys, uint64_t size, uint32_t* __restrict__ flags) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < size) flags[i] = keys[i] != HASH_EMPTY;
+}
+
+__global__ void k_dedup_compact(const unsigned long long* __restrict__ keys, uint64_t size,
+                                const uint64_t* __restrict__ uid, uint32_t* __restrict__ urow,
+                                uint32_t* __restrict__ ulen) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= size) return;
+  unsigned long long k = keys[i];
+  if (k == HASH_EMPTY) return;
+  uint64_t u = uid[i];
+  urow[u] = (uint32_t)(k >> 32); ulen[u] = (uint32_t)k;
+}
+
+// out[p] = resolved position of its segment's distinct copy
+constexpr int EXP_T = 256;
+__global__ void __launch_bounds__(EXP_T) k_dedup_expand(const uint64_t* __restrict__ seg_off, uint32_t nseg, uint64_t total,
+                                                        const uint32_t* __restrict__ seg_slot,
+                                                        const uint64_t* __restrict__ uid,
+                                                        const uint64_t* __restrict__ uoff,
+                                                        const uint2* __restrict__ uout, uint2* __restrict__ out) {
+  __shared__ uint64_t s_off[EXP_T + 1];
+  __shared__ uint64_t s_src[EXP_T];
+  __shared__ uint32_t s_first, s_cnt;
+  uint64_t p0 = (uint64_t)blockIdx.x * EXP_T;
+  uint64_t p1 = min(p0 + EXP_T, total);
+  if (threadIdx.x == 0) {
+    uint32_t lo = 0, hi = nseg;
+    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (seg_off[mid] <= p0) lo = mid; else hi = mid - 1; }
+    uint32_t first = lo;
+    hi = nseg;
+    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (seg_off[mid] <= p1 - 1) lo = mid; else hi = mid - 1; }
+    s_first = first; s_cnt = lo - first + 1;
+  }
+  __syncthreads();
+  uint32_t first = s_first, cnt = s_cnt;
+  bool local = cnt <= EXP_T;
+  if (local) {
+    for (uint32_t k = threadIdx.x; k <= cnt; k += EXP_T) s_off[k] = seg_off[first + k];
+    for (uint32_t k = threadIdx.x; k < cnt; k += EXP_T) {
+      uint32_t slot = seg_slot[first + k];
+      s_src[k] = slot == 0xFFFFFFFFu ? 0 : uoff[uid[slot]];
+    }
+  }
+  __syncthreads();
+  uint64_t p = p0 + threadIdx.x;
+  if (p >= p1) return;
+  uint64_t src;
+  if (local) {
+    uint32_t lo = 0, hi = cnt - 1;
+    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (s_off[mid] <= p) lo = mid; else hi = mid - 1; }
+    src = s_src[lo] + (p - s_off[lo]);
+  } else {
+    uint32_t lo = first, hi = nseg - 1;
+    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (seg_off[mid] <= p) lo = mid; else hi = mid - 1; }
+    src = uoff[uid[seg_slot[lo]]] + (p - seg_off[lo]);
+  }
+  out[p] = uout[src];
+}
+
 // ---- exclusive scan (u32 or u64 input) -> u64 output with out[n] = total ----------
 constexpr int SCAN_T = 256, SCAN_ITEMS = 8, SCAN_TILE = SCAN_T * SCAN_ITEMS;
 

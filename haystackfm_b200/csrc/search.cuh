@@ -126,8 +126,9 @@ __device__ __forceinline__ uint32_t backward_search_one(const DevFm& F, const Sm
     mask &= F.sym_mask;                   // symbol_count(r) == 0 -> skipped
     if (!mask) return 0;
     uint32_t nn = 0;
-    for (uint32_t i = 0; i < n; i++) {
-      uint2 iv = cur[i];
+    if (n == 1) {
+      // one source interval: symbol order is already ascending row order
+      uint2 iv = cur[0];
       uint32_t rl[16], rh[16];
       sym_ranks(F, S, iv.x, rl);
       sym_ranks(F, S, iv.y, rh);
@@ -137,6 +138,43 @@ __device__ __forceinline__ uint32_t backward_search_one(const DevFm& F, const Sm
         if (!((mask >> r) & 1)) continue;
         uint32_t nl = S.C[r] + rl[r], nh = S.C[r] + rh[r];
         if (nl < nh && !iv_insert(nxt, nn, cap, nl, nh)) return ~0u;
+      }
+    } else {
+      // Outputs for symbol r lie in [C[r], C[r+1]) in source order, so a stable counting
+      // sort by symbol yields ascending rows: count per symbol, then place.
+      uint32_t cnt[16];
+#pragma unroll
+      for (int r = 0; r < 16; r++) cnt[r] = 0;
+      for (uint32_t i = 0; i < n; i++) {
+        uint2 iv = cur[i];
+        uint32_t rl[16], rh[16];
+        sym_ranks(F, S, iv.x, rl);
+        sym_ranks(F, S, iv.y, rh);
+        if (COUNT_TOUCH) touches += (iv.x != 0) + (iv.y != 0);
+#pragma unroll
+        for (int r = 0; r < 16; r++) cnt[r] += (((mask >> r) & 1) && rh[r] > rl[r]) ? 1u : 0u;
+      }
+      uint32_t total = 0;
+#pragma unroll
+      for (int r = 0; r < 16; r++) { uint32_t t = cnt[r]; cnt[r] = total; total += t; }
+      if (total > cap) return ~0u;
+      for (uint32_t i = 0; i < n; i++) {
+        uint2 iv = cur[i];
+        uint32_t rl[16], rh[16];
+        sym_ranks(F, S, iv.x, rl);
+        sym_ranks(F, S, iv.y, rh);
+#pragma unroll
+        for (int r = 0; r < 16; r++)
+          if (((mask >> r) & 1) && rh[r] > rl[r]) nxt[cnt[r]++] = make_uint2(S.C[r] + rl[r], S.C[r] + rh[r]);
+      }
+      // coalesce touching neighbours (merge_intervals_inplace, query.rs:390-407)
+      for (uint32_t e = 0; e < total; e++) {
+        uint2 v = nxt[e];
+        if (nn > 0) {
+          uint2 last = nxt[nn - 1];
+          if (v.x <= last.y) { nxt[nn - 1] = make_uint2(last.x, max(last.y, v.y)); continue; }
+        }
+        nxt[nn++] = v;
       }
     }
     if (nn == 0) return 0;

@@ -99,10 +99,10 @@ def _build(sequences: Sequence[DnaSequence], config: FmIndexConfig, tag: int, ki
 class _Handle:
     """Owns one device-resident index (hfm_index*)."""
 
-    def __init__(self, data: bytes, kind: int, device: int = 0):
+    def __init__(self, data: bytes, kind: int, device: int = 0, flags: int = 0):
         self._buf = np.frombuffer(data, dtype=np.uint8)
         h = C.c_void_p()
-        opts = L.HfmOpts(device, 0)
+        opts = L.HfmOpts(device, flags)
         L.check(L.lib().hfm_index_load(L.ptr(self._buf, L.u8p), len(data), kind, C.byref(opts), C.byref(h)))
         self.h = h
         self.kind = kind

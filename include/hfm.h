@@ -40,9 +40,12 @@ extern "C" {
 
 typedef struct hfm_index hfm_index;   /* device-resident index, opaque */
 
+#define HFM_FLAG_DEDUP_ALWAYS 1u  /* resolve repeated SA intervals once per call, always      */
+#define HFM_FLAG_DEDUP_NEVER 2u   /* never deduplicate (default: when hits average >= 4 rows) */
+
 typedef struct hfm_opts {
   int32_t device;          /* CUDA device ordinal (one index per GPU; replicate for multi-GPU) */
-  uint32_t flags;          /* reserved, 0 */
+  uint32_t flags;          /* HFM_FLAG_* (0 = defaults)                                        */
 } hfm_opts;
 
 typedef struct hfm_index_info {
@@ -95,6 +98,7 @@ typedef struct hfm_stats {
   uint64_t lf_calls;         /* LF-walk iterations of the resolve kernel (Occ + SA-marker touch each) */
   uint64_t rows_resolved;    /* positions resolved (one sa_vals read and one output pair each) */
   uint64_t hits_out;         /* MEM hit records written                                   */
+  uint64_t rows_unique;      /* distinct rows walked after deduplication (0: no dedup)     */
 } hfm_stats;
 
 /* ---- index construction (replaces FmIndex::build_cpu_with + to_bytes,

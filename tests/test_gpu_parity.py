@@ -196,3 +196,27 @@ def test_python_api_mirror(oracle):
     again = BidirFmIndex.from_bytes(bd.to_bytes())
     assert again.find_smems_gpu([al.DnaSequence.from_str("CGTA")], 1, again.seq_boundaries()) == \
         bd.find_smems_gpu([al.DnaSequence.from_str("CGTA")], 1, bd.seq_boundaries())
+
+
+def test_resolve_dedup_paths_identical(oracle):
+    """Deduplicated and plain resolve give the same bytes (repeated intervals across reads)."""
+    from haystackfm_b200._lib import HFM_FLAG_DEDUP_ALWAYS, HFM_FLAG_DEDUP_NEVER
+    ref = synth.iupac_reference(total=400_000, n_contigs=10, seed=21)
+    reads = synth.sample_reads(ref, n_reads=300, seed=22)
+    b = _build([al.DnaSequence(c) for c in ref.contigs], FmIndexConfig(sa_sample_rate=16, lookup_depth=6), 0,
+               KIND_BIDIR)
+    o = oracle.OracleIndex(b, KIND_BIDIR)
+    flat, off = synth.pack_rows(reads)
+    flat32, off32 = synth.pack_rows(reads, 24)
+    _, _, _, bounds = None, None, None, o and __import__("haystackfm_b200.fm_index", fromlist=["x"])._header_fields(b, 4)[2]
+    want_m = o.mems_packed(flat, off, 15, 0, bounds, 300)
+    want_l = o.locate_packed(flat32, off32, 50)
+    for flags in (HFM_FLAG_DEDUP_ALWAYS, HFM_FLAG_DEDUP_NEVER, 0):
+        h = _Handle(b, KIND_BIDIR, 0, flags)
+        for _ in range(2):       # repeated calls on one handle reuse its buffers
+            got = h.mems_packed(flat, off, 15, 0, bounds, 300)
+            for g, w in zip(got, want_m):
+                assert np.array_equal(g, w)
+            got = h.locate_packed(flat32, off32, 50)
+            for g, w in zip(got, want_l):
+                assert np.array_equal(g, w)
