@@ -208,7 +208,8 @@ def test_resolve_dedup_paths_identical(oracle):
     o = oracle.OracleIndex(b, KIND_BIDIR)
     flat, off = synth.pack_rows(reads)
     flat32, off32 = synth.pack_rows(reads, 24)
-    _, _, _, bounds = None, None, None, o and __import__("haystackfm_b200.fm_index", fromlist=["x"])._header_fields(b, 4)[2]
+    from haystackfm_b200.fm_index import _header_fields
+    bounds = _header_fields(b, 4)[2]
     want_m = o.mems_packed(flat, off, 15, 0, bounds, 300)
     want_l = o.locate_packed(flat32, off32, 50)
     for flags in (HFM_FLAG_DEDUP_ALWAYS, HFM_FLAG_DEDUP_NEVER, 0):
