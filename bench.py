@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--e2e-chunk", type=int, default=250_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
 
@@ -267,11 +268,15 @@ def main():
     k_bs_ms = statistics.mean(s1.ms_search_kernel for s1, *_ in per)
     k_res_loc_ms = statistics.mean(s1.ms_resolve_kernel for s1, *_ in per)
     # algorithmic bytes (32 B per random Occ / SA-marker / sa_vals / lookup touch, read bytes,
-    # 8 B per output position, 16 B per MEM hit header)
+    # 8 B per output position, 16 B per MEM hit header).  The resolve kernel walks each
+    # distinct SA row once (rows_unique after deduplication); copying the positions to every
+    # hit is a separate streaming kernel.
+    def rows_walked(c):
+        return c.rows_unique if c.rows_unique else c.rows_resolved
     b_mems = 32 * c_mem.occ_touches + 150 * n + 16 * c_mem.hits_out
-    b_res_mem = 32 * (2 * c_mem.lf_calls + c_mem.rows_resolved) + 8 * c_mem.rows_resolved
+    b_res_mem = 32 * (2 * c_mem.lf_calls + rows_walked(c_mem)) + 8 * rows_walked(c_mem)
     b_bs = 32 * c_loc.occ_touches + 32 * n
-    b_res_loc = 32 * (2 * c_loc.lf_calls + c_loc.rows_resolved) + 8 * c_loc.rows_resolved
+    b_res_loc = 32 * (2 * c_loc.lf_calls + rows_walked(c_loc)) + 8 * rows_walked(c_loc)
     kern = {"k_mems": (k_mems_ms, b_mems, c_mem.occ_touches, "Occ touches"),
             "k_resolve(smem)": (k_res_mem_ms, b_res_mem, c_mem.lf_calls, "LF steps"),
             "k_bsearch": (k_bs_ms, b_bs, c_loc.occ_touches, "Occ touches"),
@@ -329,18 +334,20 @@ def main():
             h2d += m * 32 + (m + 1) * 8 + m * 150 + (m + 1) * 8 + nb * 4
         return h2d, d2h
 
-    e2e_step()
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        h2d, d2h = e2e_step()
-    e2e_s = time.perf_counter() - t0
+    e2e_s, h2d, d2h = 0.0, 0, 0
+    if not args.no_e2e:
+        e2e_step()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            h2d, d2h = e2e_step()
+        e2e_s = time.perf_counter() - t0
     if dist:
         t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = {"value": world * n * args.steps / e2e_s, "unit": "reads/s", "h2d_bytes_per_step": int(h2d),
+    e2e = {"value": world * n * args.steps / e2e_s if e2e_s else None, "unit": "reads/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "chunk_reads": ch}
 
     cpu = None
@@ -361,6 +368,7 @@ def main():
                        "l2": "no flush: index (0.7 GB device layout) + reads (150 MB) + outputs exceed the 126 MB L2",
                        "index_build_s": round(build_s, 1), "index_cached": not built,
                        "locate_positions": int(loc_total), "mem_hits": int(n_hits), "mem_positions": int(n_pos),
+                       "distinct_rows_walked": int(rows_walked(c_mem) + rows_walked(c_loc)),
                        "parallelism": f"replicas{world}" if world > 1 else "single"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk,
