@@ -110,7 +110,7 @@ struct hfm_index {
   // per-call work buffers (grow-only)
   DevBuf q, qoff, counts, nhits, niv, ivoff, status, ovf, ivpool, hitpool, seg_row, seg_off, pos_base, seg_base,
       scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr,
-      mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout;
+      mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout, blockmap, blockmap2;
   uint32_t flags = 0;
   int num_sms = 0;
   uint64_t iv_cap = 0, miv_cap = 0, hit_cap = 0;   // pool capacities in elements (uint2 / BIv / hit)
@@ -230,8 +230,10 @@ static int read_u64(hfm_index* x, const uint64_t* dsrc, uint64_t& v) {
   return HFM_OK;
 }
 
-static constexpr uint32_t BS_SET_CAP = 256;    // fast-path interval-set capacity (backward search)
+static constexpr uint32_t BS_SET_CAP = 64;     // fast-path interval-set capacity (backward search)
+static constexpr uint32_t BS_WARP_SET_CAP = 8192;   // long-tail pass, per warp
 static constexpr uint32_t MEM_SET_CAP = 768;   // fast-path interval-set capacity (SMEM / MEM)
+static constexpr uint32_t MEM_WARP_SET_CAP = 8192;  // long-tail pass, per warp
 static constexpr int MEM_KC = 32;              // fast-path candidate capacity (thread-local)
 
 // Backward search for a batch.  with_ivs = false: counts only.
@@ -277,27 +279,25 @@ static int run_bsearch(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
     RET(read_ctr(x));
     uint32_t n_ovf = x->h_ctr->n_ovf;
     if (n_ovf) {
-      // fallback pass over the overflowed queries: contiguous per-thread sets, 16x larger,
-      // growing 4x until every query fits
-      uint32_t set_cap = BS_SET_CAP * 16;
+      // long tail: one warp per overflowed query, sets in per-warp global regions, growing
+      // 4x until every query fits
+      uint32_t set_cap = BS_WARP_SET_CAP;
       while (true) {
-        uint64_t per_thread = (uint64_t)set_cap * 2 * 8;
-        uint32_t nthr = (uint32_t)std::max<uint64_t>(32, std::min<uint64_t>((uint64_t)n_ovf, (2ull << 30) / per_thread));
-        // every launched thread may take a read from the queue: size for the whole grid
-        nthr = (uint32_t)std::min<uint64_t>((nthr + 127) / 128 * 128, std::max<uint64_t>(threads, 128));
-        RET(x->work.ensure((size_t)nthr * per_thread));
+        uint64_t per_warp = (uint64_t)set_cap * 2 * 8;
+        uint64_t warps = std::min<uint64_t>({(uint64_t)n_ovf, (uint64_t)x->num_sms * 16,
+                                             std::max<uint64_t>(4, (2ull << 30) / per_warp)});
+        unsigned grid = (unsigned)((warps + 3) / 4);
+        RET(x->work.ensure((size_t)grid * 4 * per_warp));
         CK(cudaMemsetAsync(&dctr(x)->still_ovf, 0, 4, x->stream));
         CK(cudaMemsetAsync(&dctr(x)->queue2, 0, 4, x->stream));
-        unsigned grid = (nthr + 127) / 128;
-        if (x->work.cap < (size_t)grid * 128 * per_thread) return set_error(HFM_E_ARG, "internal: fallback work area too small");
         if (x->count_work)
-          k_bsearch<true, 1><<<grid, 128, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>(),
-                                                         n_ovf, cap, x->work.as<uint2>(), set_cap, &dctr(x)->queue2, pool,
-                                                         o, &dctr(x)->still_ovf);
+          k_bsearch_warp<true><<<grid, 128, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>(),
+                                                           n_ovf, cap, x->work.as<uint2>(), set_cap, &dctr(x)->queue2, pool,
+                                                           o, &dctr(x)->still_ovf);
         else
-          k_bsearch<false, 1><<<grid, 128, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>(),
-                                                          n_ovf, cap, x->work.as<uint2>(), set_cap, &dctr(x)->queue2, pool,
-                                                          o, &dctr(x)->still_ovf);
+          k_bsearch_warp<false><<<grid, 128, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, x->ovf.as<uint32_t>(),
+                                                            n_ovf, cap, x->work.as<uint2>(), set_cap, &dctr(x)->queue2, pool,
+                                                            o, &dctr(x)->still_ovf);
         launches++;
         CK(cudaGetLastError());
         RET(read_ctr(x));
@@ -323,9 +323,12 @@ static int resolve(hfm_index* x, const FmDev& F, const uint32_t* seg_row, uint32
                    uint32_t& launches) {
   if (total == 0) return HFM_OK;
   if (nseg >= 0xFFFFFFFFull) return set_error(HFM_E_ARG, "too many intervals in one call");
-  ResolveArgs A{seg_row, stride, seg_off, (uint32_t)nseg, total, d_bounds, nb,
-                F.rate ? F.rate : F.text_len, out, &dctr(x)->walk_err, &dctr(x)->steps};
   uint64_t blocks = (total + RES_T - 1) / RES_T;
+  RET(x->blockmap.ensure(blocks * 4 + 4));
+  k_block_first<<<(unsigned)((nseg + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)nseg, RES_T,
+                                                                     x->blockmap.as<uint32_t>());
+  ResolveArgs A{seg_row, stride, seg_off, (uint32_t)nseg, total, d_bounds, nb,
+                F.rate ? F.rate : F.text_len, out, &dctr(x)->walk_err, &dctr(x)->steps, x->blockmap.as<uint32_t>()};
   // grid.x limit 2^31-1 blocks covers 5e11 positions
   cudaEventRecord(x->evk[2], x->stream);
   if (x->count_work) k_resolve<true><<<(unsigned)blocks, RES_T, 0, x->stream>>>(F.d, A);
@@ -372,10 +375,13 @@ static int resolve_segments(hfm_index* x, const FmDev& F, const uint32_t* seg_ro
   RET(x->uout.ensure(utotal * 8 + 8));
   RET(resolve(x, F, x->urow.as<uint32_t>(), 1, x->uoff.as<uint64_t>(), nuniq, utotal, d_bounds, nb,
               x->uout.as<uint32_t>(), launches));
+  RET(x->blockmap2.ensure(((total + EXP_T - 1) / EXP_T) * 4 + 4));
+  k_block_first<<<(unsigned)((nseg + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)nseg, EXP_T,
+                                                                     x->blockmap2.as<uint32_t>());
   k_dedup_expand<<<(unsigned)((total + EXP_T - 1) / EXP_T), EXP_T, 0, x->stream>>>(
       seg_off, (uint32_t)nseg, total, x->hslot.as<uint32_t>(), x->huid.as<uint64_t>(), x->uoff.as<uint64_t>(),
-      x->uout.as<uint2>(), reinterpret_cast<uint2*>(out));
-  other++;
+      x->uout.as<uint2>(), reinterpret_cast<uint2*>(out), x->blockmap2.as<uint32_t>());
+  other += 2;
   CK(cudaGetLastError());
   x->stats.rows_unique += utotal;
   return HFM_OK;
@@ -499,28 +505,26 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
     RET(read_ctr(x));
     uint32_t n_ovf = x->h_ctr->n_ovf;
     if (n_ovf) {
-      // fallback pass: contiguous per-thread sets and candidate lists, growing 4x
-      uint32_t set_cap = MEM_SET_CAP * 8, cand_cap = 256;
+      // long tail: one warp per overflowed read, 4 sets and a candidate list per warp,
+      // growing 4x until every read fits
+      uint32_t set_cap = MEM_WARP_SET_CAP, cand_cap = 1024;
       while (true) {
-        uint64_t per_thread = (uint64_t)set_cap * 4 * 16 + (uint64_t)cand_cap * sizeof(Cand);
-        uint32_t nthr = (uint32_t)std::max<uint64_t>(32, std::min<uint64_t>((uint64_t)n_ovf, (2ull << 30) / per_thread));
-        // every launched thread may take a read from the queue: size for the whole grid
-        nthr = (uint32_t)std::min<uint64_t>((nthr + 127) / 128 * 128, std::max<uint64_t>(threads, 128));
-        RET(x->work.ensure((size_t)nthr * set_cap * 4 * 16));
-        RET(x->cwork.ensure((size_t)nthr * cand_cap * sizeof(Cand)));
+        uint64_t per_warp = (uint64_t)set_cap * 4 * 16 + (uint64_t)cand_cap * sizeof(Cand);
+        uint64_t warps = std::min<uint64_t>({(uint64_t)n_ovf, (uint64_t)x->num_sms * 16,
+                                             std::max<uint64_t>(4, (2ull << 30) / per_warp)});
+        unsigned grid = (unsigned)((warps + 3) / 4);
+        RET(x->work.ensure((size_t)grid * 4 * set_cap * 4 * 16));
+        RET(x->cwork.ensure((size_t)grid * 4 * cand_cap * sizeof(Cand)));
         CK(cudaMemsetAsync(&dctr(x)->still_ovf, 0, 4, x->stream));
         CK(cudaMemsetAsync(&dctr(x)->queue2, 0, 4, x->stream));
         MemsWork W{x->work.as<BIv>(), set_cap, x->cwork.as<Cand>(), cand_cap, &dctr(x)->queue2, x->ovf.as<uint32_t>(),
                    n_ovf, &dctr(x)->still_ovf};
-        unsigned grid = (nthr + 127) / 128;
-        if (x->work.cap < (size_t)grid * 128 * set_cap * 4 * 16 || x->cwork.cap < (size_t)grid * 128 * cand_cap * sizeof(Cand))
-          return set_error(HFM_E_ARG, "internal: fallback work area too small");
         if (x->count_work)
-          k_mems<true, 1, 0><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                         d_q, d_qoff, P, ivp, hp, o, W);
+          k_mems_warp<true><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                        d_q, d_qoff, P, ivp, hp, o, W);
         else
-          k_mems<false, 1, 0><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                          d_q, d_qoff, P, ivp, hp, o, W);
+          k_mems_warp<false><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                         d_q, d_qoff, P, ivp, hp, o, W);
         launches++;
         CK(cudaGetLastError());
         RET(read_ctr(x));
@@ -692,7 +696,8 @@ void hfm_index_free(hfm_index* x) {
                     &x->status, &x->ovf, &x->ivpool, &x->hitpool, &x->seg_row, &x->seg_off, &x->pos_base,
                     &x->seg_base, &x->scan_tmp, &x->out_pairs, &x->ref_bounds, &x->hit_start, &x->hit_count,
                     &x->hit_base, &x->hits, &x->npos_scan, &x->work, &x->cwork, &x->ctr, &x->mivpool, &x->bswork, &x->memwork,
-                    &x->hkeys, &x->hslot, &x->hflags, &x->huid, &x->urow, &x->ulen, &x->uoff, &x->uout})
+                    &x->hkeys, &x->hslot, &x->hflags, &x->huid, &x->urow, &x->ulen, &x->uoff, &x->uout,
+                    &x->blockmap, &x->blockmap2})
     b->release();
   for (auto& e : x->ev) if (e) cudaEventDestroy(e);
   for (auto& e : x->evk) if (e) cudaEventDestroy(e);

@@ -23,7 +23,27 @@ struct ResolveArgs {
   uint32_t* out;                // 2 * total u32
   uint32_t* walk_err;
   unsigned long long* steps;    // LF steps (nullptr: not counted)
+  const uint32_t* block_first;  // segment containing the first position of each block
 };
+
+// block_first[b] = segment holding position b * blk (positions are CSR over segments).
+__global__ void k_block_first(const uint64_t* __restrict__ seg_off, uint32_t nseg, uint32_t blk,
+                              uint32_t* __restrict__ block_first) {
+  uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseg) return;
+  uint64_t a = seg_off[s], e = seg_off[s + 1];
+  if (a == e) return;
+  for (uint64_t b = (a + blk - 1) / blk; b <= (e - 1) / blk; b++) block_first[b] = s;
+}
+
+// Segments [first, first + cnt) cover positions [b * blk, (b + 1) * blk) of block b.
+__device__ __forceinline__ void block_segments(const uint32_t* block_first, uint64_t nblocks, uint32_t nseg,
+                                               uint32_t& first, uint32_t& cnt) {
+  uint64_t b = blockIdx.x;
+  first = block_first[b];
+  uint32_t last = b + 1 < nblocks ? block_first[b + 1] : nseg - 1;
+  cnt = last - first + 1;
+}
 
 constexpr int RES_T = 256;
 constexpr int RES_BOUNDS_SMEM = 2048;
@@ -39,13 +59,9 @@ __global__ void __launch_bounds__(RES_T) k_resolve(DevFm F, ResolveArgs A) {
   uint64_t p0 = (uint64_t)blockIdx.x * RES_T;
   uint64_t p1 = min(p0 + RES_T, A.total);
   if (threadIdx.x == 0) {
-    // segment containing p0 / p1-1: last k with seg_off[k] <= p
-    uint32_t lo = 0, hi = A.nseg;
-    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (A.seg_off[mid] <= p0) lo = mid; else hi = mid - 1; }
-    uint32_t first = lo;
-    hi = A.nseg;
-    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (A.seg_off[mid] <= p1 - 1) lo = mid; else hi = mid - 1; }
-    s_first = first; s_cnt = lo - first + 1;
+    uint32_t f, c;
+    block_segments(A.block_first, (A.total + RES_T - 1) / RES_T, A.nseg, f, c);
+    s_first = f; s_cnt = c;
   }
   bool smem_b = A.nb <= RES_BOUNDS_SMEM;
   if (smem_b) for (uint32_t k = threadIdx.x; k < A.nb; k += RES_T) s_b[k] = A.bounds[k];
@@ -144,19 +160,17 @@ __global__ void __launch_bounds__(EXP_T) k_dedup_expand(const uint64_t* __restri
                                                         const uint32_t* __restrict__ seg_slot,
                                                         const uint64_t* __restrict__ uid,
                                                         const uint64_t* __restrict__ uoff,
-                                                        const uint2* __restrict__ uout, uint2* __restrict__ out) {
+                                                        const uint2* __restrict__ uout, uint2* __restrict__ out,
+                                                        const uint32_t* __restrict__ block_first) {
   __shared__ uint64_t s_off[EXP_T + 1];
   __shared__ uint64_t s_src[EXP_T];
   __shared__ uint32_t s_first, s_cnt;
   uint64_t p0 = (uint64_t)blockIdx.x * EXP_T;
   uint64_t p1 = min(p0 + EXP_T, total);
   if (threadIdx.x == 0) {
-    uint32_t lo = 0, hi = nseg;
-    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (seg_off[mid] <= p0) lo = mid; else hi = mid - 1; }
-    uint32_t first = lo;
-    hi = nseg;
-    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (seg_off[mid] <= p1 - 1) lo = mid; else hi = mid - 1; }
-    s_first = first; s_cnt = lo - first + 1;
+    uint32_t f, c;
+    block_segments(block_first, (total + EXP_T - 1) / EXP_T, nseg, f, c);
+    s_first = f; s_cnt = c;
   }
   __syncthreads();
   uint32_t first = s_first, cnt = s_cnt;

@@ -500,3 +500,357 @@ __global__ void __launch_bounds__(128) k_mems(DevFm Fw, DevFm Rv, const uint16_t
 }
 
 }  // namespace hfm
+
+// =====================================================================================
+// Warp-cooperative long-tail pass: one warp per read, the 32 lanes share the interval set
+// of every step (reads whose sets outgrow the per-thread fast path: ambiguity codes near
+// the start of a read, unseeded patterns inside N runs).  Same results as the per-thread
+// code; sets live in a per-warp global region.
+// =====================================================================================
+namespace hfm {
+
+__device__ __forceinline__ uint32_t lane_lt_mask() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+__device__ __forceinline__ uint32_t warp_sum(uint32_t v) {
+#pragma unroll
+  for (int d = 16; d > 0; d >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, d);
+  return v;
+}
+__device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, uint32_t& total) {
+  const int lane = threadIdx.x & 31;
+  uint32_t x = v;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) { uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d); if (lane >= d) x += y; }
+  total = __shfl_sync(0xFFFFFFFFu, x, 31);
+  return x - v;
+}
+
+// Backward-search step set (sorted, coalesced) with the warp: counting sort by symbol
+// (pass 1 counts with ballots, pass 2 places), then lane 0 coalesces touching neighbours.
+template <bool COUNT_TOUCH>
+__device__ uint32_t warp_backward_search(const DevFm& F, const SmemFm& S, const uint8_t* p, uint32_t m,
+                                         uint2*& cur, uint2*& nxt, uint32_t cap, uint64_t& touches) {
+  const int lane = threadIdx.x & 31;
+  cur[0] = make_uint2(0, F.text_len);
+  if (m == 0) return 1;
+  uint32_t n = 1, start = m;
+  if (F.lut && m >= F.lut_depth) {
+    uint64_t idx = 0; bool ok = true;
+    for (int k = (int)F.lut_depth - 1; k >= 0; --k) {
+      uint8_t c = p[m - F.lut_depth + k];
+      uint32_t d = c < 16 ? S.dig[c] : 0xFF;
+      if (d == 0xFF) { ok = false; break; }
+      idx = idx * F.lut_radix + d;
+    }
+    if (ok) {
+      uint2 iv = __ldg(F.lut + idx);
+      if (COUNT_TOUCH && lane == 0) touches++;
+      if (iv.x >= iv.y) return 0;
+      if (lane == 0) cur[0] = iv;
+      start = m - F.lut_depth;
+    }
+  }
+  __syncwarp();
+  for (uint32_t k = start; k-- > 0;) {
+    uint8_t c = p[k];
+    uint32_t mask = (c < 16 ? S.compat_mask[c] : 0) & F.sym_mask;
+    if (!mask) return 0;
+    uint32_t cnt[16];
+#pragma unroll
+    for (int r = 0; r < 16; r++) cnt[r] = 0;
+    for (uint32_t b = 0; b < n; b += 32) {
+      uint32_t i = b + lane;
+      uint32_t rl[16], rh[16];
+      uint2 iv = i < n ? cur[i] : make_uint2(0, 0);
+      sym_ranks(F, S, iv.x, rl);
+      sym_ranks(F, S, iv.y, rh);
+      if (COUNT_TOUCH && i < n) touches += (iv.x != 0) + (iv.y != 0);
+#pragma unroll
+      for (int r = 0; r < 16; r++) cnt[r] += __popc(__ballot_sync(0xFFFFFFFFu, i < n && ((mask >> r) & 1) && rh[r] > rl[r]));
+    }
+    uint32_t total = 0;
+#pragma unroll
+    for (int r = 0; r < 16; r++) { uint32_t t = cnt[r]; cnt[r] = total; total += t; }
+    if (total > cap) return ~0u;
+    if (total == 0) return 0;
+    for (uint32_t b = 0; b < n; b += 32) {
+      uint32_t i = b + lane;
+      uint32_t rl[16], rh[16];
+      uint2 iv = i < n ? cur[i] : make_uint2(0, 0);
+      sym_ranks(F, S, iv.x, rl);
+      sym_ranks(F, S, iv.y, rh);
+#pragma unroll
+      for (int r = 0; r < 16; r++) {
+        bool e = i < n && ((mask >> r) & 1) && rh[r] > rl[r];
+        uint32_t bal = __ballot_sync(0xFFFFFFFFu, e);
+        if (e) nxt[cnt[r] + __popc(bal & lane_lt_mask())] = make_uint2(S.C[r] + rl[r], S.C[r] + rh[r]);
+        cnt[r] += __popc(bal);
+      }
+    }
+    __syncwarp();
+    uint32_t nn = 0;
+    if (lane == 0) {   // coalesce touching neighbours (merge_intervals_inplace, query.rs:390-407)
+      for (uint32_t e = 0; e < total; e++) {
+        uint2 v = nxt[e];
+        if (nn > 0) { uint2 last = nxt[nn - 1]; if (v.x <= last.y) { nxt[nn - 1] = make_uint2(last.x, max(last.y, v.y)); continue; } }
+        nxt[nn++] = v;
+      }
+    }
+    nn = __shfl_sync(0xFFFFFFFFu, nn, 0);
+    __syncwarp();
+    uint2* t = cur; cur = nxt; nxt = t; n = nn;
+  }
+  return n;
+}
+
+template <bool COUNT_TOUCH>
+__global__ void __launch_bounds__(128) k_bsearch_warp(DevFm F, const uint16_t* __restrict__ compat_masks,
+                                                     const uint8_t* __restrict__ q, const uint64_t* __restrict__ qoff,
+                                                     const uint32_t* __restrict__ ids, uint32_t n, uint32_t hit_cap,
+                                                     uint2* work, uint32_t set_cap, unsigned int* queue, Pool pool,
+                                                     BsOut out, uint32_t* still_ovf) {
+  __shared__ SmemFm S;
+  smem_fm_init(S, F, compat_masks);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  uint2* A = work + warp * 2 * set_cap;
+  uint2* B = A + set_cap;
+  uint64_t touches = 0;
+  for (;;) {
+    uint32_t k = 0;
+    if (lane == 0) k = atomicAdd(queue, 1u);
+    k = __shfl_sync(0xFFFFFFFFu, k, 0);
+    if (k >= n) break;
+    uint32_t i = ids[k];
+    uint2* cur = A; uint2* nxt = B;
+    uint64_t o = qoff[i];
+    uint32_t niv = warp_backward_search<COUNT_TOUCH>(F, S, q + o, (uint32_t)(qoff[i + 1] - o), cur, nxt, set_cap, touches);
+    if (niv == ~0u) {
+      if (lane == 0) { atomicAdd(still_ovf, 1u); out.status[i] = ST_SET_OVF; }
+      continue;
+    }
+    uint32_t cnt = 0; uint64_t hits = 0;
+    for (uint32_t b = lane; b < niv; b += 32) {
+      uint2 v = cur[b]; uint32_t sz = v.y - v.x;
+      cnt += sz; hits += (hit_cap && sz > hit_cap) ? hit_cap : sz;
+    }
+    cnt = warp_sum(cnt);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) hits += __shfl_xor_sync(0xFFFFFFFFu, hits, d);
+    uint64_t off = 0; uint32_t st = ST_OK;
+    if (out.nhits && niv) {
+      if (lane == 0) off = thread_reserve(pool, niv);
+      off = __shfl_sync(0xFFFFFFFFu, off, 0);
+      if (off == ~0ull) st = ST_POOL_OVF;
+      else { uint2* dst = (uint2*)pool.base + off; for (uint32_t b = lane; b < niv; b += 32) dst[b] = cur[b]; }
+    }
+    if (lane == 0) {
+      out.counts[i] = cnt;
+      if (out.nhits) { out.nhits[i] = hits; out.niv[i] = niv; out.ivoff[i] = off; }
+      out.status[i] = st;
+    }
+    __syncwarp();
+  }
+  if (COUNT_TOUCH && touches) atomicAdd(out.touches, (unsigned long long)touches);
+}
+
+// One extension of the whole set by the warp (outputs in lane-chunk order).
+template <int DIR, bool COUNT_TOUCH>
+__device__ uint32_t warp_extend_set(const DevFm& X, const SmemFm& S, uint32_t mask, const BIv* in, uint32_t nin,
+                                    BIv* out, uint32_t cap, uint32_t& cov, bool& ovf, uint64_t& touches) {
+  const int lane = threadIdx.x & 31;
+  uint32_t nout = 0, covl = 0;
+  for (uint32_t b = 0; b < nin; b += 32) {
+    uint32_t i = b + lane;
+    BIv iv = i < nin ? in[i] : BIv{0, 0, 0, 0};
+    uint32_t a = DIR == 0 ? iv.rlo : iv.flo, e = DIR == 0 ? iv.rhi : iv.fhi;
+    uint32_t base = DIR == 0 ? iv.flo : iv.rlo;
+    uint32_t rl[16], rh[16];
+    sym_ranks(X, S, a, rl);
+    sym_ranks(X, S, e, rh);
+    if (COUNT_TOUCH && i < nin) touches += (a != 0) + (e != 0);
+    uint32_t k = 0;
+#pragma unroll
+    for (int s = 0; s < 16; s++) k += (i < nin && ((mask >> s) & 1) && rh[s] > rl[s]) ? 1u : 0u;
+    uint32_t total;
+    uint32_t pos = nout + warp_excl_scan(k, total);
+    if (nout + total > cap) { ovf = true; return nout; }
+    uint32_t run = 0;
+#pragma unroll
+    for (int s = 0; s < 16; s++) {
+      uint32_t d = rh[s] - rl[s];
+      if (i < nin && ((mask >> s) & 1) && d) {
+        BIv o;
+        if (DIR == 0) { o.flo = base + run; o.fhi = base + run + d; o.rlo = S.C[s] + rl[s]; o.rhi = S.C[s] + rh[s]; }
+        else { o.flo = S.C[s] + rl[s]; o.fhi = S.C[s] + rh[s]; o.rlo = base + run; o.rhi = base + run + d; }
+        out[pos++] = o;
+        covl += d;
+      }
+      run += d;
+    }
+    nout += total;
+  }
+  cov = warp_sum(covl);
+  __syncwarp();
+  return nout;
+}
+
+template <int DIR, bool COUNT_TOUCH>
+__device__ bool warp_any_extend(const DevFm& X, const SmemFm& S, uint32_t mask, const BIv* in, uint32_t nin,
+                                uint64_t& touches) {
+  const int lane = threadIdx.x & 31;
+  bool any = false;
+  for (uint32_t b = 0; b < nin && !any; b += 32) {
+    uint32_t i = b + lane;
+    BIv iv = i < nin ? in[i] : BIv{0, 0, 0, 0};
+    uint32_t a = DIR == 0 ? iv.rlo : iv.flo, e = DIR == 0 ? iv.rhi : iv.fhi;
+    uint32_t rl[16], rh[16];
+    sym_ranks(X, S, a, rl);
+    sym_ranks(X, S, e, rh);
+    if (COUNT_TOUCH && i < nin) touches += (a != 0) + (e != 0);
+    bool mine = false;
+#pragma unroll
+    for (int s = 0; s < 16; s++) mine |= i < nin && ((mask >> s) & 1) && rh[s] != rl[s];
+    any = __any_sync(0xFFFFFFFFu, mine);
+  }
+  return any;
+}
+
+// Candidate search of one read by the warp; control flow is warp-uniform.
+template <bool COUNT_TOUCH>
+__device__ uint32_t warp_mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf, const SmemFm& Sr,
+                                  const uint8_t* q, uint32_t n, const MemsParams& P, BIv* curr, BIv* nxt, BIv* wa,
+                                  BIv* wb, uint32_t set_cap, Cand* cands, uint32_t cand_cap, Pool& ivpool,
+                                  uint32_t& st, uint64_t& touches) {
+  const int lane = threadIdx.x & 31;
+  uint32_t nc = 0;
+  if (n == 0 || P.min_len == 0) return 0;
+  const BIv full = {0, Fw.text_len, 0, Fw.text_len};
+  bool ovf = false;
+  auto qmask = [&](const SmemFm& S, uint8_t c) -> uint32_t { return c < 16 ? S.compat_mask[c] : 0u; };
+  auto emit = [&](uint32_t qs, uint32_t qe, uint32_t count, const BIv* ivs, uint32_t niv) -> bool {
+    if (nc >= cand_cap) { st |= ST_CAND_OVF; return false; }
+    uint64_t off = 0;
+    if (lane == 0) off = thread_reserve(ivpool, niv);
+    off = __shfl_sync(0xFFFFFFFFu, off, 0);
+    if (off == ~0ull) { st |= ST_POOL_OVF; return false; }
+    BIv* dst = (BIv*)ivpool.base + off;
+    for (uint32_t k = lane; k < niv; k += 32) dst[k] = ivs[k];
+    if (lane == 0) cands[nc] = Cand{qs, qe, count, niv, off};
+    nc++;
+    __syncwarp();
+    return true;
+  };
+  if (P.mode == 1) {
+    for (uint32_t i = 0; i < n; i++) {
+      BIv* c = curr; BIv* x = nxt;
+      if (lane == 0) c[0] = full;
+      __syncwarp();
+      uint32_t ncur = 1, cov = 0, j = i;
+      bool matched = false;
+      while (j < n) {
+        uint32_t ncov;
+        uint32_t nn = warp_extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, ncur, x, set_cap, ncov, ovf, touches);
+        if (ovf) { st |= ST_SET_OVF; return ~0u; }
+        if (nn == 0) break;
+        BIv* t = c; c = x; x = t; ncur = nn; cov = ncov; j++; matched = true;
+      }
+      if (!matched || j - i < P.min_len) continue;
+      bool lmax = i == 0 || !warp_any_extend<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[i - 1]), c, ncur, touches);
+      if (!lmax) continue;
+      if (!emit(i, j, cov, c, ncur)) return ~0u;
+    }
+    return nc;
+  }
+  uint32_t pivot = 0;
+  while (pivot < n) {
+    BIv* c = curr; BIv* x = nxt;
+    if (lane == 0) x[0] = full;
+    __syncwarp();
+    uint32_t cov;
+    uint32_t ncur = warp_extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[pivot]), x, 1, c, set_cap, cov, ovf, touches);
+    if (ovf) { st |= ST_SET_OVF; return ~0u; }
+    if (ncur == 0) { pivot++; continue; }
+    uint32_t j = pivot + 1, reach = pivot + 1;
+    for (;;) {
+      uint32_t end, nn = 0, ncov = 0;
+      bool next_empty, record;
+      if (j == n) { end = n; next_empty = true; record = true; }
+      else {
+        nn = warp_extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, ncur, x, set_cap, ncov, ovf, touches);
+        if (ovf) { st |= ST_SET_OVF; return ~0u; }
+        end = j; next_empty = nn == 0; record = ncov != cov;
+      }
+      if (record) {
+        reach = end;
+        const BIv* b = c;
+        uint32_t nb = ncur, start = pivot, bcov = cov;
+        BIv* bufs[2] = {wa, wb};
+        int t = 0;
+        while (start > 0) {
+          uint32_t lcov;
+          uint32_t nl = warp_extend_set<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[start - 1]), b, nb, bufs[t], set_cap, lcov, ovf, touches);
+          if (ovf) { st |= ST_SET_OVF; return ~0u; }
+          if (nl == 0) break;
+          b = bufs[t]; nb = nl; bcov = lcov; t ^= 1; start--;
+        }
+        if (end - start >= P.min_len) {
+          bool rmax = end == n ||
+                      (start == pivot ? next_empty : !warp_any_extend<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[end]), b, nb, touches));
+          if (rmax && !emit(start, end, bcov, b, nb)) return ~0u;
+        }
+      }
+      if (j == n || nn == 0) break;
+      BIv* tt = c; c = x; x = tt; ncur = nn; cov = ncov; j++;
+    }
+    pivot = max(reach, pivot + 1);
+  }
+  return nc;
+}
+
+template <bool COUNT_TOUCH>
+__global__ void __launch_bounds__(128) k_mems_warp(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
+                                                  const uint16_t* __restrict__ compat_rv, const uint8_t* __restrict__ q,
+                                                  const uint64_t* __restrict__ qoff, MemsParams P, Pool ivpool,
+                                                  Pool hitpool, MemsOut out, MemsWork W) {
+  __shared__ SmemFm Sf, Sr;
+  smem_fm_init(Sf, Fw, compat_fw);
+  smem_fm_init(Sr, Rv, compat_rv);
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  BIv* base = W.sets + warp * 4 * W.set_cap;
+  Cand* cands = W.cands + warp * W.cand_cap;
+  uint64_t touches = 0;
+  for (;;) {
+    uint32_t k = 0;
+    if (lane == 0) k = atomicAdd(W.queue, 1u);
+    k = __shfl_sync(0xFFFFFFFFu, k, 0);
+    if (k >= W.n) break;
+    uint32_t i = W.ids[k];
+    uint32_t st = ST_OK;
+    uint64_t o = qoff[i];
+    uint32_t nc = warp_mems_one<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, (uint32_t)(qoff[i + 1] - o), P, base,
+                                             base + W.set_cap, base + 2 * W.set_cap, base + 3 * W.set_cap, W.set_cap,
+                                             cands, W.cand_cap, ivpool, st, touches);
+    __syncwarp();
+    if (lane == 0) {
+      uint64_t hs = 0; uint32_t hc = 0;
+      if (nc != ~0u) {
+        if (P.mode == 0) nc = finalize_smems(cands, nc);
+        if (!write_hits(cands, nc, P, ivpool, hitpool, hs, hc)) st |= ST_POOL_OVF;
+      }
+      if (st) { hs = 0; hc = 0; }
+      out.hit_start[i] = hs; out.hit_count[i] = hc; out.status[i] = st;
+      if (st & (ST_SET_OVF | ST_CAND_OVF)) atomicAdd(W.still_ovf, 1u);
+    }
+    __syncwarp();
+  }
+  if (COUNT_TOUCH && touches) atomicAdd(out.touches, (unsigned long long)touches);
+}
+
+}  // namespace hfm
