@@ -232,7 +232,7 @@ static int read_u64(hfm_index* x, const uint64_t* dsrc, uint64_t& v) {
 
 static constexpr uint32_t BS_SET_CAP = 64;     // fast-path interval-set capacity (backward search)
 static constexpr uint32_t BS_WARP_SET_CAP = 8192;   // long-tail pass, per warp
-static constexpr uint32_t MEM_SET_CAP = 512;   // fast-path interval-set capacity (SMEM / MEM)
+static constexpr uint32_t MEM_SET_CAP = 768;   // fast-path interval-set capacity (SMEM / MEM)
 static constexpr uint32_t MEM_WARP_SET_CAP = 8192;  // long-tail pass, per warp
 static constexpr int MEM_KC = 32;              // fast-path candidate capacity (thread-local)
 

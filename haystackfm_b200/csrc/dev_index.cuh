@@ -106,57 +106,6 @@ __device__ __forceinline__ void sym_ranks(const DevFm& F, const SmemFm& S, uint3
   }
 }
 
-// Ranks of every symbol at two positions a <= b.  When both fall in one 64-row record
-// (78% of the interval borders of a SMEM search) the record is loaded once.
-__device__ __forceinline__ void sym_ranks2(const DevFm& F, const SmemFm& S, uint32_t a, uint32_t b, uint32_t rl[16],
-                                           uint32_t rh[16]) {
-  if (a == 0 || ((a - 1) >> 6) != ((b - 1) >> 6)) {
-    sym_ranks(F, S, a, rl);
-    sym_ranks(F, S, b, rh);
-    return;
-  }
-  uint32_t pa = a - 1, pb = b - 1;
-  OccRec o = load_occ(F, pa >> 6);
-  SbRec sb = load_sb(F, pa >> 12);
-  uint64_t pl[4] = {u2to64(o.p0.x, o.p0.y), u2to64(o.p0.z, o.p0.w), u2to64(o.p1.x, o.p1.y), u2to64(o.p1.z, o.p1.w)};
-  uint64_t m[16];
-  m[0] = ~0ull;
-#pragma unroll
-  for (int p = 3; p >= 0; --p) {
-    const int cnt = 1 << (3 - p);
-#pragma unroll
-    for (int k = cnt - 1; k >= 0; --k) { uint64_t v = m[k]; m[2 * k + 1] = v & pl[p]; m[2 * k] = v & ~pl[p]; }
-  }
-  uint64_t la = (2ull << (pa & 63)) - 1ull, lb = (2ull << (pb & 63)) - 1ull;
-  uint32_t dw[8] = {o.d0.x, o.d0.y, o.d0.z, o.d0.w, o.d1.x, o.d1.y, o.d1.z, o.d1.w};
-  uint32_t sw[16] = {sb.a.x, sb.a.y, sb.a.z, sb.a.w, sb.b.x, sb.b.y, sb.b.z, sb.b.w,
-                     sb.c.x, sb.c.y, sb.c.z, sb.c.w, sb.d.x, sb.d.y, sb.d.z, sb.d.w};
-#pragma unroll
-  for (int s = 0; s < 16; s++) {
-    uint32_t base = sw[s] + ((s & 1) ? (dw[s >> 1] >> 16) : (dw[s >> 1] & 0xFFFFu));
-    rl[s] = base + (uint32_t)__popcll(m[s] & la);
-    rh[s] = base + (uint32_t)__popcll(m[s] & lb);
-  }
-}
-
-// Symbol of row `row` and its rank there (occurrences before the row): the LF step of a
-// single-row interval.  One record and one superblock load.
-__device__ __forceinline__ void row_symbol_rank(const DevFm& F, uint32_t row, uint32_t& sym, uint32_t& rank) {
-  uint32_t off = row & 63;
-  OccRec o = load_occ(F, row >> 6);
-  SbRec sb = load_sb(F, row >> 12);
-  uint64_t p0 = u2to64(o.p0.x, o.p0.y), p1 = u2to64(o.p0.z, o.p0.w);
-  uint64_t p2 = u2to64(o.p1.x, o.p1.y), p3 = u2to64(o.p1.z, o.p1.w);
-  uint32_t s = (uint32_t)((p0 >> off) & 1) | ((uint32_t)((p1 >> off) & 1) << 1) |
-               ((uint32_t)((p2 >> off) & 1) << 2) | ((uint32_t)((p3 >> off) & 1) << 3);
-  uint64_t m = ((1ull << off) - 1ull) & ((s & 1) ? p0 : ~p0) & ((s & 2) ? p1 : ~p1) & ((s & 4) ? p2 : ~p2) &
-               ((s & 8) ? p3 : ~p3);
-  uint32_t dwv = sel16(o.d0, o.d1, make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0), s >> 1);
-  uint32_t delta = (s & 1) ? (dwv >> 16) : (dwv & 0xFFFFu);
-  sym = s;
-  rank = sel16(sb.a, sb.b, sb.c, sb.d, s) + delta + (uint32_t)__popcll(m);
-}
-
 // One LF step with the sampled-SA test (FmIndex::resolve_sa loop body,
 // src/fm_index/query.rs:282-291; lf_step src/occ/mod.rs:456-480).  Returns true with
 // *val = SA value when row `pos` is sampled; otherwise advances pos = LF(pos).

@@ -130,8 +130,9 @@ __device__ __forceinline__ uint32_t backward_search_one(const DevFm& F, const Sm
       // one source interval: symbol order is already ascending row order
       uint2 iv = cur[0];
       uint32_t rl[16], rh[16];
-      sym_ranks2(F, S, iv.x, iv.y, rl, rh);
-      if (COUNT_TOUCH) touches += (iv.x != 0) + (iv.y != 0 && (iv.x == 0 || ((iv.x - 1) >> 6) != ((iv.y - 1) >> 6)));
+      sym_ranks(F, S, iv.x, rl);
+      sym_ranks(F, S, iv.y, rh);
+      if (COUNT_TOUCH) touches += (iv.x != 0) + (iv.y != 0);
 #pragma unroll
       for (int r = 0; r < 16; r++) {
         if (!((mask >> r) & 1)) continue;
@@ -147,8 +148,9 @@ __device__ __forceinline__ uint32_t backward_search_one(const DevFm& F, const Sm
       for (uint32_t i = 0; i < n; i++) {
         uint2 iv = cur[i];
         uint32_t rl[16], rh[16];
-        sym_ranks2(F, S, iv.x, iv.y, rl, rh);
-        if (COUNT_TOUCH) touches += (iv.x != 0) + (iv.y != 0 && (iv.x == 0 || ((iv.x - 1) >> 6) != ((iv.y - 1) >> 6)));
+        sym_ranks(F, S, iv.x, rl);
+        sym_ranks(F, S, iv.y, rh);
+        if (COUNT_TOUCH) touches += (iv.x != 0) + (iv.y != 0);
 #pragma unroll
         for (int r = 0; r < 16; r++) cnt[r] += (((mask >> r) & 1) && rh[r] > rl[r]) ? 1u : 0u;
       }
@@ -159,7 +161,8 @@ __device__ __forceinline__ uint32_t backward_search_one(const DevFm& F, const Sm
       for (uint32_t i = 0; i < n; i++) {
         uint2 iv = cur[i];
         uint32_t rl[16], rh[16];
-        sym_ranks2(F, S, iv.x, iv.y, rl, rh);
+        sym_ranks(F, S, iv.x, rl);
+        sym_ranks(F, S, iv.y, rh);
 #pragma unroll
         for (int r = 0; r < 16; r++)
           if (((mask >> r) & 1) && rh[r] > rl[r]) nxt[cnt[r]++] = make_uint2(S.C[r] + rl[r], S.C[r] + rh[r]);
@@ -243,24 +246,10 @@ __device__ __forceinline__ uint32_t extend_set(const DevFm& X, const SmemFm& S, 
     BIv iv = in[i];
     uint32_t a = DIR == 0 ? iv.rlo : iv.flo, b = DIR == 0 ? iv.rhi : iv.fhi;
     uint32_t base = DIR == 0 ? iv.flo : iv.rlo;
-    if (b - a == 1) {
-      // a single row extends only by its own symbol: one LF step
-      uint32_t s0, rk;
-      row_symbol_rank(X, a, s0, rk);
-      if (COUNT_TOUCH) touches += 1;
-      if ((mask >> s0) & 1) {
-        if (nout >= cap) { ovf = true; return nout; }
-        BIv e;
-        if (DIR == 0) { e.flo = base; e.fhi = base + 1; e.rlo = S.C[s0] + rk; e.rhi = S.C[s0] + rk + 1; }
-        else { e.flo = S.C[s0] + rk; e.fhi = S.C[s0] + rk + 1; e.rlo = base; e.rhi = base + 1; }
-        out[nout++] = e;
-        cov += 1;
-      }
-      continue;
-    }
     uint32_t rl[16], rh[16];
-    sym_ranks2(X, S, a, b, rl, rh);
-    if (COUNT_TOUCH) touches += (a != 0) + (b != 0 && (a == 0 || ((a - 1) >> 6) != ((b - 1) >> 6)));
+    sym_ranks(X, S, a, rl);
+    sym_ranks(X, S, b, rh);
+    if (COUNT_TOUCH) touches += (a != 0) + (b != 0);
     uint32_t run = 0;
 #pragma unroll
     for (int s = 0; s < 16; s++) {
@@ -286,16 +275,10 @@ __device__ __forceinline__ bool any_extend(const DevFm& X, const SmemFm& S, uint
   for (uint32_t i = 0; i < nin; i++) {
     BIv iv = in[i];
     uint32_t a = DIR == 0 ? iv.rlo : iv.flo, b = DIR == 0 ? iv.rhi : iv.fhi;
-    if (b - a == 1) {
-      uint32_t s0, rk;
-      row_symbol_rank(X, a, s0, rk);
-      if (COUNT_TOUCH) touches += 1;
-      if ((mask >> s0) & 1) return true;
-      continue;
-    }
     uint32_t rl[16], rh[16];
-    sym_ranks2(X, S, a, b, rl, rh);
-    if (COUNT_TOUCH) touches += (a != 0) + (b != 0 && (a == 0 || ((a - 1) >> 6) != ((b - 1) >> 6)));
+    sym_ranks(X, S, a, rl);
+    sym_ranks(X, S, b, rh);
+    if (COUNT_TOUCH) touches += (a != 0) + (b != 0);
 #pragma unroll
     for (int s = 0; s < 16; s++) if (((mask >> s) & 1) && rh[s] != rl[s]) return true;
   }
