@@ -91,10 +91,10 @@ struct Counters {                    // device-side counters, one block per hand
 
 struct FmDev {
   DevFm d{};
-  DevBuf occ, sbc, ssa, sa_vals, lut, bounds, compat;
+  DevBuf occ, ssa, sa_vals, lut, bounds, compat;
   uint32_t text_len = 0, num_seqs = 0, lookup_depth = 0, tag = 0, num_lanes = 0, encoding = 0, rate = 0;
   std::vector<uint32_t> seq_boundaries;
-  size_t bytes() const { return occ.cap + sbc.cap + ssa.cap + sa_vals.cap + lut.cap + bounds.cap + compat.cap; }
+  size_t bytes() const { return occ.cap + ssa.cap + sa_vals.cap + lut.cap + bounds.cap + compat.cap; }
 };
 
 }  // namespace hfm
@@ -112,6 +112,7 @@ struct hfm_index {
       scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr,
       mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout, blockmap, blockmap2;
   uint32_t flags = 0;
+  int mems_variant = 1;   // register-budget variant of the SMEM fast kernel (see mems_device)
   int num_sms = 0;
   uint64_t iv_cap = 0, miv_cap = 0, hit_cap = 0;   // pool capacities in elements (uint2 / BIv / hit)
   Counters* h_ctr = nullptr;        // pinned
@@ -134,10 +135,9 @@ static int upload(DevBuf& b, const void* src, size_t bytes, cudaStream_t s) {
 
 static int build_device_fm(const HostFm& h, FmDev& f, cudaStream_t s) {
   const uint32_t n = h.text_len, L = h.num_lanes;
-  const uint64_t nblk = ((uint64_t)n + 63) / 64, nsb = ((uint64_t)n + 4095) / 4096;
-  std::vector<uint32_t> occ(nblk * 16, 0), sbc(nsb * 16, 0);
+  const uint64_t nblk = ((uint64_t)n + 63) / 64;
+  std::vector<uint32_t> occ(nblk * 24, 0);
   std::vector<uint32_t> ssa(nblk * 4, 0);
-  uint32_t cur_sb[16] = {0};
   const uint64_t width = h.encoding == 0 ? h.num_planes : L;
   for (uint64_t b = 0; b < nblk; b++) {
     const uint8_t* r = h.block_data + b * h.block_stride;
@@ -157,11 +157,8 @@ static int build_device_fm(const HostFm& h, FmDev& f, cudaStream_t s) {
       if (b == nblk - 1 && (n & 63)) m &= (1ull << (n & 63)) - 1;   // rows past the text
       for (int p = 0; p < 4; p++) if ((sym >> p) & 1) planes[p] |= m;
     }
-    if (b % 64 == 0) { std::memcpy(cur_sb, cnt, 64); std::memcpy(&sbc[(b / 64) * 16], cnt, 64); }
-    uint16_t deltas[16];
-    for (int sy = 0; sy < 16; sy++) deltas[sy] = (uint16_t)(cnt[sy] - cur_sb[sy]);
-    std::memcpy(&occ[b * 16], deltas, 32);
-    std::memcpy(&occ[b * 16 + 8], planes, 32);
+    std::memcpy(&occ[b * 24], cnt, 64);
+    std::memcpy(&occ[b * 24 + 16], planes, 32);
     // sampled-SA record: bits + rank before (validated equal to the stored sb + delta)
     uint64_t word; uint32_t sb; uint16_t d;
     std::memcpy(&word, h.ssa_words + b * 14, 8); std::memcpy(&sb, h.ssa_words + b * 14 + 8, 4);
@@ -173,7 +170,6 @@ static int build_device_fm(const HostFm& h, FmDev& f, cudaStream_t s) {
   uint16_t sym_mask = 0;
   for (int sy = 0; sy < 16; sy++) if (h.s2l[sy] != 0xFF) sym_mask |= (uint16_t)(1u << sy);
   RET(upload(f.occ, occ.data(), occ.size() * 4, s));
-  RET(upload(f.sbc, sbc.data(), sbc.size() * 4, s));
   RET(upload(f.ssa, ssa.data(), ssa.size() * 4, s));
   RET(upload(f.sa_vals, h.sa_vals, h.n_sa_vals * 4, s));
   RET(upload(f.bounds, h.seq_boundaries.data(), h.seq_boundaries.size() * 4, s));
@@ -183,7 +179,7 @@ static int build_device_fm(const HostFm& h, FmDev& f, cudaStream_t s) {
   RET(upload(f.compat, cm, sizeof(cm), s));
   CK(cudaStreamSynchronize(s));      // host vectors die at return
   DevFm& d = f.d;
-  d.occ = f.occ.as<uint4>(); d.sbc = f.sbc.as<uint4>(); d.ssa = f.ssa.as<uint4>();
+  d.occ = f.occ.as<uint4>(); d.ssa = f.ssa.as<uint4>();
   d.sa_vals = f.sa_vals.as<uint32_t>(); d.seq_bounds = f.bounds.as<uint32_t>();
   d.lut = h.has_lookup ? f.lut.as<uint2>() : nullptr;
   d.text_len = n; d.num_seqs = (uint32_t)h.seq_boundaries.size(); d.sample_rate = h.sample_rate;
@@ -472,9 +468,13 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   if (x->hit_cap < (uint64_t)nq * 24 + 4096) x->hit_cap = (uint64_t)nq * 24 + 4096;   // hit = 32 B
   MemsParams P{min_len, mode, cap, nb ? 1u : 0u};
   const FmDev& Fw = x->fwd; const FmDev& Rv = x->rev;
-  // persistent fast pass: one wave of resident threads, MEM_SET_CAP intervals per set
+  // persistent fast pass: one wave of resident threads, MEM_SET_CAP intervals per set.
+  // Register budget variants: 5, 6 or 8 resident blocks of 128 threads per SM.
+  int variant = x->mems_variant;
   int bpsm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC>, 128, 0));
+  if (variant == 0) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC, 5>, 128, 0));
+  else if (variant == 1) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC, 6>, 128, 0));
+  else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC, 8>, 128, 0));
   uint64_t threads = (uint64_t)std::max(1, bpsm) * x->num_sms * 128;
   threads = std::min<uint64_t>(threads, ((uint64_t)nq + 127) / 128 * 128);
   RET(x->memwork.ensure(std::max<uint64_t>(threads, 32) * 4 * MEM_SET_CAP * 16));
@@ -492,11 +492,17 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       if (x->memwork.cap < (size_t)grid * 128 * 4 * MEM_SET_CAP * 16) return set_error(HFM_E_ARG, "internal: work area too small");
       cudaEventRecord(x->evk[0], x->stream);
       if (x->count_work)
-        k_mems<true, 32, MEM_KC><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                             d_q, d_qoff, P, ivp, hp, o, W);
+        k_mems<true, 32, MEM_KC, 5><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                                d_q, d_qoff, P, ivp, hp, o, W);
+      else if (variant == 0)
+        k_mems<false, 32, MEM_KC, 5><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                                 d_q, d_qoff, P, ivp, hp, o, W);
+      else if (variant == 1)
+        k_mems<false, 32, MEM_KC, 6><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                                 d_q, d_qoff, P, ivp, hp, o, W);
       else
-        k_mems<false, 32, MEM_KC><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                              d_q, d_qoff, P, ivp, hp, o, W);
+        k_mems<false, 32, MEM_KC, 8><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                                 d_q, d_qoff, P, ivp, hp, o, W);
       cudaEventRecord(x->evk[1], x->stream);
       x->k_search_rec = true;
       launches++;
@@ -674,6 +680,7 @@ int hfm_index_load(const uint8_t* bytes, size_t len, int kind, const hfm_opts* o
   CK(cudaSetDevice(dev));
   std::unique_ptr<hfm_index> x(new hfm_index());
   x->device = dev; x->kind = kind; x->flags = opts ? opts->flags : 0;
+  if (const char* v = std::getenv("HFM_MEMS_VARIANT")) x->mems_variant = std::atoi(v);
   CK(cudaDeviceGetAttribute(&x->num_sms, cudaDevAttrMultiProcessorCount, dev));
   CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
   for (auto& e : x->ev) CK(cudaEventCreate(&e));
@@ -690,8 +697,8 @@ void hfm_index_free(hfm_index* x) {
   if (!x) return;
   cudaSetDevice(x->device);
   if (x->stream) cudaStreamSynchronize(x->stream);
-  for (DevBuf* b : {&x->fwd.occ, &x->fwd.sbc, &x->fwd.ssa, &x->fwd.sa_vals, &x->fwd.lut, &x->fwd.bounds,
-                    &x->fwd.compat, &x->rev.occ, &x->rev.sbc, &x->rev.ssa, &x->rev.sa_vals, &x->rev.lut,
+  for (DevBuf* b : {&x->fwd.occ, &x->fwd.ssa, &x->fwd.sa_vals, &x->fwd.lut, &x->fwd.bounds,
+                    &x->fwd.compat, &x->rev.occ, &x->rev.ssa, &x->rev.sa_vals, &x->rev.lut,
                     &x->rev.bounds, &x->rev.compat, &x->q, &x->qoff, &x->counts, &x->nhits, &x->niv, &x->ivoff,
                     &x->status, &x->ovf, &x->ivpool, &x->hitpool, &x->seg_row, &x->seg_off, &x->pos_base,
                     &x->seg_base, &x->scan_tmp, &x->out_pairs, &x->ref_bounds, &x->hit_start, &x->hit_count,

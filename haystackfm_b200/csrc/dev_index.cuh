@@ -2,16 +2,15 @@
 // primitives every kernel uses.
 //
 // Device layout (built once by hfm_index_load from the reference's bincode records):
-//   occ   : one 64-byte record per 64 BWT rows: 16 x u16 symbol counts since the record's
-//           4096-row superblock, then 4 x u64 bitplanes of each row's 4-bit symbol code.
-//           The reference compacts symbols to lanes; on the device the lane IS the symbol
-//           code, so no lane map is consulted.  One random record touch = 2 DRAM sectors.
-//   sbc   : one 64-byte record per 4096 rows: 16 x u32 symbol counts before the superblock
-//           (1.5 MB per 100 Mbp: L2-resident).
+//   occ   : one 96-byte record per 64 BWT rows: 16 x u32 counts of every symbol code before
+//           the block, then 4 x u64 bitplanes of each row's 4-bit symbol code.  The reference
+//           compacts symbols to lanes and splits counts into superblock + u16 delta; on the
+//           device the lane IS the symbol code and the count is whole, so a rank is one
+//           record read (3 DRAM sectors) and no table lookup.
 //   ssa   : one 16-byte record per 64 rows: u64 "row is sampled" bits + u32 count of
 //           sampled rows before the word (SampledSuffixArray, src/suffix_array/mod.rs:54-63).
 //   sa_vals, seq_boundaries, lookup intervals: as in the reference.
-// rank(c, i) = sbc[(i-1)/4096][c] + occ[(i-1)/64].delta[c] + popc(rows of code c <= (i-1)%64),
+// rank(c, i) = occ[(i-1)/64].count[c] + popc(rows of code c <= (i-1)%64),
 // identical to OccTable::rank (src/occ/mod.rs:330-363).
 #pragma once
 #include <cstdint>
@@ -19,8 +18,7 @@
 namespace hfm {
 
 struct DevFm {
-  const uint4* occ;          // 4 x uint4 per block
-  const uint4* sbc;          // 4 x uint4 per superblock
+  const uint4* occ;          // 6 x uint4 per block
   const uint4* ssa;          // 1 x uint4 per block
   const uint32_t* sa_vals;
   const uint2* lut;          // nullptr when the index has no lookup table
@@ -61,18 +59,14 @@ __device__ __forceinline__ uint32_t sel16(uint4 a, uint4 b, uint4 c, uint4 d, ui
   return sel4(x, i & 3);
 }
 
-struct OccRec { uint4 d0, d1, p0, p1; };
+struct OccRec { uint4 c0, c1, c2, c3, p0, p1; };
 
 __device__ __forceinline__ OccRec load_occ(const DevFm& F, uint32_t blk) {
-  const uint4* r = F.occ + (size_t)blk * 4;
-  OccRec o; o.d0 = __ldg(r); o.d1 = __ldg(r + 1); o.p0 = __ldg(r + 2); o.p1 = __ldg(r + 3);
+  const uint4* r = F.occ + (size_t)blk * 6;
+  OccRec o;
+  o.c0 = __ldg(r); o.c1 = __ldg(r + 1); o.c2 = __ldg(r + 2); o.c3 = __ldg(r + 3);
+  o.p0 = __ldg(r + 4); o.p1 = __ldg(r + 5);
   return o;
-}
-struct SbRec { uint4 a, b, c, d; };
-__device__ __forceinline__ SbRec load_sb(const DevFm& F, uint32_t sb) {
-  const uint4* r = F.sbc + (size_t)sb * 4;
-  SbRec s; s.a = __ldg(r); s.b = __ldg(r + 1); s.c = __ldg(r + 2); s.d = __ldg(r + 3);
-  return s;
 }
 
 // Rank of every symbol code at position i (counts of code s in bwt[0..i)), absent codes 0.
@@ -84,10 +78,9 @@ __device__ __forceinline__ void sym_ranks(const DevFm& F, const SmemFm& S, uint3
   }
   uint32_t pos = i - 1, off = pos & 63;
   OccRec o = load_occ(F, pos >> 6);
-  SbRec sb = load_sb(F, pos >> 12);
   uint64_t low = (2ull << off) - 1ull;          // bits 0..off (off = 63 -> all ones)
   uint64_t pl[4] = {u2to64(o.p0.x, o.p0.y), u2to64(o.p0.z, o.p0.w), u2to64(o.p1.x, o.p1.y), u2to64(o.p1.z, o.p1.w)};
-  // lane masks by successive splits on planes 3,2,1,0: m[l] = rows of lane l among bits <= off
+  // symbol masks by successive splits on planes 3,2,1,0: m[s] = rows of code s among bits <= off
   uint64_t m[16];
   m[0] = low;
 #pragma unroll
@@ -96,14 +89,10 @@ __device__ __forceinline__ void sym_ranks(const DevFm& F, const SmemFm& S, uint3
 #pragma unroll
     for (int k = cnt - 1; k >= 0; --k) { uint64_t v = m[k]; m[2 * k + 1] = v & pl[p]; m[2 * k] = v & ~pl[p]; }
   }
-  uint32_t dw[8] = {o.d0.x, o.d0.y, o.d0.z, o.d0.w, o.d1.x, o.d1.y, o.d1.z, o.d1.w};
-  uint32_t sw[16] = {sb.a.x, sb.a.y, sb.a.z, sb.a.w, sb.b.x, sb.b.y, sb.b.z, sb.b.w,
-                     sb.c.x, sb.c.y, sb.c.z, sb.c.w, sb.d.x, sb.d.y, sb.d.z, sb.d.w};
+  uint32_t cw[16] = {o.c0.x, o.c0.y, o.c0.z, o.c0.w, o.c1.x, o.c1.y, o.c1.z, o.c1.w,
+                     o.c2.x, o.c2.y, o.c2.z, o.c2.w, o.c3.x, o.c3.y, o.c3.z, o.c3.w};
 #pragma unroll
-  for (int s = 0; s < 16; s++) {
-    uint32_t delta = (s & 1) ? (dw[s >> 1] >> 16) : (dw[s >> 1] & 0xFFFFu);
-    r[s] = sw[s] + delta + (uint32_t)__popcll(m[s]);
-  }
+  for (int s = 0; s < 16; s++) r[s] = cw[s] + (uint32_t)__popcll(m[s]);
 }
 
 // One LF step with the sampled-SA test (FmIndex::resolve_sa loop body,
@@ -113,7 +102,6 @@ __device__ __forceinline__ bool lf_or_sample(const DevFm& F, const SmemFm& S, ui
   uint32_t blk = pos >> 6, off = pos & 63;
   uint4 w = __ldg(F.ssa + blk);
   OccRec o = load_occ(F, blk);            // issued before the sampled test: overlaps its latency
-  SbRec sb = load_sb(F, pos >> 12);
   uint64_t word = u2to64(w.x, w.y);
   uint64_t below = (1ull << off) - 1ull;
   if ((word >> off) & 1ull) {
@@ -126,9 +114,7 @@ __device__ __forceinline__ bool lf_or_sample(const DevFm& F, const SmemFm& S, ui
                   ((uint32_t)((p2 >> off) & 1) << 2) | ((uint32_t)((p3 >> off) & 1) << 3);
   uint64_t m = below & ((lane & 1) ? p0 : ~p0) & ((lane & 2) ? p1 : ~p1) & ((lane & 4) ? p2 : ~p2) &
                ((lane & 8) ? p3 : ~p3);
-  uint32_t dwv = sel16(o.d0, o.d1, make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0), lane >> 1);
-  uint32_t delta = (lane & 1) ? (dwv >> 16) : (dwv & 0xFFFFu);
-  uint32_t rank = sel16(sb.a, sb.b, sb.c, sb.d, lane) + delta + (uint32_t)__popcll(m);
+  uint32_t rank = sel16(o.c0, o.c1, o.c2, o.c3, lane) + (uint32_t)__popcll(m);
   pos = S.C[lane] + rank;
   return false;
 }

@@ -457,8 +457,8 @@ struct MemsWork {
   uint32_t* still_ovf;
 };
 
-template <bool COUNT_TOUCH, int STRIDE, int KC>
-__global__ void __launch_bounds__(128) k_mems(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
+template <bool COUNT_TOUCH, int STRIDE, int KC, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_mems(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
                                              const uint16_t* __restrict__ compat_rv, const uint8_t* __restrict__ q,
                                              const uint64_t* __restrict__ qoff, MemsParams P, Pool ivpool,
                                              Pool hitpool, MemsOut out, MemsWork W) {
