@@ -112,7 +112,7 @@ struct hfm_index {
       scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr,
       mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout, blockmap, blockmap2;
   uint32_t flags = 0;
-  int mems_variant = 1;   // register-budget variant of the SMEM fast kernel (see mems_device)
+  int mems_variant = 2;   // register-budget variant of the SMEM fast kernel (see mems_device)
   int num_sms = 0;
   uint64_t iv_cap = 0, miv_cap = 0, hit_cap = 0;   // pool capacities in elements (uint2 / BIv / hit)
   Counters* h_ctr = nullptr;        // pinned
