@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-smem", action="store_true",
+                    help="one SMEM search launch (no position resolve) for ncu, then its work counters")
     return ap.parse_args()
 
 
@@ -179,10 +181,33 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def profile_smem(args):
+    """One SMEM search pass without position resolve (the launch ncu captures), then the
+    same pass with work counters to report its Occ touches."""
+    import torch
+    from haystackfm_b200 import _lib as L
+    from haystackfm_b200.fm_index import BidirFmIndex
+    _, data, reads, _, _ = workload(args)
+    idx = BidirFmIndex.from_bytes(data)
+    h, lib, n = idx.handle, L.lib(), args.reads
+    rd = torch.from_numpy(reads.reshape(-1)).cuda()
+    off = torch.arange(0, (n + 1) * 150, 150, dtype=torch.int64, device="cuda")
+    dm = L.HfmDevMems()
+    L.check(lib.hfm_mems_batch_device(h.h, rd.data_ptr(), off.data_ptr(), n, 19, 0, None, 0, 1024, C.byref(dm)))
+    s = h.stats()
+    h.set_counters(True)
+    L.check(lib.hfm_mems_batch_device(h.h, rd.data_ptr(), off.data_ptr(), n, 19, 0, None, 0, 1024, C.byref(dm)))
+    print(json.dumps({"profile": "smem_search", "reads": n, "k_mems_ms": s.ms_search_kernel,
+                      "fallback_reads": s.fallback_reads, "mem_hits": dm.n_hits,
+                      "occ_touches": h.stats().occ_touches}), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_smem:
+        return profile_smem(args)
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
