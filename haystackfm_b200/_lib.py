@@ -86,6 +86,7 @@ SIGNATURES = {
     "hfm_mems_batch": (C.c_int, [C.c_void_p, u8p, u64p, C.c_uint32, C.c_uint32, C.c_uint32, u32p, C.c_uint32,
                                  C.c_uint32, C.POINTER(C.POINTER(HfmMemOut))]),
     "hfm_count_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "hfm_count_batch_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
     "hfm_locate_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                           C.POINTER(HfmDevHits)]),
     "hfm_mems_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,

@@ -819,3 +819,108 @@ int hfm_mems_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free count entry point.
+//
+// Some callers cannot let a library call cudaMalloc: a host framework that owns all of
+// the GPU's memory through its own pool allocator (and would be pushed out of memory or
+// bypassed by foreign allocations), or a latency-bound serving loop where cudaMalloc's
+// implicit device synchronisation and multi-millisecond cost are not acceptable.
+// hfm_count_batch_noalloc serves them: it runs the same backward-search kernels as
+// hfm_count_batch_device, but its work area (interval sets, queue counters, per-query
+// status and overflow list) is the file-scope device array below instead of buffers the
+// handle allocates.  The caller passes device inputs and the device output.
+//
+// Costs and limits:
+//  * the array (NOALLOC_SCRATCH_BYTES, 17 MiB) exists on every GPU that loads this
+//    library, for the life of the process;
+//  * at most NOALLOC_MAX_QUERIES queries per call, and an interval set of at most
+//    NOALLOC_WARP_SET_CAP intervals per query (larger sets return HFM_E_OVERFLOW);
+//  * every call shares the one array, so calls that overlap on the GPU (two streams, two
+//    handles, two host threads) race and must be serialised by the caller;
+//  * the first call on a device resolves the array's device address with
+//    cudaGetSymbolAddress (with that device current); make that first call before any
+//    stream capture is started.
+// ===========================================================================
+namespace hfm {
+
+constexpr uint32_t NOALLOC_MAX_QUERIES = 1u << 20;
+constexpr uint32_t NOALLOC_THREADS = 16384;        // fast pass: 64 blocks x 256 threads
+constexpr uint32_t NOALLOC_SET_CAP = 32;           // fast pass: intervals per set
+constexpr uint32_t NOALLOC_WARPS = 32;             // long-tail pass: 8 blocks x 4 warps
+constexpr uint32_t NOALLOC_WARP_SET_CAP = 2048;    // long-tail pass: intervals per set
+constexpr size_t NOALLOC_CTR_BYTES = 256;
+constexpr size_t NOALLOC_FAST_BYTES = (size_t)NOALLOC_THREADS * 2 * NOALLOC_SET_CAP * sizeof(uint2);
+constexpr size_t NOALLOC_TAIL_BYTES = (size_t)NOALLOC_WARPS * 2 * NOALLOC_WARP_SET_CAP * sizeof(uint2);
+constexpr size_t NOALLOC_LIST_BYTES = (size_t)NOALLOC_MAX_QUERIES * sizeof(uint32_t);
+constexpr size_t NOALLOC_SCRATCH_BYTES =
+    NOALLOC_CTR_BYTES + NOALLOC_FAST_BYTES + NOALLOC_TAIL_BYTES + 2 * NOALLOC_LIST_BYTES;   // 17 MiB + 256 B
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+
+struct NoallocCtr { unsigned int queue, queue2; uint32_t n_ovf, still_ovf; unsigned long long used, touches; };
+
+// Device address of g_noalloc_scratch per device ordinal (host code cannot use the
+// symbol itself: on the host it names a stand-in, not device memory).
+static std::mutex g_noalloc_mu;
+static void* g_noalloc_addr[256] = {nullptr};
+
+static int noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= 256) return set_error(HFM_E_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);   // the calling device is current
+    if (e != cudaSuccess || !p)
+      return set_error(HFM_E_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+    g_noalloc_addr[device] = p;
+  }
+  *out = (unsigned char*)g_noalloc_addr[device];
+  return HFM_OK;
+}
+
+}  // namespace hfm
+
+extern "C" int hfm_count_batch_noalloc(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq,
+                                       uint32_t* d_counts) {
+  if (!x || (nq && (!d_qoff || !d_counts))) return set_error(HFM_E_ARG, "NULL argument");
+  if (nq > NOALLOC_MAX_QUERIES)
+    return set_error(HFM_E_ARG, "hfm_count_batch_noalloc: " + std::to_string(nq) + " queries exceed the limit of " +
+                                    std::to_string(NOALLOC_MAX_QUERIES) + " per call");
+  Guard g(x);
+  unsigned char* base = nullptr;
+  RET(noalloc_scratch(x->device, &base));
+  if (nq == 0) return HFM_OK;
+  NoallocCtr* ctr = (NoallocCtr*)base;
+  uint2* fast = (uint2*)(base + NOALLOC_CTR_BYTES);
+  uint2* tail = (uint2*)(base + NOALLOC_CTR_BYTES + NOALLOC_FAST_BYTES);
+  uint32_t* status = (uint32_t*)(base + NOALLOC_CTR_BYTES + NOALLOC_FAST_BYTES + NOALLOC_TAIL_BYTES);
+  uint32_t* ovf = status + NOALLOC_MAX_QUERIES;
+  const FmDev& F = x->fwd;
+  // the previous call's counters are still in the array: clear them
+  CK(cudaMemsetAsync(ctr, 0, sizeof(NoallocCtr), x->stream));
+  Pool pool{nullptr, &ctr->used, 0};
+  BsOut o{d_counts, nullptr, nullptr, nullptr, status, ovf, &ctr->n_ovf, &ctr->touches};
+  k_bsearch<false, 32><<<NOALLOC_THREADS / 256, 256, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, nullptr,
+                                                                     nq, 0, fast, NOALLOC_SET_CAP, &ctr->queue, pool,
+                                                                     o, &ctr->still_ovf);
+  CK(cudaGetLastError());
+  uint32_t n_ovf = 0;
+  CK(cudaMemcpyAsync(&n_ovf, &ctr->n_ovf, sizeof(uint32_t), cudaMemcpyDeviceToHost, x->stream));
+  CK(cudaStreamSynchronize(x->stream));
+  if (n_ovf) {
+    k_bsearch_warp<false><<<NOALLOC_WARPS / 4, 128, 0, x->stream>>>(F.d, F.compat.as<uint16_t>(), d_q, d_qoff, ovf, n_ovf,
+                                                                   0, tail, NOALLOC_WARP_SET_CAP, &ctr->queue2, pool,
+                                                                   o, &ctr->still_ovf);
+    CK(cudaGetLastError());
+    uint32_t still = 0;
+    CK(cudaMemcpyAsync(&still, &ctr->still_ovf, sizeof(uint32_t), cudaMemcpyDeviceToHost, x->stream));
+    CK(cudaStreamSynchronize(x->stream));
+    if (still)
+      return set_error(HFM_E_OVERFLOW, "hfm_count_batch_noalloc: an interval set exceeds " +
+                                           std::to_string(NOALLOC_WARP_SET_CAP) + " intervals (use hfm_count_batch)");
+  }
+  CK(cudaStreamSynchronize(x->stream));
+  return HFM_OK;
+}

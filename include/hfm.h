@@ -167,6 +167,19 @@ int hfm_mems_batch_device(hfm_index* idx, const uint8_t* d_q, const uint64_t* d_
                           uint32_t min_len, uint32_t mode, const uint32_t* ref_bounds, uint32_t n_bounds,
                           uint32_t max_hits, hfm_dev_mems* out);
 
+/* Allocation-free count (no counterpart in the reference).  Same results as
+ * hfm_count_batch_device, for callers that must not let a library allocate GPU memory:
+ * frameworks that own the device's memory through their own pool, and latency-bound
+ * serving loops that cannot absorb cudaMalloc's synchronisation.  Its work area is one
+ * static 17 MiB device array inside libhfm.so (present on every GPU that loads the library
+ * until exit) instead of handle buffers; inputs and output are the caller's device memory.
+ * Limits: nq <= 1,048,576 per call (else HFM_E_ARG); interval sets of at most 2,048
+ * intervals per query (else HFM_E_OVERFLOW, use hfm_count_batch).  All calls share the
+ * array: calls that overlap on the GPU race, so serialise them.  The first call on a
+ * device looks up the array's device address; make it before any stream capture. */
+int hfm_count_batch_noalloc(hfm_index* idx, const uint8_t* d_q, const uint64_t* d_q_off, uint32_t nq,
+                            uint32_t* d_counts_out);
+
 /* ---- misc ----------------------------------------------------------------- */
 void hfm_free(void* p);                    /* frees hfm_hits*, hfm_mem_out*, build bytes */
 const char* hfm_last_error(void);          /* thread-local message of the last failure   */
