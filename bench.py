@@ -49,7 +49,8 @@ def parse():
     ap.add_argument("--reads", type=int, default=1_000_000)
     ap.add_argument("--ref-len", type=int, default=100_000_000)
     ap.add_argument("--contigs", type=int, default=200)
-    ap.add_argument("--e2e-chunk", type=int, default=250_000)
+    ap.add_argument("--e2e-chunk", type=int, default=125_000)
+    ap.add_argument("--e2e-streams", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-e2e", action="store_true")
@@ -340,24 +341,42 @@ def main():
     rp, kp = reads_pin.numpy(), k32_pin.numpy()
     ch = min(args.e2e_chunk, n)
 
-    def e2e_step():
+    # Two handles (two index replicas, two streams) driven by two host threads: one handle's
+    # kernels overlap the other's result copies.  Handles are independent by contract.
+    handles = [h] + [BidirFmIndex.from_bytes(data, device=local).handle for _ in range(args.e2e_streams - 1)]
+
+    def run_chunks(hh, chunks, acc):
         h2d = d2h = 0
-        for a in range(0, n, ch):
+        for a in chunks:
             b = min(n, a + ch)
             m = b - a
             off150 = np.arange(0, (m + 1) * 150, 150, dtype=np.uint64)
             off32 = np.arange(0, (m + 1) * 32, 32, dtype=np.uint64)
             res = C.POINTER(L.HfmHits)()
-            L.check(lib.hfm_locate_batch(h.h, L.ptr(kp[a * 32:], L.u8p), L.ptr(off32, L.u64p), m, 1024, C.byref(res)))
+            L.check(lib.hfm_locate_batch(hh.h, L.ptr(kp[a * 32:], L.u8p), L.ptr(off32, L.u64p), m, 1024, C.byref(res)))
             d2h += (m + 1) * 8 + m * 4 + res.contents.total * 8
             lib.hfm_free(res)
             mo = C.POINTER(L.HfmMemOut)()
-            L.check(lib.hfm_mems_batch(h.h, L.ptr(rp[a * 150:], L.u8p), L.ptr(off150, L.u64p), m, 19, 0,
+            L.check(lib.hfm_mems_batch(hh.h, L.ptr(rp[a * 150:], L.u8p), L.ptr(off150, L.u64p), m, 19, 0,
                                        L.ptr(bounds, L.u32p), nb, 1024, C.byref(mo)))
             d2h += (m + 1) * 8 + mo.contents.n_hits * 32 + mo.contents.n_positions * 8
             lib.hfm_free(mo)
             h2d += m * 32 + (m + 1) * 8 + m * 150 + (m + 1) * 8 + nb * 4
-        return h2d, d2h
+        acc.append((h2d, d2h))
+
+    def e2e_step():
+        import threading
+        starts = list(range(0, n, ch))
+        acc, threads = [], []
+        for k, hh in enumerate(handles):
+            t = threading.Thread(target=run_chunks, args=(hh, starts[k::len(handles)], acc))
+            t.start()
+            threads.append(t)
+        for t in threads:
+            t.join()
+        if len(acc) != len(handles):
+            raise RuntimeError("an end-to-end worker failed")
+        return sum(a for a, _ in acc), sum(b for _, b in acc)
 
     e2e_s, h2d, d2h = 0.0, 0, 0
     if not args.no_e2e:
@@ -373,7 +392,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e = {"value": world * n * args.steps / e2e_s if e2e_s else None, "unit": "reads/s", "h2d_bytes_per_step": int(h2d),
-           "d2h_bytes_per_step": int(d2h), "chunk_reads": ch}
+           "d2h_bytes_per_step": int(d2h), "chunk_reads": ch, "handles": args.e2e_streams}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
