@@ -236,14 +236,54 @@ __global__ void __launch_bounds__(256) k_bsearch(DevFm F, const uint16_t* __rest
 // emitted in ascending fwd_lo order at the end.
 // =====================================================================================
 
+// A thread's interval set is kept as two lists in one slice of `cap` entries: intervals
+// of one row from the front ([0, n1)) and larger ones from the back ([cap-nb, cap)).  A
+// one-row interval extends only by the symbol of its row — one LF step on one record —
+// so every lane runs a cheap uniform loop over its singles, then the full 16-symbol rank
+// loop over the rest, instead of branching per interval (which diverges within a warp).
+template <class SR>
+struct TwoList {
+  SR s; uint32_t n1, nb;
+  __device__ __forceinline__ uint32_t size() const { return n1 + nb; }
+};
+
+// One row's symbol and its rank at that row (LF step of a one-row interval).
+__device__ __forceinline__ void row_symbol_rank(const DevFm& F, uint32_t row, uint32_t& sym, uint32_t& rank) {
+  uint32_t off = row & 63;
+  OccRec o = load_occ(F, row >> 6);
+  uint64_t p0 = u2to64(o.p0.x, o.p0.y), p1 = u2to64(o.p0.z, o.p0.w);
+  uint64_t p2 = u2to64(o.p1.x, o.p1.y), p3 = u2to64(o.p1.z, o.p1.w);
+  uint32_t c = (uint32_t)((p0 >> off) & 1) | ((uint32_t)((p1 >> off) & 1) << 1) |
+               ((uint32_t)((p2 >> off) & 1) << 2) | ((uint32_t)((p3 >> off) & 1) << 3);
+  uint64_t m = ((1ull << off) - 1ull) & ((c & 1) ? p0 : ~p0) & ((c & 2) ? p1 : ~p1) & ((c & 4) ? p2 : ~p2) &
+               ((c & 8) ? p3 : ~p3);
+  sym = c;
+  rank = sel16(o.c0, o.c1, o.c2, o.c3, c) + (uint32_t)__popcll(m);
+}
+
 // DIR 0 = right (ranks on the reverse index), 1 = left (ranks on the forward index).
-template <int DIR, bool COUNT_TOUCH, class SRI, class SRO>
-__device__ __forceinline__ uint32_t extend_set(const DevFm& X, const SmemFm& S, uint32_t mask, const SRI& in,
-                                               uint32_t nin, const SRO& out, uint32_t cap, uint32_t& cov,
-                                               bool& ovf, uint64_t& touches) {
-  uint32_t nout = 0; cov = 0;
-  for (uint32_t i = 0; i < nin; i++) {
-    BIv iv = in[i];
+template <int DIR, bool COUNT_TOUCH, class SR>
+__device__ __forceinline__ void extend_set(const DevFm& X, const SmemFm& S, uint32_t mask, const TwoList<SR>& in,
+                                           TwoList<SR>& out, uint32_t cap, uint32_t& cov, bool& ovf,
+                                           uint64_t& touches) {
+  out.n1 = 0; out.nb = 0; cov = 0;
+  for (uint32_t i = 0; i < in.n1; i++) {
+    BIv iv = in.s[i];
+    uint32_t a = DIR == 0 ? iv.rlo : iv.flo, base = DIR == 0 ? iv.flo : iv.rlo;
+    uint32_t s0, rk;
+    row_symbol_rank(X, a, s0, rk);
+    if (COUNT_TOUCH) touches += 1;
+    if ((mask >> s0) & 1) {
+      if (out.n1 + out.nb >= cap) { ovf = true; return; }
+      BIv e;
+      if (DIR == 0) { e.flo = base; e.fhi = base + 1; e.rlo = S.C[s0] + rk; e.rhi = S.C[s0] + rk + 1; }
+      else { e.flo = S.C[s0] + rk; e.fhi = S.C[s0] + rk + 1; e.rlo = base; e.rhi = base + 1; }
+      out.s[out.n1++] = e;
+      cov += 1;
+    }
+  }
+  for (uint32_t k = 0; k < in.nb; k++) {
+    BIv iv = in.s[cap - 1 - k];
     uint32_t a = DIR == 0 ? iv.rlo : iv.flo, b = DIR == 0 ? iv.rhi : iv.fhi;
     uint32_t base = DIR == 0 ? iv.flo : iv.rlo;
     uint32_t rl[16], rh[16];
@@ -255,25 +295,34 @@ __device__ __forceinline__ uint32_t extend_set(const DevFm& X, const SmemFm& S, 
     for (int s = 0; s < 16; s++) {
       uint32_t d = rh[s] - rl[s];
       if (((mask >> s) & 1) && d) {
-        if (nout >= cap) { ovf = true; return nout; }
+        if (out.n1 + out.nb >= cap) { ovf = true; return; }
         BIv e;
         if (DIR == 0) { e.flo = base + run; e.fhi = base + run + d; e.rlo = S.C[s] + rl[s]; e.rhi = S.C[s] + rh[s]; }
         else { e.flo = S.C[s] + rl[s]; e.fhi = S.C[s] + rh[s]; e.rlo = base + run; e.rhi = base + run + d; }
-        out[nout++] = e;
+        if (d == 1) out.s[out.n1++] = e;
+        else out.s[cap - 1 - out.nb++] = e;
         cov += d;
       }
       run += d;
     }
   }
-  return nout;
 }
 
 // Does any interval of the set extend by a compatible symbol?
 template <int DIR, bool COUNT_TOUCH, class SR>
-__device__ __forceinline__ bool any_extend(const DevFm& X, const SmemFm& S, uint32_t mask, const SR& in,
-                                           uint32_t nin, uint64_t& touches) {
-  for (uint32_t i = 0; i < nin; i++) {
-    BIv iv = in[i];
+__device__ __forceinline__ bool any_extend(const DevFm& X, const SmemFm& S, uint32_t mask, const TwoList<SR>& in,
+                                           uint32_t cap, uint64_t& touches) {
+  bool any = false;
+  for (uint32_t i = 0; i < in.n1; i++) {
+    BIv iv = in.s[i];
+    uint32_t s0, rk;
+    row_symbol_rank(X, DIR == 0 ? iv.rlo : iv.flo, s0, rk);
+    if (COUNT_TOUCH) touches += 1;
+    any |= (mask >> s0) & 1;
+  }
+  if (any) return true;
+  for (uint32_t k = 0; k < in.nb; k++) {
+    BIv iv = in.s[cap - 1 - k];
     uint32_t a = DIR == 0 ? iv.rlo : iv.flo, b = DIR == 0 ? iv.rhi : iv.fhi;
     uint32_t rl[16], rh[16];
     sym_ranks(X, S, a, rl);
@@ -317,84 +366,92 @@ __device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf,
                              const uint8_t* q, uint32_t n, const MemsParams& P, const SR& curr, const SR& nxt,
                              const SR& wa, const SR& wb, uint32_t set_cap, Cand* cands, uint32_t cand_cap,
                              Pool& ivpool, uint32_t& st, uint64_t& touches) {
+  using TL = TwoList<SR>;
   uint32_t nc = 0;
   if (n == 0 || P.min_len == 0) return 0;
   const BIv full = {0, Fw.text_len, 0, Fw.text_len};
   bool ovf = false;
   auto qmask = [&](const SmemFm& S, uint8_t c) -> uint32_t { return c < 16 ? S.compat_mask[c] : 0u; };
-  auto emit = [&](uint32_t qs, uint32_t qe, uint32_t count, const SR& ivs, uint32_t niv) -> bool {
+  auto emit = [&](uint32_t qs, uint32_t qe, uint32_t count, const TL& ivs) -> bool {
     if (nc >= cand_cap) { st |= ST_CAND_OVF; return false; }
+    uint32_t niv = ivs.size();
     uint64_t off = thread_reserve(ivpool, niv);
     if (off == ~0ull) { st |= ST_POOL_OVF; return false; }
     BIv* dst = (BIv*)ivpool.base + off;
-    for (uint32_t k = 0; k < niv; k++) dst[k] = ivs[k];
+    for (uint32_t k = 0; k < ivs.n1; k++) dst[k] = ivs.s[k];
+    for (uint32_t k = 0; k < ivs.nb; k++) dst[ivs.n1 + k] = ivs.s[set_cap - 1 - k];
     cands[nc++] = Cand{qs, qe, count, niv, off};
     return true;
+  };
+  // the full interval (the empty pattern) as a one-element list
+  auto start_full = [&](TL& t) {
+    if (full.fhi - full.flo == 1) { t.s[0] = full; t.n1 = 1; t.nb = 0; }
+    else { t.s[set_cap - 1] = full; t.n1 = 0; t.nb = 1; }
   };
   if (P.mode == 1) {
     // find_mems: raw_mem_from(i) for every start (src/fm_index/smem.rs:250-295)
     for (uint32_t i = 0; i < n; i++) {
-      SR c = curr, x = nxt;
-      c[0] = full;
-      uint32_t ncur = 1, cov = 0, j = i;
+      TL c{curr, 0, 0}, x{nxt, 0, 0};
+      start_full(c);
+      uint32_t cov = 0, j = i;
       bool matched = false;
       while (j < n) {
         uint32_t ncov;
-        uint32_t nn = extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, ncur, x, set_cap, ncov, ovf, touches);
+        extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, x, set_cap, ncov, ovf, touches);
         if (ovf) { st |= ST_SET_OVF; return ~0u; }
-        if (nn == 0) break;
-        SR t = c; c = x; x = t; ncur = nn; cov = ncov; j++; matched = true;
+        if (x.size() == 0) break;
+        TL t = c; c = x; x = t; cov = ncov; j++; matched = true;
       }
       if (!matched || j - i < P.min_len) continue;
-      bool lmax = i == 0 || !any_extend<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[i - 1]), c, ncur, touches);
+      bool lmax = i == 0 || !any_extend<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[i - 1]), c, set_cap, touches);
       if (!lmax) continue;
-      if (!emit(i, j, cov, c, ncur)) return ~0u;
+      if (!emit(i, j, cov, c)) return ~0u;
     }
     return nc;
   }
   // find_smems: collect_smem_candidates (src/fm_index/smem.rs:154-222)
   uint32_t pivot = 0;
   while (pivot < n) {
-    SR c = curr, x = nxt;
-    x[0] = full;
+    TL c{curr, 0, 0}, x{nxt, 0, 0};
+    start_full(x);
     uint32_t cov;
-    uint32_t ncur = extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[pivot]), x, 1, c, set_cap, cov, ovf, touches);
+    extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[pivot]), x, c, set_cap, cov, ovf, touches);
     if (ovf) { st |= ST_SET_OVF; return ~0u; }
-    if (ncur == 0) { pivot++; continue; }
+    if (c.size() == 0) { pivot++; continue; }
     uint32_t j = pivot + 1, reach = pivot + 1;
     for (;;) {
-      uint32_t end, nn = 0, ncov = 0;
+      uint32_t end, ncov = 0;
       bool next_empty, record;
+      x.n1 = x.nb = 0;
       if (j == n) { end = n; next_empty = true; record = true; }
       else {
-        nn = extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, ncur, x, set_cap, ncov, ovf, touches);
+        extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, x, set_cap, ncov, ovf, touches);
         if (ovf) { st |= ST_SET_OVF; return ~0u; }
-        end = j; next_empty = nn == 0; record = ncov != cov;
+        end = j; next_empty = x.size() == 0; record = ncov != cov;
       }
       if (record) {
         // right-maximal prefix [pivot, end): extend_left_maximally (smem.rs:227-243)
         reach = end;
-        SR b = c;
-        uint32_t nb = ncur, start = pivot, bcov = cov;
-        SR bufs[2] = {wa, wb};
+        TL b = c;
+        uint32_t start = pivot, bcov = cov;
+        TL bufs[2] = {TL{wa, 0, 0}, TL{wb, 0, 0}};
         int t = 0;
         while (start > 0) {
           uint32_t lcov;
-          uint32_t nl = extend_set<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[start - 1]), b, nb, bufs[t], set_cap, lcov,
-                                                   ovf, touches);
+          extend_set<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[start - 1]), b, bufs[t], set_cap, lcov, ovf, touches);
           if (ovf) { st |= ST_SET_OVF; return ~0u; }
-          if (nl == 0) break;
-          b = bufs[t]; nb = nl; bcov = lcov; t ^= 1; start--;
+          if (bufs[t].size() == 0) break;
+          b = bufs[t]; bcov = lcov; t ^= 1; start--;
         }
         if (end - start >= P.min_len) {
           // right-maximality (smem.rs:202-207); with no left extension it is next_empty
           bool rmax = end == n ||
-                      (start == pivot ? next_empty : !any_extend<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[end]), b, nb, touches));
-          if (rmax && !emit(start, end, bcov, b, nb)) return ~0u;
+                      (start == pivot ? next_empty : !any_extend<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[end]), b, set_cap, touches));
+          if (rmax && !emit(start, end, bcov, b)) return ~0u;
         }
       }
-      if (j == n || nn == 0) break;
-      SR tt = c; c = x; x = tt; ncur = nn; cov = ncov; j++;
+      if (j == n || x.size() == 0) break;
+      TL tt = c; c = x; x = tt; cov = ncov; j++;
     }
     pivot = max(reach, pivot + 1);
   }
