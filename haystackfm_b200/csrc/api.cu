@@ -371,10 +371,10 @@ static int resolve_segments(hfm_index* x, const FmDev& F, const uint32_t* seg_ro
   RET(x->uout.ensure(utotal * 8 + 8));
   RET(resolve(x, F, x->urow.as<uint32_t>(), 1, x->uoff.as<uint64_t>(), nuniq, utotal, d_bounds, nb,
               x->uout.as<uint32_t>(), launches));
-  RET(x->blockmap2.ensure(((total + EXP_T - 1) / EXP_T) * 4 + 4));
-  k_block_first<<<(unsigned)((nseg + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)nseg, EXP_T,
+  RET(x->blockmap2.ensure(((total + EXP_BLK - 1) / EXP_BLK) * 4 + 4));
+  k_block_first<<<(unsigned)((nseg + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)nseg, EXP_BLK,
                                                                      x->blockmap2.as<uint32_t>());
-  k_dedup_expand<<<(unsigned)((total + EXP_T - 1) / EXP_T), EXP_T, 0, x->stream>>>(
+  k_dedup_expand<<<(unsigned)((total + EXP_BLK - 1) / EXP_BLK), EXP_T, 0, x->stream>>>(
       seg_off, (uint32_t)nseg, total, x->hslot.as<uint32_t>(), x->huid.as<uint64_t>(), x->uoff.as<uint64_t>(),
       x->uout.as<uint2>(), reinterpret_cast<uint2*>(out), x->blockmap2.as<uint32_t>());
   other += 2;

@@ -154,27 +154,29 @@ __global__ void k_dedup_compact(const unsigned long long* __restrict__ keys, uin
   urow[u] = (uint32_t)(k >> 32); ulen[u] = (uint32_t)k;
 }
 
-// out[p] = resolved position of its segment's distinct copy
-constexpr int EXP_T = 256;
+// out[p] = resolved position of its segment's distinct copy.  A block copies EXP_BLK
+// consecutive positions (EXP_PER per thread, strided for coalescing); its segments are
+// staged in shared memory once.
+constexpr int EXP_T = 256, EXP_PER = 8, EXP_BLK = EXP_T * EXP_PER;
 __global__ void __launch_bounds__(EXP_T) k_dedup_expand(const uint64_t* __restrict__ seg_off, uint32_t nseg, uint64_t total,
                                                         const uint32_t* __restrict__ seg_slot,
                                                         const uint64_t* __restrict__ uid,
                                                         const uint64_t* __restrict__ uoff,
                                                         const uint2* __restrict__ uout, uint2* __restrict__ out,
                                                         const uint32_t* __restrict__ block_first) {
-  __shared__ uint64_t s_off[EXP_T + 1];
-  __shared__ uint64_t s_src[EXP_T];
+  __shared__ uint64_t s_off[EXP_BLK + 1];
+  __shared__ uint64_t s_src[EXP_BLK];
   __shared__ uint32_t s_first, s_cnt;
-  uint64_t p0 = (uint64_t)blockIdx.x * EXP_T;
-  uint64_t p1 = min(p0 + EXP_T, total);
+  uint64_t p0 = (uint64_t)blockIdx.x * EXP_BLK;
+  uint64_t p1 = min(p0 + EXP_BLK, total);
   if (threadIdx.x == 0) {
     uint32_t f, c;
-    block_segments(block_first, (total + EXP_T - 1) / EXP_T, nseg, f, c);
+    block_segments(block_first, (total + EXP_BLK - 1) / EXP_BLK, nseg, f, c);
     s_first = f; s_cnt = c;
   }
   __syncthreads();
   uint32_t first = s_first, cnt = s_cnt;
-  bool local = cnt <= EXP_T;
+  bool local = cnt <= EXP_BLK;
   if (local) {
     for (uint32_t k = threadIdx.x; k <= cnt; k += EXP_T) s_off[k] = seg_off[first + k];
     for (uint32_t k = threadIdx.x; k < cnt; k += EXP_T) {
@@ -183,19 +185,22 @@ __global__ void __launch_bounds__(EXP_T) k_dedup_expand(const uint64_t* __restri
     }
   }
   __syncthreads();
-  uint64_t p = p0 + threadIdx.x;
-  if (p >= p1) return;
-  uint64_t src;
-  if (local) {
-    uint32_t lo = 0, hi = cnt - 1;
-    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (s_off[mid] <= p) lo = mid; else hi = mid - 1; }
-    src = s_src[lo] + (p - s_off[lo]);
-  } else {
-    uint32_t lo = first, hi = nseg - 1;
-    while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (seg_off[mid] <= p) lo = mid; else hi = mid - 1; }
-    src = uoff[uid[seg_slot[lo]]] + (p - seg_off[lo]);
+  uint32_t lo = 0;                       // positions ascend per thread: resume the search
+  for (int k = 0; k < EXP_PER; k++) {
+    uint64_t p = p0 + threadIdx.x + (uint64_t)k * EXP_T;
+    if (p >= p1) return;
+    uint64_t src;
+    if (local) {
+      uint32_t hi = cnt - 1;
+      while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (s_off[mid] <= p) lo = mid; else hi = mid - 1; }
+      src = s_src[lo] + (p - s_off[lo]);
+    } else {
+      uint32_t l = first, hi = nseg - 1;
+      while (l < hi) { uint32_t mid = (l + hi + 1) >> 1; if (seg_off[mid] <= p) l = mid; else hi = mid - 1; }
+      src = uoff[uid[seg_slot[l]]] + (p - seg_off[l]);
+    }
+    out[p] = uout[src];
   }
-  out[p] = uout[src];
 }
 
 // ---- exclusive scan (u32 or u64 input) -> u64 output with out[n] = total ----------
