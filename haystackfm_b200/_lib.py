@@ -60,6 +60,10 @@ class HfmDevMems(C.Structure):
                 ("d_hit_offsets", C.c_void_p), ("d_hits", C.c_void_p), ("d_positions", C.c_void_p)]
 
 
+class HfmSched(C.Structure):
+    _fields_ = [("d_order", C.c_void_p), ("n_warp", C.c_uint32), ("_pad", C.c_uint32), ("d_work_log", C.c_void_p)]
+
+
 class HfmStats(C.Structure):
     _fields_ = [("ms_search", C.c_float), ("ms_resolve", C.c_float), ("ms_total", C.c_float),
                 ("ms_search_kernel", C.c_float), ("ms_resolve_kernel", C.c_float),
@@ -91,6 +95,9 @@ SIGNATURES = {
                                           C.POINTER(HfmDevHits)]),
     "hfm_mems_batch_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
                                         u32p, C.c_uint32, C.c_uint32, C.POINTER(HfmDevMems)]),
+    "hfm_mems_batch_device_sched": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
+                                              C.c_uint32, u32p, C.c_uint32, C.c_uint32, C.POINTER(HfmSched),
+                                              C.POINTER(HfmDevMems)]),
     "hfm_free": (None, [C.c_void_p]),
     "hfm_last_error": (C.c_char_p, []),
     "hfm_index_stream": (C.c_void_p, [C.c_void_p]),

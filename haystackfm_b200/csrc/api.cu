@@ -455,11 +455,29 @@ static int locate_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qof
 }
 
 static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t min_len,
-                       uint32_t mode, const uint32_t* h_bounds, uint32_t nb, uint32_t cap, hfm_dev_mems* out) {
+                       uint32_t mode, const uint32_t* h_bounds, uint32_t nb, uint32_t cap, hfm_dev_mems* out,
+                       const hfm_sched* sc = nullptr) {
   if (x->kind != HFM_KIND_BIDIR) return set_error(HFM_E_ARG, "MEM/SMEM search needs a bidirectional index");
   if (mode > 1) return set_error(HFM_E_ARG, "mode must be 0 (SMEM) or 1 (MEM)");
+  const uint32_t* order = sc ? sc->d_order : nullptr;
+  uint32_t n_warp = sc ? sc->n_warp : 0;
+  uint32_t* wlog = sc ? sc->d_work_log : nullptr;
+  if (n_warp > nq) return set_error(HFM_E_ARG, "sched.n_warp exceeds nq");
+  if (n_warp && !order) return set_error(HFM_E_ARG, "sched.n_warp needs sched.d_order");
   begin_stats(x);
   uint32_t launches = 0, other = 0;
+  if (order && nq) {
+    // the order must be a permutation of 0..nq-1: every read is processed exactly once
+    RET(x->hflags.ensure((size_t)nq * 4));
+    CK(cudaMemsetAsync(x->hflags.p, 0, (size_t)nq * 4, x->stream));
+    CK(cudaMemsetAsync(&dctr(x)->walk_err, 0, 4, x->stream));
+    k_check_perm<<<(nq + 255) / 256, 256, 0, x->stream>>>(order, nq, x->hflags.as<uint32_t>(), &dctr(x)->walk_err);
+    other++;
+    CK(cudaGetLastError());
+    RET(read_ctr(x));
+    if (x->h_ctr->walk_err) return set_error(HFM_E_ARG, "sched.d_order is not a permutation of 0..nq-1");
+  }
+  bool counting = x->count_work || wlog;
   RET(x->ref_bounds.ensure((size_t)nb * 4 + 4));
   if (nb) CK(cudaMemcpyAsync(x->ref_bounds.p, h_bounds, (size_t)nb * 4, cudaMemcpyHostToDevice, x->stream));
   RET(x->hit_start.ensure((size_t)nq * 8 + 8)); RET(x->hit_count.ensure((size_t)nq * 4 + 4));
@@ -483,15 +501,21 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
     RET(x->mivpool.ensure(x->miv_cap * 16)); x->miv_cap = x->mivpool.cap / 16;
     RET(x->hitpool.ensure(x->hit_cap * 32)); x->hit_cap = x->hitpool.cap / 32;
     CK(cudaMemsetAsync(x->ctr.p, 0, sizeof(Counters), x->stream));
+    if (wlog && nq) CK(cudaMemsetAsync(wlog, 0, (size_t)nq * 16, x->stream));
     Pool ivp{x->mivpool.p, &dctr(x)->iv_used, x->miv_cap}, hp{x->hitpool.p, &dctr(x)->hit_used, x->hit_cap};
     MemsOut o{x->hit_start.as<uint64_t>(), x->hit_count.as<uint32_t>(), x->status.as<uint32_t>(),
               x->ovf.as<uint32_t>(), &dctr(x)->n_ovf, &dctr(x)->touches};
-    if (nq) {
-      MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, nullptr, 0, &dctr(x)->queue, nullptr, nq, &dctr(x)->still_ovf};
+    if (n_warp) {   // reads the schedule sends straight to the warp-per-read kernel head the long-tail list
+      CK(cudaMemcpyAsync(x->ovf.p, order, (size_t)n_warp * 4, cudaMemcpyDeviceToDevice, x->stream));
+      CK(cudaMemcpyAsync(&dctr(x)->n_ovf, &n_warp, 4, cudaMemcpyHostToDevice, x->stream));
+    }
+    if (nq > n_warp) {
+      MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, nullptr, 0, &dctr(x)->queue, order ? order + n_warp : nullptr,
+                 nq - n_warp, &dctr(x)->still_ovf, 0u, wlog};
       unsigned grid = (unsigned)(threads / 128);
       if (x->memwork.cap < (size_t)grid * 128 * 4 * MEM_SET_CAP * 16) return set_error(HFM_E_ARG, "internal: work area too small");
       cudaEventRecord(x->evk[0], x->stream);
-      if (x->count_work)
+      if (counting)
         k_mems<true, 32, MEM_KC, 5><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                                 d_q, d_qoff, P, ivp, hp, o, W);
       else if (variant == 0)
@@ -524,8 +548,8 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
         CK(cudaMemsetAsync(&dctr(x)->still_ovf, 0, 4, x->stream));
         CK(cudaMemsetAsync(&dctr(x)->queue2, 0, 4, x->stream));
         MemsWork W{x->work.as<BIv>(), set_cap, x->cwork.as<Cand>(), cand_cap, &dctr(x)->queue2, x->ovf.as<uint32_t>(),
-                   n_ovf, &dctr(x)->still_ovf};
-        if (x->count_work)
+                   n_ovf, &dctr(x)->still_ovf, 1u, wlog};
+        if (counting)
           k_mems_warp<true><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                         d_q, d_qoff, P, ivp, hp, o, W);
         else
@@ -565,6 +589,11 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   RET(read_u64(x, x->npos_scan.as<uint64_t>() + nh, npos));
   if (nh) {
     k_set_pos_off<<<(unsigned)((nh + 255) / 256), 256, 0, x->stream>>>(x->hits.as<uint32_t>(), x->npos_scan.as<uint64_t>(), nh);
+    other++;
+    CK(cudaGetLastError());
+  }
+  if (wlog && nq) {
+    k_work_log<<<(nq + 255) / 256, 256, 0, x->stream>>>(x->hit_base.as<uint64_t>(), x->npos_scan.as<uint64_t>(), nq, wlog);
     other++;
     CK(cudaGetLastError());
   }
@@ -754,6 +783,14 @@ int hfm_mems_batch_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qo
   if (!x || !out || (nq && !d_qoff) || (nb && !ref_bounds)) return set_error(HFM_E_ARG, "NULL argument");
   Guard g(x);
   return mems_device(x, d_q, d_qoff, nq, min_len, mode, ref_bounds, nb, cap, out);
+}
+
+int hfm_mems_batch_device_sched(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq,
+                                uint32_t min_len, uint32_t mode, const uint32_t* ref_bounds, uint32_t nb, uint32_t cap,
+                                const hfm_sched* sched, hfm_dev_mems* out) {
+  if (!x || !out || (nq && !d_qoff) || (nb && !ref_bounds)) return set_error(HFM_E_ARG, "NULL argument");
+  Guard g(x);
+  return mems_device(x, d_q, d_qoff, nq, min_len, mode, ref_bounds, nb, cap, out, sched);
 }
 
 int hfm_count_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32_t nq, uint32_t* counts_out) {

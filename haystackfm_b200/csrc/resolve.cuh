@@ -303,4 +303,24 @@ __global__ void k_set_pos_off(uint32_t* __restrict__ hits, const uint64_t* __res
   hits[i * 8 + 6] = (uint32_t)o; hits[i * 8 + 7] = (uint32_t)(o >> 32);
 }
 
+// Per-read work record, words 1 and 2: MemHits and positions reported for read i.
+__global__ void k_work_log(const uint64_t* __restrict__ hit_base, const uint64_t* __restrict__ npos_scan, uint32_t nq,
+                           uint32_t* __restrict__ log) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  uint64_t h0 = hit_base[i], h1 = hit_base[i + 1];
+  log[4 * (size_t)i + 1] = (uint32_t)(h1 - h0);
+  uint64_t np = npos_scan[h1] - npos_scan[h0];
+  log[4 * (size_t)i + 2] = np > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)np;
+}
+
+// seen[] zeroed by the caller; *bad set when ids is not a permutation of 0..n-1.
+__global__ void k_check_perm(const uint32_t* __restrict__ ids, uint32_t n, uint32_t* __restrict__ seen,
+                             uint32_t* __restrict__ bad) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  uint32_t i = ids[k];
+  if (i >= n || atomicExch(seen + i, 1u) != 0) atomicExch(bad, 1u);
+}
+
 }  // namespace hfm

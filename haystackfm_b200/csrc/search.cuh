@@ -510,8 +510,10 @@ struct MemsWork {
   BIv* sets; uint32_t set_cap;        // 4 sets per thread
   Cand* cands; uint32_t cand_cap;     // contiguous per thread (fallback pass); nullptr: local
   unsigned int* queue;
-  const uint32_t* ids; uint32_t n;    // reads to process (ids == nullptr: 0..n-1)
+  const uint32_t* ids; uint32_t n;    // reads to process, in queue order (ids == nullptr: 0..n-1)
   uint32_t* still_ovf;
+  uint32_t rerun;                     // 1: a rerun of overflowed reads (counted in still_ovf)
+  uint32_t* work_log;                 // COUNT_TOUCH only: 4 u32 per read, [0] += Occ touches, [3] |= 1 on overflow
 };
 
 template <bool COUNT_TOUCH, int STRIDE, int KC, int MINB>
@@ -539,6 +541,7 @@ __global__ void __launch_bounds__(128, MINB) k_mems(DevFm Fw, DevFm Rv, const ui
   while (next_read(W.queue, W.n, W.ids, i)) {
     uint32_t st = ST_OK;
     uint64_t o = qoff[i];
+    uint64_t t0 = touches;
     uint32_t nc = mems_one<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, (uint32_t)(qoff[i + 1] - o), P, s0, s1, s2, s3,
                                         W.set_cap, cands, cand_cap, ivpool, st, touches);
     uint64_t hs = 0; uint32_t hc = 0;
@@ -548,8 +551,13 @@ __global__ void __launch_bounds__(128, MINB) k_mems(DevFm Fw, DevFm Rv, const ui
     }
     if (st) { hs = 0; hc = 0; }
     out.hit_start[i] = hs; out.hit_count[i] = hc; out.status[i] = st;
-    if (st & (ST_SET_OVF | ST_CAND_OVF)) {
-      if (W.ids) atomicAdd(W.still_ovf, 1u);
+    bool ovf = st & (ST_SET_OVF | ST_CAND_OVF);
+    if (COUNT_TOUCH && W.work_log) {
+      W.work_log[4 * (size_t)i] += (uint32_t)(touches - t0);
+      if (ovf) W.work_log[4 * (size_t)i + 3] |= 1u;
+    }
+    if (ovf) {
+      if (W.rerun) atomicAdd(W.still_ovf, 1u);
       else out.ovf_list[atomicAdd(out.n_ovf, 1u)] = i;
     }
   }
@@ -891,10 +899,15 @@ __global__ void __launch_bounds__(128) k_mems_warp(DevFm Fw, DevFm Rv, const uin
     uint32_t i = W.ids[k];
     uint32_t st = ST_OK;
     uint64_t o = qoff[i];
+    uint64_t t0 = touches;
     uint32_t nc = warp_mems_one<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, (uint32_t)(qoff[i + 1] - o), P, base,
                                              base + W.set_cap, base + 2 * W.set_cap, base + 3 * W.set_cap, W.set_cap,
                                              cands, W.cand_cap, ivpool, st, touches);
     __syncwarp();
+    if (COUNT_TOUCH && W.work_log) {
+      uint32_t d = warp_sum((uint32_t)(touches - t0));
+      if (lane == 0) { W.work_log[4 * (size_t)i] += d; W.work_log[4 * (size_t)i + 3] |= 1u; }
+    }
     if (lane == 0) {
       uint64_t hs = 0; uint32_t hc = 0;
       if (nc != ~0u) {

@@ -173,6 +173,53 @@ class _Handle:
         return hit_off, hits, pos
 
 
+    def mems_sched_packed(self, flat: np.ndarray, off: np.ndarray, min_len: int, mode: int, ref_bounds,
+                          max_hits: int, order=None, n_warp: int = 0, work_log: bool = False):
+        """hfm_mems_batch_device_sched on a host batch staged through torch device tensors.
+
+        order: permutation of 0..nq-1 (queue order) or None; n_warp: the first n_warp reads
+        of `order` run on the warp-per-read kernel.  -> (hit_offsets, hits, positions, log)
+        with log u32[nq, 4] (touches, MemHits, positions, flags) when work_log, else None."""
+        import torch
+        nq = len(off) - 1
+        dev = torch.device("cuda", self.device)
+        q_d = torch.from_numpy(np.ascontiguousarray(flat, dtype=np.uint8)).to(dev)
+        off_d = torch.from_numpy(np.ascontiguousarray(off, dtype=np.uint64).view(np.int64)).to(dev)
+        ord_d = (torch.from_numpy(np.ascontiguousarray(order, dtype=np.uint32).view(np.int32)).to(dev)
+                 if order is not None else None)
+        log_d = torch.zeros(max(4 * nq, 1), dtype=torch.int32, device=dev) if work_log else None
+        rb = np.ascontiguousarray(ref_bounds if ref_bounds is not None else [], dtype=np.uint32)
+        rbp = L.ptr(rb, L.u32p) if len(rb) else None
+        sc = L.HfmSched(ord_d.data_ptr() if ord_d is not None else None, n_warp, 0,
+                        log_d.data_ptr() if log_d is not None else None)
+        dm = L.HfmDevMems()
+        torch.cuda.synchronize(dev)
+        L.check(L.lib().hfm_mems_batch_device_sched(self.h, q_d.data_ptr(), off_d.data_ptr(), nq, min_len, mode,
+                                                    rbp, len(rb), max_hits, C.byref(sc), C.byref(dm)))
+        hit_off = device_to_host(dm.d_hit_offsets, nq + 1, "<i8", dev).view(np.uint64)
+        hits = device_to_host(dm.d_hits, 8 * dm.n_hits, "<i4", dev).view(np.uint32).reshape(-1, 8)
+        pos = device_to_host(dm.d_positions, 2 * dm.n_positions, "<i4", dev).view(np.uint32).reshape(-1, 2)
+        log = log_d[:4 * nq].cpu().numpy().view(np.uint32).reshape(nq, 4) if work_log else None
+        return hit_off, hits, pos, log
+
+
+class _DeviceArray:
+    """A raw device pointer exposed through __cuda_array_interface__ (read by torch)."""
+
+    def __init__(self, ptr: int, n: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3}
+
+
+def device_to_host(ptr, n: int, typestr: str, device) -> np.ndarray:
+    """Copy n elements at a library-owned device pointer to a new numpy array."""
+    import torch
+    dt = {"<i4": np.int32, "<i8": np.int64, "<f4": np.float32}[typestr]
+    if n == 0 or not ptr:
+        return np.zeros(0, dtype=dt)
+    with torch.cuda.device(device):
+        return torch.as_tensor(_DeviceArray(int(ptr), int(n), typestr), device=device).cpu().numpy()
+
+
 class FmIndex:
     """Device-resident FmIndex (src/fm_index/mod.rs:58-72)."""
 

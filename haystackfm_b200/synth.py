@@ -10,6 +10,9 @@ shapes and value distributions of the two workloads:
   (geometric run lengths, mean 500) and 0.5% single ambiguity codes (R..V uniform).  Reads
   (150 bp) are drawn from either strand of the unmasked ACGT sequence — the N runs and
   ambiguity codes mask only the reference — with 1% substitutions and 0.1% N.
+* sample_mixed_reads — mixed-length reads on the same reference: 80% 150 bp (1%
+  substitutions), 20% lognormal lengths (median 3 kbp, clipped to 100 bp .. 10 kbp) with 8%
+  mixed substitutions / insertions / deletions.
 """
 from __future__ import annotations
 
@@ -91,6 +94,69 @@ def sample_reads(ref: Reference, n_reads=1_000_000, read_len=150, sub_rate=0.01,
     reads = np.where(sub, ((reads - 1 + shift) % 4) + 1, reads).astype(np.uint8)
     reads[rng.random(reads.shape) < n_rate] = N
     return reads
+
+
+def _mutate(seq: np.ndarray, rate: float, rng) -> np.ndarray:
+    """Mixed errors at `rate` per base: substitutions, 1-base insertions and deletions in
+    equal shares."""
+    ev = rng.random(len(seq))
+    kind = rng.integers(0, 3, size=len(seq))
+    hit = ev < rate
+    sub = hit & (kind == 0)
+    ins = hit & (kind == 1)
+    dele = hit & (kind == 2)
+    out = seq.copy()
+    shift = rng.integers(1, 4, size=len(seq), dtype=np.uint8)
+    out[sub] = ((out[sub] - 1 + shift[sub]) % 4) + 1
+    reps = np.ones(len(seq), dtype=np.int64)
+    reps[dele] = 0
+    reps[ins] = 2
+    res = np.repeat(out, reps)
+    # the second copy of an inserted base becomes a random base
+    first = np.cumsum(reps) - reps
+    pos = first[ins] + 1
+    res[pos] = rng.integers(1, 5, size=len(pos), dtype=np.uint8)
+    return res
+
+
+def sample_mixed_reads(ref: Reference, n_reads=200_000, short_frac=0.8, short_len=150, long_median=3000,
+                       long_sigma=0.6, min_len=100, max_len=10_000, short_sub=0.01, long_err=0.08,
+                       n_rate=0.001, seed=5):
+    """Mixed-length reads as a flat batch: `short_frac` of fixed `short_len` reads with
+    substitutions, the rest lognormal (median `long_median`, clipped to [min_len, max_len])
+    with mixed substitutions / insertions / deletions at `long_err`; either strand, Ns at
+    `n_rate`.  Returns (flat u8 codes, u64 offsets[n+1], lengths)."""
+    rng = np.random.default_rng(seed)
+    is_long = rng.random(n_reads) >= short_frac
+    lens = np.full(n_reads, short_len, dtype=np.int64)
+    ll = np.exp(np.log(long_median) + long_sigma * rng.standard_normal(int(is_long.sum())))
+    lens[is_long] = np.clip(ll.astype(np.int64), min_len, max_len)
+    src_len = np.where(is_long, (lens * 1.05).astype(np.int64) + 8, lens)   # room for deletions
+    clen = np.array([len(t) for t in ref.truth])
+    # contig by length-weighted draw among contigs that hold the longest source span
+    w_all = (clen - src_len.max() + 1).clip(min=0).astype(np.float64)
+    cid = rng.choice(len(clen), size=n_reads, p=w_all / w_all.sum())
+    starts = (rng.random(n_reads) * (clen[cid] - src_len + 1)).astype(np.int64)
+    rc = rng.random(n_reads) < 0.5
+    out = []
+    for i in range(n_reads):
+        s = ref.truth[cid[i]][starts[i]:starts[i] + src_len[i]]
+        if rc[i]:
+            s = (5 - s)[::-1]
+        if is_long[i]:
+            s = _mutate(np.ascontiguousarray(s), long_err, rng)[:lens[i]]
+        else:
+            s = s.copy()
+            sub = rng.random(len(s)) < short_sub
+            shift = rng.integers(1, 4, size=len(s), dtype=np.uint8)
+            s[sub] = ((s[sub] - 1 + shift[sub]) % 4) + 1
+        out.append(s)
+    lens = np.array([len(s) for s in out], dtype=np.int64)
+    flat = np.concatenate(out).astype(np.uint8) if out else np.zeros(0, np.uint8)
+    flat[rng.random(len(flat)) < n_rate] = N
+    off = np.zeros(n_reads + 1, dtype=np.uint64)
+    np.cumsum(lens, out=off[1:])
+    return flat, off, lens
 
 
 def pack_rows(rows: np.ndarray, width=None):

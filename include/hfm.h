@@ -180,6 +180,28 @@ int hfm_mems_batch_device(hfm_index* idx, const uint8_t* d_q, const uint64_t* d_
 int hfm_count_batch_noalloc(hfm_index* idx, const uint8_t* d_q, const uint64_t* d_q_off, uint32_t nq,
                             uint32_t* d_counts_out);
 
+/* Scheduled SMEM/MEM search (no counterpart in the reference): the hook of the learned
+ * read scheduler.  Results are identical to hfm_mems_batch_device for every schedule.
+ *   d_order    device permutation of 0..nq-1: the order in which the persistent per-thread
+ *              kernel takes reads from its queue (NULL: 0..nq-1).  Checked on the device;
+ *              anything else is HFM_E_ARG before any search runs.
+ *   n_warp     the first n_warp reads of d_order skip the per-thread kernel and go to the
+ *              warp-per-read kernel (reads predicted to outgrow per-thread interval sets).
+ *   d_work_log device array of 4*nq u32, or NULL.  When set, the call runs the counting
+ *              kernel variants and logs the exact work of each read i:
+ *              [4i] Occ record touches (backward and forward extension steps, every pass),
+ *              [4i+1] MemHits reported, [4i+2] positions reported,
+ *              [4i+3] bit 0: the read ran on the warp-per-read kernel. */
+typedef struct hfm_sched {
+  const uint32_t* d_order;
+  uint32_t n_warp;
+  uint32_t _pad;
+  uint32_t* d_work_log;
+} hfm_sched;
+int hfm_mems_batch_device_sched(hfm_index* idx, const uint8_t* d_q, const uint64_t* d_q_off, uint32_t nq,
+                                uint32_t min_len, uint32_t mode, const uint32_t* ref_bounds, uint32_t n_bounds,
+                                uint32_t max_hits, const hfm_sched* sched, hfm_dev_mems* out);
+
 /* ---- misc ----------------------------------------------------------------- */
 void hfm_free(void* p);                    /* frees hfm_hits*, hfm_mem_out*, build bytes */
 const char* hfm_last_error(void);          /* thread-local message of the last failure   */

@@ -1,0 +1,83 @@
+"""The scheduled SMEM entry point: any read order and any warp routing give the oracle's
+bytes, and the per-read work log agrees with the results it describes."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from haystackfm_b200 import alphabet as al
+from haystackfm_b200 import synth
+from haystackfm_b200.errors import FmIndexError
+from haystackfm_b200.fm_index import BidirFmIndex, FmIndexConfig, KIND_BIDIR, _build
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def mixed_case(oracle):
+    """2 Mbp IUPAC reference; 240 mixed-length reads (150 bp and 100 bp .. 10 kbp)."""
+    ref = synth.iupac_reference(total=2_000_000, n_contigs=20, seed=31)
+    flat, off, lens = synth.sample_mixed_reads(ref, n_reads=240, seed=32)
+    b = _build([al.DnaSequence(c) for c in ref.contigs], FmIndexConfig(sa_sample_rate=32, lookup_depth=10), 0,
+               KIND_BIDIR)
+    idx = BidirFmIndex.from_bytes(b)
+    bounds = idx.seq_boundaries()
+    want = oracle.OracleIndex(b, KIND_BIDIR).mems_packed(flat, off, 19, 0, bounds, 64, threads=8)
+    return idx, flat, off, lens, bounds, want
+
+
+def _same(got, want):
+    for g, w in zip(got[:3], want):
+        assert np.array_equal(g, w)
+
+
+def test_orders_and_routing_bit_exact(mixed_case):
+    idx, flat, off, lens, bounds, want = mixed_case
+    h = idx.handle
+    nq = len(off) - 1
+    rng = np.random.default_rng(0)
+    _same(h.mems_sched_packed(flat, off, 19, 0, bounds, 64), want)
+    _same(h.mems_sched_packed(flat, off, 19, 0, bounds, 64, order=np.arange(nq)[::-1]), want)
+    perm = rng.permutation(nq)
+    _same(h.mems_sched_packed(flat, off, 19, 0, bounds, 64, order=perm), want)
+    _same(h.mems_sched_packed(flat, off, 19, 0, bounds, 64, order=perm, n_warp=17), want)
+    _same(h.mems_sched_packed(flat, off, 19, 0, bounds, 64, order=np.argsort(-lens), n_warp=nq), want)
+
+
+def test_work_log(mixed_case):
+    idx, flat, off, lens, bounds, want = mixed_case
+    h = idx.handle
+    nq = len(off) - 1
+    order = np.argsort(-lens, kind="stable")
+    got = h.mems_sched_packed(flat, off, 19, 0, bounds, 64, order=order, n_warp=5, work_log=True)
+    _same(got, want)
+    hit_off, hits, _, log = got
+    assert np.array_equal(log[:, 1], np.diff(hit_off.astype(np.int64)))
+    npos = np.add.reduceat(np.r_[hits[:, 5].astype(np.int64), 0], hit_off[:-1].astype(np.int64))
+    npos[np.diff(hit_off.astype(np.int64)) == 0] = 0
+    assert np.array_equal(log[:, 2], npos)
+    assert (log[:, 0] > 0).all()
+    assert (log[order[:5], 3] & 1).all()             # routed reads ran on the warp kernel
+    # longer reads do more extension work
+    assert np.corrcoef(lens, log[:, 0].astype(np.float64))[0, 1] > 0.6
+    # the log does not depend on the order for reads that stay on one kernel
+    got2 = h.mems_sched_packed(flat, off, 19, 0, bounds, 64, work_log=True)
+    same_path = ((got2[3][:, 3] & 1) == 0) & ((log[:, 3] & 1) == 0)
+    assert np.array_equal(got2[3][same_path, 0], log[same_path, 0])
+
+
+def test_bad_order_rejected(mixed_case):
+    idx, flat, off, lens, bounds, want = mixed_case
+    h = idx.handle
+    nq = len(off) - 1
+    bad = np.arange(nq)
+    bad[3] = 4                                        # duplicate: not a permutation
+    with pytest.raises(FmIndexError):
+        h.mems_sched_packed(flat, off, 19, 0, bounds, 64, order=bad)
+    big = np.arange(nq)
+    big[0] = nq                                       # out of range
+    with pytest.raises(FmIndexError):
+        h.mems_sched_packed(flat, off, 19, 0, bounds, 64, order=big)
+    with pytest.raises(FmIndexError):
+        h.mems_sched_packed(flat, off, 19, 0, bounds, 64, order=None, n_warp=3)
+    _same(h.mems_sched_packed(flat, off, 19, 0, bounds, 64), want)   # handle still usable
