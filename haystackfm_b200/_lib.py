@@ -98,6 +98,20 @@ SIGNATURES = {
     "hfm_mems_batch_device_sched": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32,
                                               C.c_uint32, u32p, C.c_uint32, C.c_uint32, C.POINTER(HfmSched),
                                               C.POINTER(HfmDevMems)]),
+    "hfm_mlp_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(C.c_void_p)]),
+    "hfm_mlp_free": (None, [C.c_void_p]),
+    "hfm_mlp_set_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "hfm_mlp_get_params": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "hfm_mlp_stream": (C.c_void_p, [C.c_void_p]),
+    "hfm_mlp_features": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "hfm_mlp_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "hfm_mlp_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]),
+    "hfm_mlp_grad": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                               C.POINTER(C.c_float)]),
+    "hfm_mlp_train": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
+    "hfm_mlp_schedule": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p,
+                                   C.POINTER(C.c_uint32)]),
     "hfm_free": (None, [C.c_void_p]),
     "hfm_last_error": (C.c_char_p, []),
     "hfm_index_stream": (C.c_void_p, [C.c_void_p]),

@@ -202,6 +202,44 @@ int hfm_mems_batch_device_sched(hfm_index* idx, const uint8_t* d_q, const uint64
                                 uint32_t min_len, uint32_t mode, const uint32_t* ref_bounds, uint32_t n_bounds,
                                 uint32_t max_hits, const hfm_sched* sched, hfm_dev_mems* out);
 
+/* ---- learned read-cost model (no counterpart in the reference) -------------
+ * A 257 -> 128 -> 128 -> 3 ReLU MLP (BF16 weights and activations, FP32 accumulation)
+ * predicting, per read, log1p of the exact SMEM kernel's work log (hfm_sched.d_work_log):
+ * Occ touches, MemHits, positions.  Input row (HFM_MLP_IN_PAD BF16 values): 256 4-mer
+ * frequencies x[f] = 256*c_f/V - 1 (V = 4-mers without an ambiguity code; all 0 when
+ * V == 0), x[256] = (log2(len+1) - 10)/4, zeros to the end.  Parameters (FP32, in this
+ * order): W1[128][272], b1[128], W2[128][128], b2[128], W3[3][128], b3[3]; W1 columns
+ * 257..271 multiply zero inputs.  Training runs the model's own forward and backward CUDA
+ * kernels and Adam (lr as given, betas 0.9 / 0.999, eps 1e-8) on the MSE of the outputs.
+ * Every call completes its work before returning; device arrays must be 16-byte aligned. */
+#define HFM_MLP_IN_PAD 272
+#define HFM_MLP_HIDDEN 128
+#define HFM_MLP_OUT 3
+#define HFM_MLP_NPARAM (128 * 272 + 128 + 128 * 128 + 128 + 3 * 128 + 3)
+typedef struct hfm_mlp hfm_mlp;
+int hfm_mlp_create(int device, uint64_t seed, hfm_mlp** out);      /* He-uniform init from seed */
+void hfm_mlp_free(hfm_mlp* m);
+int hfm_mlp_set_params(hfm_mlp* m, const float* params);          /* host, HFM_MLP_NPARAM; resets Adam */
+int hfm_mlp_get_params(hfm_mlp* m, float* params);                /* host, HFM_MLP_NPARAM */
+void* hfm_mlp_stream(hfm_mlp* m);
+/* d_x[nq][HFM_MLP_IN_PAD] (BF16 bits) from encoded reads */
+int hfm_mlp_features(hfm_mlp* m, const uint8_t* d_q, const uint64_t* d_q_off, uint32_t nq, uint16_t* d_x);
+/* d_y[n][3] = model(d_x) */
+int hfm_mlp_forward(hfm_mlp* m, const uint16_t* d_x, uint32_t n, float* d_y);
+/* features + forward: d_y[nq][3] predicted log1p(touches, MemHits, positions) */
+int hfm_mlp_predict(hfm_mlp* m, const uint8_t* d_q, const uint64_t* d_q_off, uint32_t nq, float* d_y);
+/* gradient of the MSE over all n rows (one batch) into d_grad[HFM_MLP_NPARAM]; *loss = MSE */
+int hfm_mlp_grad(hfm_mlp* m, const uint16_t* d_x, const float* d_t, uint32_t n, float* d_grad, float* loss);
+/* Adam over shuffled mini-batches (Fisher-Yates order from seed); loss_per_epoch[epochs] or NULL */
+int hfm_mlp_train(hfm_mlp* m, const uint16_t* d_x, const float* d_t, uint32_t n, uint32_t epochs,
+                  uint32_t batch, float lr, uint64_t seed, float* loss_per_epoch);
+/* Schedule for hfm_mems_batch_device_sched: d_order = reads binned by predicted Occ
+ * touches (4096 bins, costliest first); reads predicted to report at least warp_min_hits
+ * MemHits (<= 0: none) come first and are counted in *n_warp (routed to the warp kernel).
+ * Within a bin the order is unspecified; results never depend on it. */
+int hfm_mlp_schedule(hfm_mlp* m, const float* d_y, uint32_t nq, float warp_min_hits, uint32_t* d_order,
+                     uint32_t* n_warp);
+
 /* ---- misc ----------------------------------------------------------------- */
 void hfm_free(void* p);                    /* frees hfm_hits*, hfm_mem_out*, build bytes */
 const char* hfm_last_error(void);          /* thread-local message of the last failure   */
