@@ -54,6 +54,14 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="time the plain order only")
+    ap.add_argument("--train-reads", type=int, default=1_000_000,
+                    help="reads (a separate seeded sample) whose logged work trains the cost model")
+    ap.add_argument("--train-epochs", type=int, default=4)
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-length workload")
+    ap.add_argument("--mixed-reads", type=int, default=200_000)
+    ap.add_argument("--no-serving", action="store_true", help="skip the batch-latency measurement")
+    ap.add_argument("--serving-batches", type=int, default=300)
     ap.add_argument("--profile-smem", action="store_true",
                     help="one SMEM search launch (no position resolve) for ncu, then its work counters")
     return ap.parse_args()
@@ -203,6 +211,118 @@ def profile_smem(args):
                       "occ_touches": h.stats().occ_touches}), flush=True)
 
 
+def serving_latency(h, lib, L, kp, rp, bounds, n, n_batches, seed=17):
+    """Batch latency through the host-buffer C ABI: batches of log-uniform size 1..100,000
+    reads (mean ~8.7k) taken from the workload's reads, each a locate of the first 32-mer
+    plus find_smems with every result copied back, issued back to back on one handle.
+    -> p50 / p99 / max latency per batch and the sustained reads/s."""
+    rng = np.random.default_rng(seed)
+    sizes = np.minimum(np.exp(rng.uniform(0, np.log(100_000), n_batches)).astype(np.int64), n)
+    starts = rng.integers(0, n - sizes + 1)
+    nb = len(bounds)
+    lat = []
+    t_all = time.perf_counter()
+    for a, m in zip(starts, sizes):
+        a, m = int(a), int(m)
+        off150 = np.arange(0, (m + 1) * 150, 150, dtype=np.uint64)
+        off32 = np.arange(0, (m + 1) * 32, 32, dtype=np.uint64)
+        t0 = time.perf_counter()
+        res = C.POINTER(L.HfmHits)()
+        L.check(lib.hfm_locate_batch(h.h, L.ptr(kp[a * 32:], L.u8p), L.ptr(off32, L.u64p), m, 1024, C.byref(res)))
+        mo = C.POINTER(L.HfmMemOut)()
+        L.check(lib.hfm_mems_batch(h.h, L.ptr(rp[a * 150:], L.u8p), L.ptr(off150, L.u64p), m, 19, 0,
+                                   L.ptr(bounds, L.u32p), nb, 1024, C.byref(mo)))
+        lat.append((time.perf_counter() - t0) * 1e3)
+        lib.hfm_free(res)
+        lib.hfm_free(mo)
+    total_s = time.perf_counter() - t_all
+    lat = np.array(lat)
+    return {"batches": int(n_batches), "batch_reads": "log-uniform 1..100000", "mean_batch": float(sizes.mean()),
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "max_ms": float(lat.max()), "reads_per_s": float(sizes.sum() / total_s),
+            "path": "hfm_locate_batch + hfm_mems_batch, host buffers, one handle, back to back"}
+
+
+def mixed_workload(args, device, torch):
+    """Mixed-length reads (80% 150 bp, 20% lognormal median 3 kbp up to 10 kbp, 8% indel
+    errors) on an ACGT-only 100 Mbp genome with repeat families and tandem repeats
+    (ExactDna bidirectional index, rate 32, lookup 10): locate of each read's first 32-mer +
+    find_smems (min_len 19, max_hits 1024), plain order vs the learned schedule."""
+    from haystackfm_b200 import alphabet as al, synth
+    from haystackfm_b200 import _lib as L
+    from haystackfm_b200.cost_model import LearnedSmem, prediction_error, work_targets
+    from haystackfm_b200.fm_index import BidirFmIndex, FmIndexConfig, KIND_BIDIR, _build
+    t0 = time.time()
+    ref = synth.repeat_reference(total=args.ref_len, seed=11)
+    key = hashlib.sha1(f"repeat-v1-{args.ref_len}-11-exact-rate32-lut10".encode()).hexdigest()[:16]
+    path = os.path.join(tempfile.gettempdir(), "hfm_bench_cache", key + ".bin")
+    if os.path.exists(path):
+        data = open(path, "rb").read()
+    else:
+        data = _build([al.DnaSequence(c) for c in ref.contigs],
+                      FmIndexConfig(sa_sample_rate=32, lookup_depth=10, build_threads=2), 1, KIND_BIDIR)
+        tmp = path + f".{os.getpid()}"
+        with open(tmp, "wb") as f:
+            f.write(data)
+        os.replace(tmp, path)
+    idx = BidirFmIndex.from_bytes(data, device=device)
+    h = idx.handle
+    lib = L.lib()
+    bounds = np.ascontiguousarray(idx.seq_boundaries(), dtype=np.uint32)
+    nb = len(bounds)
+    m = args.mixed_reads
+    flat, off, lens = synth.sample_mixed_reads(ref, n_reads=m, seed=5, n_rate=0.0)
+    flat_t, off_t, _ = synth.sample_mixed_reads(ref, n_reads=m, seed=6, n_rate=0.0)
+    dev = torch.device("cuda", device)
+    q = torch.from_numpy(flat).to(dev)
+    o = torch.from_numpy(off.view(np.int64)).to(dev)
+    k32 = torch.from_numpy(np.ascontiguousarray(np.stack([flat[int(a):int(a) + 32] for a in off[:-1]]))
+                           .reshape(-1)).to(dev)
+    o32 = torch.arange(0, (m + 1) * 32, 32, dtype=torch.int64, device=dev)
+    setup_s = time.time() - t0
+    ls = LearnedSmem(h, device, seed=1)
+    qt = torch.from_numpy(flat_t).to(dev)
+    ot = torch.from_numpy(off_t.view(np.int64)).to(dev)
+    losses, _, _ = ls.fit(qt, ot, m, 19, 0, bounds, 1024, epochs=8, batch=4096, lr=1e-3)
+    del qt, ot
+    ev_log = ls.log_work(q, o, m, 19, 0, bounds, 1024)
+    _, _, y = ls.plan(q, o, m)
+    err = prediction_error(y, work_targets(ev_log)).as_dict()
+    del ev_log
+
+    def step(learned):
+        dh = L.HfmDevHits()
+        L.check(lib.hfm_locate_batch_device(h.h, k32.data_ptr(), o32.data_ptr(), m, 1024, C.byref(dh)))
+        if learned:
+            ls.run(q, o, m, 19, 0, L.ptr(bounds, L.u32p), nb, 1024)
+        else:
+            dm = L.HfmDevMems()
+            L.check(lib.hfm_mems_batch_device(h.h, q.data_ptr(), o.data_ptr(), m, 19, 0, L.ptr(bounds, L.u32p), nb,
+                                              1024, C.byref(dm)))
+
+    stream = torch.cuda.ExternalStream(h.stream(), device=dev)
+    res = {}
+    for name, learned in (("plain", False), ("learned", True)):
+        for _ in range(max(args.warmup, 3)):
+            step(learned)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step(learned)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        res[name] = e0.elapsed_time(e1) / args.steps
+    return {"workload": "mixed_length_repeats_locate_smem", "reads": m, "read_mbp": round(len(flat) / 1e6, 1),
+            "genome": f"{args.ref_len // 1_000_000} Mbp ACGT, 40% interspersed repeats, 5% tandem repeats",
+            "alphabet": "ExactDna", "setup_s": round(setup_s, 1),
+            "plain_ms_per_step": res["plain"], "plain_reads_per_s": m / (res["plain"] / 1000),
+            "learned_ms_per_step": res["learned"], "learned_reads_per_s": m / (res["learned"] / 1000),
+            "learned_enabled": bool(ls.enabled), "calibration": ls.calibration,
+            "holdout_error": ls.holdout_error.as_dict() if ls.holdout_error else None, "eval_error": err,
+            "train_mse": [round(float(v), 4) for v in losses]}
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -245,23 +365,51 @@ def main():
     torch.cuda.synchronize()
     stream = torch.cuda.ExternalStream(h.stream(), device=dev)
 
-    def step(stats_out=None):
+    # learned cost model: trained on the logged work of a separate seeded read sample
+    learned, learned_info = None, None
+    if not args.no_learned:
+        from haystackfm_b200.cost_model import LearnedSmem, prediction_error, work_targets
+        tr = synth.sample_reads(ref, n_reads=args.train_reads, seed=1000 + rank)
+        tr_d = torch.from_numpy(tr.reshape(-1)).to(dev)
+        tr_off = torch.arange(0, (args.train_reads + 1) * 150, 150, dtype=torch.int64, device=dev)
+        learned = LearnedSmem(h, local, seed=1)
+        t0 = time.perf_counter()
+        losses, _, _ = learned.fit(tr_d, tr_off, args.train_reads, 19, 0, bounds, 1024, epochs=args.train_epochs,
+                                   batch=8192, lr=1e-3)
+        torch.cuda.synchronize()
+        fit_s = time.perf_counter() - t0
+        del tr_d, tr_off
+        ev_log = learned.log_work(reads_d, off_d, n, 19, 0, bounds, 1024)
+        _, _, y_ev = learned.plan(reads_d, off_d, n)
+        learned_info = {"train_reads": args.train_reads, "epochs": args.train_epochs, "fit_s": round(fit_s, 2),
+                        "train_mse": [round(float(v), 5) for v in losses],
+                        "holdout_error": learned.holdout_error.as_dict() if learned.holdout_error else None,
+                        "eval_error": prediction_error(y_ev, work_targets(ev_log)).as_dict(),
+                        "enabled": bool(learned.enabled)}
+        del ev_log
+
+    def step(stats_out=None, plain=False):
         dh = L.HfmDevHits()
         L.check(lib.hfm_locate_batch_device(h.h, k32_d.data_ptr(), off32_d.data_ptr(), n, 1024, C.byref(dh)))
         s1 = h.stats()
-        dm = L.HfmDevMems()
-        L.check(lib.hfm_mems_batch_device(h.h, reads_d.data_ptr(), off_d.data_ptr(), n, 19, 0,
-                                          L.ptr(bounds, L.u32p), nb, 1024, C.byref(dm)))
+        if learned is not None and not plain:
+            dm = learned.run(reads_d, off_d, n, 19, 0, L.ptr(bounds, L.u32p), nb, 1024)
+            extra = 5 if learned.enabled else 0          # features, MLP forward, 3 binning kernels
+        else:
+            dm = L.HfmDevMems()
+            L.check(lib.hfm_mems_batch_device(h.h, reads_d.data_ptr(), off_d.data_ptr(), n, 19, 0,
+                                              L.ptr(bounds, L.u32p), nb, 1024, C.byref(dm)))
+            extra = 0
         s2 = h.stats()
         if stats_out is not None:
-            stats_out.append((s1, s2, dh.total, dm.n_hits, dm.n_positions))
+            stats_out.append((s1, s2, dh.total, dm.n_hits, dm.n_positions, extra))
 
     # work counters (one untimed pass): algorithmic bytes per launch
     h.set_counters(True)
     cnt = []
     step(cnt)
     h.set_counters(False)
-    c_loc, c_mem, loc_total, n_hits, n_pos = cnt[0]
+    c_loc, c_mem, loc_total, n_hits, n_pos, _ = cnt[0]
 
     for _ in range(args.warmup):
         step()
@@ -287,7 +435,29 @@ def main():
         ms = float(t.item())
     value = world * n * args.steps / (ms / 1000.0)
     launches = sum(s1.search_launches + s1.resolve_launches + s1.other_launches + s2.search_launches +
-                   s2.resolve_launches + s2.other_launches for s1, s2, *_ in per)
+                   s2.resolve_launches + s2.other_launches + p[5] for p in per for s1, s2 in [p[:2]])
+
+    # the plain order, same loop (the learned path's fallback and judge)
+    plain_info = None
+    if learned is not None:
+        for _ in range(args.warmup):
+            step(plain=True)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step(plain=True)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        pms = ev0.elapsed_time(ev1)
+        if dist:
+            t = torch.tensor([pms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            pms = float(t.item())
+        plain_info = {"value": world * n * args.steps / (pms / 1000.0), "ms_per_step": pms / args.steps}
+        learned_info["speedup_vs_plain"] = round(plain_info["ms_per_step"] / (ms / args.steps), 4)
     # kernel times (CUDA events around each launch, recorded by the library on its stream)
     k_mems_ms = statistics.mean(s2.ms_search_kernel for _, s2, *_ in per)
     k_res_mem_ms = statistics.mean(s2.ms_resolve_kernel for _, s2, *_ in per)
@@ -394,6 +564,14 @@ def main():
     e2e = {"value": world * n * args.steps / e2e_s if e2e_s else None, "unit": "reads/s", "h2d_bytes_per_step": int(h2d),
            "d2h_bytes_per_step": int(d2h), "chunk_reads": ch, "handles": args.e2e_streams}
 
+    serving = None
+    if not args.no_serving and rank == 0:
+        serving = serving_latency(h, lib, L, kp, rp, bounds, n, args.serving_batches)
+    mixed = None
+    if not args.no_mixed and rank == 0:
+        del handles
+        mixed = mixed_workload(args, local, torch)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -408,13 +586,17 @@ def main():
             "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generators, haystackfm_b200/synth.py)",
             "config": {"workload": "iupac_batch_locate_smem", "reads_per_step_per_gpu": n, "read_len": 150,
                        "ref_len": args.ref_len, "contigs": args.contigs, "sa_sample_rate": 32, "lookup_depth": 10,
-                       "min_len": 19, "max_hits_per_mem": 1024, "locate_kmer": 32, "path": "plain",
+                       "min_len": 19, "max_hits_per_mem": 1024, "locate_kmer": 32,
+                       "path": ("learned-binned" if learned is not None and learned.enabled else
+                                "plain order (cost model not predictive on held-out reads)" if learned is not None
+                                else "plain"),
                        "l2": "no flush: index (0.7 GB device layout) + reads (150 MB) + outputs exceed the 126 MB L2",
                        "index_build_s": round(build_s, 1), "index_cached": not built,
                        "locate_positions": int(loc_total), "mem_hits": int(n_hits), "mem_positions": int(n_pos),
                        "distinct_rows_walked": int(rows_walked(c_mem) + rows_walked(c_loc)),
                        "parallelism": f"replicas{world}" if world > 1 else "single"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "plain": plain_info, "learned": learned_info, "serving": serving, "mixed": mixed,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

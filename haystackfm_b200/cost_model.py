@@ -155,10 +155,15 @@ class LearnedSmem:
     fit(): run the exact kernel with its work log on training reads, train the model on
     the log.  run(): predict, bin, and search through hfm_mems_batch_device_sched."""
 
-    def __init__(self, handle, device: int = 0, seed: int = 0, warp_min_hits: float = 0.0):
+    def __init__(self, handle, device: int = 0, seed: int = 0, warp_min_hits: float = 0.0,
+                 min_spearman: float = 0.3):
         self.handle = handle
         self.model = ReadCostModel(device, seed)
         self.warp_min_hits = warp_min_hits
+        self.min_spearman = min_spearman
+        self.enabled = True            # False: the model does not rank work; run the plain order
+        self.holdout_error: Optional[PredictionError] = None
+        self.calibration: Optional[dict] = None
         self._order = None
         self._y = None
 
@@ -173,13 +178,60 @@ class LearnedSmem:
                                                     max_hits, C.byref(sc), C.byref(dm)))
         return log[:4 * nq].view(nq, 4)
 
-    def fit(self, q_d, off_d, nq, min_len, mode, bounds, max_hits, epochs=4, batch=8192, lr=1e-3, seed=0):
+    def fit(self, q_d, off_d, nq, min_len, mode, bounds, max_hits, epochs=4, batch=8192, lr=1e-3, seed=0,
+            holdout: float = 0.1, calibrate: bool = True):
+        """Log the exact kernel's work on the training reads, train on the first
+        (1 - holdout) of them, and judge the model on the rest: the learned order is used
+        only when its predicted Occ touches rank the held-out reads' true touches with
+        Spearman >= min_spearman and (calibrate) the learned order runs the held-out reads
+        at least 2% faster than the plain order; otherwise run() keeps the plain order."""
         log = self.log_work(q_d, off_d, nq, min_len, mode, bounds, max_hits)
         t = work_targets(log).to(q_d.device)
         x = self.model.features(q_d, off_d, nq)
-        self.model.init_output_bias(t)
-        losses = self.model.train(x, t, epochs, batch, lr, seed)
+        ntr = nq - int(nq * holdout) if nq > 10 else nq
+        self.model.init_output_bias(t[:ntr])
+        losses = self.model.train(x[:ntr].contiguous(), t[:ntr].contiguous(), epochs, batch, lr, seed)
+        if ntr < nq:
+            self.holdout_error = prediction_error(self.model.forward(x[ntr:].contiguous()), t[ntr:])
+            self.enabled = self.holdout_error.spearman_touches >= self.min_spearman
+            if self.enabled and calibrate:
+                self.calibrate(q_d, off_d, ntr, nq, min_len, mode, bounds, max_hits)
         return losses, x, t
+
+    def calibrate(self, q_d, off_d, a, b, min_len, mode, bounds, max_hits, reps=2):
+        """Time the plain and the learned order on reads a..b (held out from training);
+        keep the learned order only when it is at least 2% faster."""
+        import time
+        torch = _torch()
+        base = int(off_d[a].item())
+        q = q_d[base:int(off_d[b].item())]
+        o = (off_d[a:b + 1] - base).contiguous()
+        n = b - a
+        rb = np.ascontiguousarray(bounds, dtype=np.uint32)
+        bp = L.ptr(rb, L.u32p) if len(rb) else None
+
+        def plain():
+            dm = L.HfmDevMems()
+            L.check(L.lib().hfm_mems_batch_device(self.handle.h, q.data_ptr(), o.data_ptr(), n, min_len, mode, bp,
+                                                  len(rb), max_hits, C.byref(dm)))
+
+        def learned():
+            self.run(q, o, n, min_len, mode, bp, len(rb), max_hits)
+
+        def best(f):
+            ts = []
+            for _ in range(reps + 1):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                f()
+                torch.cuda.synchronize()
+                ts.append(time.perf_counter() - t0)
+            return min(ts[1:]) * 1e3
+
+        self.enabled = True
+        tp, tl = best(plain), best(learned)
+        self.calibration = {"reads": n, "plain_ms": round(tp, 3), "learned_ms": round(tl, 3)}
+        self.enabled = tl < 0.98 * tp
 
     def plan(self, q_d, off_d, nq):
         """Predict and bin: -> (order tensor, n_warp, predictions)."""
@@ -192,8 +244,11 @@ class LearnedSmem:
         return order, nw, y
 
     def run(self, q_d, off_d, nq, min_len, mode, bounds_ptr, n_bounds, max_hits) -> L.HfmDevMems:
-        order, nw, _ = self.plan(q_d, off_d, nq)
-        sc = L.HfmSched(order.data_ptr() if nq else None, nw, 0, None)
+        if self.enabled:
+            order, nw, _ = self.plan(q_d, off_d, nq)
+            sc = L.HfmSched(order.data_ptr() if nq else None, nw, 0, None)
+        else:
+            sc = L.HfmSched(None, 0, 0, None)
         dm = L.HfmDevMems()
         L.check(L.lib().hfm_mems_batch_device_sched(self.handle.h, q_d.data_ptr(), off_d.data_ptr(), nq, min_len,
                                                     mode, bounds_ptr, n_bounds, max_hits, C.byref(sc),

@@ -86,7 +86,7 @@ struct DevBuf {
 
 struct Counters {                    // device-side counters, one block per handle
   unsigned long long iv_used, hit_used, touches, steps;
-  uint32_t n_ovf, still_ovf, walk_err, queue, queue2, _pad[3];
+  uint32_t n_ovf, still_ovf, walk_err, queue, queue2, n_mid, n_wrp, queue3;
 };
 
 struct FmDev {
@@ -110,9 +110,10 @@ struct hfm_index {
   // per-call work buffers (grow-only)
   DevBuf q, qoff, counts, nhits, niv, ivoff, status, ovf, ivpool, hitpool, seg_row, seg_off, pos_base, seg_base,
       scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr,
-      mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout, blockmap, blockmap2;
+      mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout, blockmap, blockmap2, ovf2, ovf3;
   uint32_t flags = 0;
-  int mems_variant = 2;   // register-budget variant of the SMEM fast kernel (see mems_device)
+  int mems_variant = 3;   // SMEM fast-kernel variant (see mems_device): 0/1/2 local 32-entry
+                          // candidate lists at 5/6/8 blocks per SM; 3 global 1024-entry lists
   int num_sms = 0;
   uint64_t iv_cap = 0, miv_cap = 0, hit_cap = 0;   // pool capacities in elements (uint2 / BIv / hit)
   Counters* h_ctr = nullptr;        // pinned
@@ -231,6 +232,9 @@ static constexpr uint32_t BS_WARP_SET_CAP = 8192;   // long-tail pass, per warp
 static constexpr uint32_t MEM_SET_CAP = 768;   // fast-path interval-set capacity (SMEM / MEM)
 static constexpr uint32_t MEM_WARP_SET_CAP = 8192;  // long-tail pass, per warp
 static constexpr int MEM_KC = 32;              // fast-path candidate capacity (thread-local)
+static constexpr uint32_t MID_CAND_CAP = 1024;  // candidate list of the per-thread rerun (global memory)
+static constexpr uint32_t MID_THREADS_PER_SM = 256;
+static constexpr uint32_t FAST_CAND_CAP = 1024;  // global candidate list of fast-pass variant 3
 
 // Backward search for a batch.  with_ivs = false: counts only.
 static int run_bsearch(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t cap,
@@ -297,7 +301,6 @@ static int run_bsearch(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
         launches++;
         CK(cudaGetLastError());
         RET(read_ctr(x));
-        x->stats.fallback_reads += n_ovf;
         if (x->h_ctr->still_ovf == 0) break;
         if (set_cap >= (1u << 24)) return set_error(HFM_E_OVERFLOW, "interval set exceeds 2^24 intervals");
         set_cap *= 4;
@@ -487,15 +490,21 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   MemsParams P{min_len, mode, cap, nb ? 1u : 0u};
   const FmDev& Fw = x->fwd; const FmDev& Rv = x->rev;
   // persistent fast pass: one wave of resident threads, MEM_SET_CAP intervals per set.
-  // Register budget variants: 5, 6 or 8 resident blocks of 128 threads per SM.
+  // Variants 0-2: 5, 6 or 8 resident blocks of 128 threads per SM with a 32-entry
+  // candidate list in local memory; variant 3 (default): 8 blocks per SM with a 1024-entry
+  // list per thread in global memory, so reads up to ~10 kbp finish in this pass.
   int variant = x->mems_variant;
   int bpsm = 0;
   if (variant == 0) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC, 5>, 128, 0));
   else if (variant == 1) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC, 6>, 128, 0));
+  else if (variant == 3) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, 0, 8>, 128, 0));
   else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC, 8>, 128, 0));
   uint64_t threads = (uint64_t)std::max(1, bpsm) * x->num_sms * 128;
   threads = std::min<uint64_t>(threads, ((uint64_t)nq + 127) / 128 * 128);
   RET(x->memwork.ensure(std::max<uint64_t>(threads, 32) * 4 * MEM_SET_CAP * 16));
+  // variant 3: candidate lists in global memory (FAST_CAND_CAP per thread), so long reads
+  // stay on the fast pass instead of overflowing a 32-entry local list
+  if (variant == 3) RET(x->cwork.ensure((size_t)std::max<uint64_t>(threads, 128) * FAST_CAND_CAP * sizeof(Cand)));
   bool done = false;
   for (int attempt = 0; attempt < 8 && !done; attempt++) {
     RET(x->mivpool.ensure(x->miv_cap * 16)); x->miv_cap = x->mivpool.cap / 16;
@@ -510,12 +519,17 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       CK(cudaMemcpyAsync(&dctr(x)->n_ovf, &n_warp, 4, cudaMemcpyHostToDevice, x->stream));
     }
     if (nq > n_warp) {
-      MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, nullptr, 0, &dctr(x)->queue, order ? order + n_warp : nullptr,
+      MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, variant == 3 ? x->cwork.as<Cand>() : nullptr,
+                 variant == 3 ? FAST_CAND_CAP : 0u, &dctr(x)->queue, order ? order + n_warp : nullptr,
                  nq - n_warp, &dctr(x)->still_ovf, 0u, wlog};
       unsigned grid = (unsigned)(threads / 128);
       if (x->memwork.cap < (size_t)grid * 128 * 4 * MEM_SET_CAP * 16) return set_error(HFM_E_ARG, "internal: work area too small");
       cudaEventRecord(x->evk[0], x->stream);
-      if (counting)
+      if (counting && variant == 3) {
+        if (x->cwork.cap < (size_t)grid * 128 * FAST_CAND_CAP * sizeof(Cand)) return set_error(HFM_E_ARG, "internal: candidate area too small");
+        k_mems<true, 32, 0, 5><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                           d_q, d_qoff, P, ivp, hp, o, W);
+      } else if (counting)
         k_mems<true, 32, MEM_KC, 5><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                                 d_q, d_qoff, P, ivp, hp, o, W);
       else if (variant == 0)
@@ -524,6 +538,11 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       else if (variant == 1)
         k_mems<false, 32, MEM_KC, 6><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                                  d_q, d_qoff, P, ivp, hp, o, W);
+      else if (variant == 3) {
+        if (x->cwork.cap < (size_t)grid * 128 * FAST_CAND_CAP * sizeof(Cand)) return set_error(HFM_E_ARG, "internal: candidate area too small");
+        k_mems<false, 32, 0, 8><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                            d_q, d_qoff, P, ivp, hp, o, W);
+      }
       else
         k_mems<false, 32, MEM_KC, 8><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                                  d_q, d_qoff, P, ivp, hp, o, W);
@@ -534,6 +553,47 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
     }
     RET(read_ctr(x));
     uint32_t n_ovf = x->h_ctr->n_ovf;
+    const uint32_t* wlist = x->ovf.as<uint32_t>();
+    if (n_ovf) {
+      x->stats.fallback_reads += n_ovf;
+      // Reads that outgrew only the 32-entry candidate list (long reads) rerun on the
+      // per-thread kernel with a MID_CAND_CAP-entry list in global memory; set overflows,
+      // reads the schedule routed, and middle-tier overflows go to the warp-per-read kernel.
+      RET(x->ovf2.ensure((size_t)nq * 4 + 4));
+      RET(x->ovf3.ensure((size_t)nq * 4 + 4));
+      CK(cudaMemsetAsync(&dctr(x)->n_mid, 0, 12, x->stream));
+      k_split_ovf<<<(n_ovf + 255) / 256, 256, 0, x->stream>>>(x->ovf.as<uint32_t>(), n_ovf, n_warp,
+                                                              x->status.as<uint32_t>(), x->ovf3.as<uint32_t>(),
+                                                              &dctr(x)->n_mid, x->ovf2.as<uint32_t>(), &dctr(x)->n_wrp);
+      other++;
+      CK(cudaGetLastError());
+      RET(read_ctr(x));
+      uint32_t n_mid = x->h_ctr->n_mid;
+      if (n_mid) {
+        uint64_t tm = std::min<uint64_t>({((uint64_t)n_mid + 127) / 128 * 128, (uint64_t)x->num_sms * MID_THREADS_PER_SM,
+                                          threads / 128 * 128});
+        tm = std::max<uint64_t>(tm, 128);
+        unsigned grid = (unsigned)(tm / 128);
+        if (x->memwork.cap < (size_t)grid * 128 * 4 * MEM_SET_CAP * 16) return set_error(HFM_E_ARG, "internal: work area too small");
+        RET(x->cwork.ensure((size_t)grid * 128 * MID_CAND_CAP * sizeof(Cand)));
+        MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), MID_CAND_CAP, &dctr(x)->queue3,
+                   x->ovf3.as<uint32_t>(), n_mid, &dctr(x)->still_ovf, 0u, wlog};
+        MemsOut o2 = o;
+        o2.ovf_list = x->ovf2.as<uint32_t>();
+        o2.n_ovf = &dctr(x)->n_wrp;
+        if (counting)
+          k_mems<true, 32, 0, 5><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                             d_q, d_qoff, P, ivp, hp, o2, W);
+        else
+          k_mems<false, 32, 0, 8><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                              d_q, d_qoff, P, ivp, hp, o2, W);
+        launches++;
+        CK(cudaGetLastError());
+        RET(read_ctr(x));
+      }
+      n_ovf = x->h_ctr->n_wrp;
+      wlist = x->ovf2.as<uint32_t>();
+    }
     if (n_ovf) {
       // long tail: one warp per overflowed read, 4 sets and a candidate list per warp,
       // growing 4x until every read fits
@@ -547,7 +607,7 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
         RET(x->cwork.ensure((size_t)grid * 4 * cand_cap * sizeof(Cand)));
         CK(cudaMemsetAsync(&dctr(x)->still_ovf, 0, 4, x->stream));
         CK(cudaMemsetAsync(&dctr(x)->queue2, 0, 4, x->stream));
-        MemsWork W{x->work.as<BIv>(), set_cap, x->cwork.as<Cand>(), cand_cap, &dctr(x)->queue2, x->ovf.as<uint32_t>(),
+        MemsWork W{x->work.as<BIv>(), set_cap, x->cwork.as<Cand>(), cand_cap, &dctr(x)->queue2, wlist,
                    n_ovf, &dctr(x)->still_ovf, 1u, wlog};
         if (counting)
           k_mems_warp<true><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
@@ -558,7 +618,6 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
         launches++;
         CK(cudaGetLastError());
         RET(read_ctr(x));
-        x->stats.fallback_reads += n_ovf;
         if (x->h_ctr->still_ovf == 0) break;
         if (set_cap >= (1u << 22)) return set_error(HFM_E_OVERFLOW, "MEM interval set exceeds 2^22 intervals");
         set_cap *= 4; cand_cap *= 4;
@@ -733,7 +792,7 @@ void hfm_index_free(hfm_index* x) {
                     &x->seg_base, &x->scan_tmp, &x->out_pairs, &x->ref_bounds, &x->hit_start, &x->hit_count,
                     &x->hit_base, &x->hits, &x->npos_scan, &x->work, &x->cwork, &x->ctr, &x->mivpool, &x->bswork, &x->memwork,
                     &x->hkeys, &x->hslot, &x->hflags, &x->huid, &x->urow, &x->ulen, &x->uoff, &x->uout,
-                    &x->blockmap, &x->blockmap2})
+                    &x->blockmap, &x->blockmap2, &x->ovf2, &x->ovf3})
     b->release();
   for (auto& e : x->ev) if (e) cudaEventDestroy(e);
   for (auto& e : x->evk) if (e) cudaEventDestroy(e);

@@ -470,10 +470,16 @@ __device__ __forceinline__ uint32_t finalize_smems(Cand* c, uint32_t n) {
   for (uint32_t i = 0; i < n; i++)
     if (w == 0 || c[w - 1].qs != c[i].qs || c[w - 1].qe != c[i].qe) c[w++] = c[i];
   n = w; w = 0;
+  // Sorted by (qs, qe) and distinct, c[i] lies inside another candidate exactly when the
+  // next one shares its start (and so ends later) or an earlier one (qs <= c[i].qs) ends
+  // at or after c[i].qe: a running maximum of qe replaces the all-pairs test.
+  uint32_t max_qe = 0;
+  bool any = false;
   for (uint32_t i = 0; i < n; i++) {
-    bool contained = false;
-    for (uint32_t j = 0; j < n && !contained; j++)
-      if (j != i && c[j].qs <= c[i].qs && c[i].qe <= c[j].qe) contained = true;   // distinct after dedup
+    bool contained = (i + 1 < n && c[i + 1].qs == c[i].qs) || (any && max_qe >= c[i].qe);
+    uint32_t qe = c[i].qe;
+    if (!any || qe > max_qe) max_qe = qe;
+    any = true;
     if (!contained) c[w++] = c[i];
   }
   return w;
@@ -514,7 +520,21 @@ struct MemsWork {
   uint32_t* still_ovf;
   uint32_t rerun;                     // 1: a rerun of overflowed reads (counted in still_ovf)
   uint32_t* work_log;                 // COUNT_TOUCH only: 4 u32 per read, [0] += Occ touches, [3] |= 1 on overflow
+                                      // (the warp-per-read kernel also sets bit 1)
 };
+
+// Splits the fast pass's overflow list: the first `first_warp` entries (reads a schedule
+// routed) and reads whose interval sets overflowed go to the warp-per-read list; reads that
+// outgrew only the candidate list go to the per-thread rerun with a larger global list.
+__global__ void k_split_ovf(const uint32_t* __restrict__ list, uint32_t n, uint32_t first_warp,
+                            const uint32_t* __restrict__ status, uint32_t* __restrict__ mid,
+                            uint32_t* __restrict__ n_mid, uint32_t* __restrict__ wrp, uint32_t* __restrict__ n_wrp) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  uint32_t i = list[k];
+  if (k < first_warp || (status[i] & ST_SET_OVF)) wrp[atomicAdd(n_wrp, 1u)] = i;
+  else mid[atomicAdd(n_mid, 1u)] = i;
+}
 
 template <bool COUNT_TOUCH, int STRIDE, int KC, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_mems(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
@@ -906,7 +926,7 @@ __global__ void __launch_bounds__(128) k_mems_warp(DevFm Fw, DevFm Rv, const uin
     __syncwarp();
     if (COUNT_TOUCH && W.work_log) {
       uint32_t d = warp_sum((uint32_t)(touches - t0));
-      if (lane == 0) { W.work_log[4 * (size_t)i] += d; W.work_log[4 * (size_t)i + 3] |= 1u; }
+      if (lane == 0) { W.work_log[4 * (size_t)i] += d; W.work_log[4 * (size_t)i + 3] |= 3u; }
     }
     if (lane == 0) {
       uint64_t hs = 0; uint32_t hc = 0;

@@ -10,7 +10,10 @@ shapes and value distributions of the two workloads:
   (geometric run lengths, mean 500) and 0.5% single ambiguity codes (R..V uniform).  Reads
   (150 bp) are drawn from either strand of the unmasked ACGT sequence — the N runs and
   ambiguity codes mask only the reference — with 1% substitutions and 0.1% N.
-* sample_mixed_reads — mixed-length reads on the same reference: 80% 150 bp (1%
+* repeat_reference — ACGT-only genome with interspersed repeat families (300 bp and 6 kbp
+  consensus, 10-20% divergent copies, 40% of the bases) and tandem repeats (period 2-60,
+  5%), the scaled shape of a mammalian assembly.
+* sample_mixed_reads — mixed-length reads on either reference: 80% 150 bp (1%
   substitutions), 20% lognormal lengths (median 3 kbp, clipped to 100 bp .. 10 kbp) with 8%
   mixed substitutions / insertions / deletions.
 """
@@ -75,6 +78,56 @@ def iupac_reference(total=100_000_000, n_contigs=200, n_frac=0.02, n_run_mean=50
     return Reference(contigs, truth, seed)
 
 
+def repeat_reference(total=100_000_000, n_contigs=24, interspersed_frac=0.40, tandem_frac=0.05,
+                     n_short_families=10, n_long_families=10, short_len=300, long_len=6000,
+                     divergence=(0.10, 0.20), seed=11) -> Reference:
+    """ACGT-only genome with repeats, the scaled shape of a mammalian assembly: uniform
+    background; interspersed copies of `n_short_families` 300 bp and `n_long_families`
+    6 kbp consensus sequences (long-family copies 5'-truncated to a uniform length in
+    [500, 6000]) at per-copy substitution divergence uniform in `divergence`, covering
+    `interspersed_frac` of the bases; tandem repeats (period uniform in 2..60, array length
+    uniform in 100..3000, 5% substitutions) covering `tandem_frac`.  Contig lengths are
+    lognormal (mu=13, sigma=1) rescaled to `total`.  No N runs, no ambiguity codes."""
+    rng = np.random.default_rng(seed)
+    lens = _lognormal_lengths(rng, n_contigs, total)
+    g = rng.integers(1, 5, size=int(lens.sum()), dtype=np.uint8)
+    fams = [rng.integers(1, 5, size=short_len, dtype=np.uint8) for _ in range(n_short_families)] + \
+           [rng.integers(1, 5, size=long_len, dtype=np.uint8) for _ in range(n_long_families)]
+    placed = 0
+    target = interspersed_frac * len(g)
+    while placed < target:
+        f = int(rng.integers(0, len(fams)))
+        cons = fams[f]
+        if f >= n_short_families:
+            cons = cons[len(cons) - int(rng.integers(500, len(cons) + 1)):]
+        d = rng.uniform(*divergence)
+        cp = cons.copy()
+        sub = rng.random(len(cp)) < d
+        cp[sub] = ((cp[sub] - 1 + rng.integers(1, 4, size=int(sub.sum()), dtype=np.uint8)) % 4) + 1
+        if rng.random() < 0.5:
+            cp = (5 - cp)[::-1]
+        at = int(rng.integers(0, len(g) - len(cp)))
+        g[at:at + len(cp)] = cp
+        placed += len(cp)
+    placed = 0
+    target = tandem_frac * len(g)
+    while placed < target:
+        per = int(rng.integers(2, 61))
+        L = int(rng.integers(100, 3001))
+        unit = rng.integers(1, 5, size=per, dtype=np.uint8)
+        arr = np.tile(unit, L // per + 1)[:L]
+        sub = rng.random(L) < 0.05
+        arr[sub] = ((arr[sub] - 1 + rng.integers(1, 4, size=int(sub.sum()), dtype=np.uint8)) % 4) + 1
+        at = int(rng.integers(0, len(g) - L))
+        g[at:at + L] = arr
+        placed += L
+    contigs, o = [], 0
+    for l in lens:
+        contigs.append(g[o:o + int(l)].copy())
+        o += int(l)
+    return Reference(contigs=contigs, truth=contigs, seed=seed)
+
+
 def sample_reads(ref: Reference, n_reads=1_000_000, read_len=150, sub_rate=0.01, n_rate=0.001, seed=3):
     """Reads from either strand of the unmasked sequence with substitutions and Ns."""
     rng = np.random.default_rng(seed)
@@ -121,11 +174,13 @@ def _mutate(seq: np.ndarray, rate: float, rng) -> np.ndarray:
 
 def sample_mixed_reads(ref: Reference, n_reads=200_000, short_frac=0.8, short_len=150, long_median=3000,
                        long_sigma=0.6, min_len=100, max_len=10_000, short_sub=0.01, long_err=0.08,
-                       n_rate=0.001, seed=5):
+                       n_rate=0.001, seed=5, avoid_masked=False):
     """Mixed-length reads as a flat batch: `short_frac` of fixed `short_len` reads with
     substitutions, the rest lognormal (median `long_median`, clipped to [min_len, max_len])
     with mixed substitutions / insertions / deletions at `long_err`; either strand, Ns at
-    `n_rate`.  Returns (flat u8 codes, u64 offsets[n+1], lengths)."""
+    `n_rate`.  avoid_masked: draw only source spans whose reference holds no N (reads from
+    sequenced regions; spans across an N run make the SMEM search quadratic in the run
+    length).  Returns (flat u8 codes, u64 offsets[n+1], lengths)."""
     rng = np.random.default_rng(seed)
     is_long = rng.random(n_reads) >= short_frac
     lens = np.full(n_reads, short_len, dtype=np.int64)
@@ -137,20 +192,37 @@ def sample_mixed_reads(ref: Reference, n_reads=200_000, short_frac=0.8, short_le
     w_all = (clen - src_len.max() + 1).clip(min=0).astype(np.float64)
     cid = rng.choice(len(clen), size=n_reads, p=w_all / w_all.sum())
     starts = (rng.random(n_reads) * (clen[cid] - src_len + 1)).astype(np.int64)
+    if avoid_masked:
+        base = np.concatenate([[0], np.cumsum(clen)])
+        gsum = np.concatenate([[0], np.cumsum(np.concatenate(ref.contigs) == N)])
+        for _ in range(1000):
+            a = base[cid] + starts
+            bad = gsum[a + src_len] - gsum[a] > 0
+            if not bad.any():
+                break
+            k = int(bad.sum())
+            cid[bad] = rng.choice(len(clen), size=k, p=w_all / w_all.sum())
+            starts[bad] = (rng.random(k) * (clen[cid[bad]] - src_len[bad] + 1)).astype(np.int64)
     rc = rng.random(n_reads) < 0.5
-    out = []
-    for i in range(n_reads):
+    out = [None] * n_reads
+    # short reads, vectorised per contig
+    sh = np.nonzero(~is_long)[0]
+    rows = np.empty((len(sh), short_len), dtype=np.uint8)
+    for c in np.unique(cid[sh]):
+        sel = np.nonzero(cid[sh] == c)[0]
+        rows[sel] = ref.truth[c][starts[sh[sel], None] + np.arange(short_len)[None, :]]
+    flip = rc[sh]
+    rows[flip] = (5 - rows[flip])[:, ::-1]
+    sub = rng.random(rows.shape) < short_sub
+    shift = rng.integers(1, 4, size=rows.shape, dtype=np.uint8)
+    rows = np.where(sub, ((rows - 1 + shift) % 4) + 1, rows).astype(np.uint8)
+    for k, i in enumerate(sh):
+        out[i] = rows[k]
+    for i in np.nonzero(is_long)[0]:
         s = ref.truth[cid[i]][starts[i]:starts[i] + src_len[i]]
         if rc[i]:
             s = (5 - s)[::-1]
-        if is_long[i]:
-            s = _mutate(np.ascontiguousarray(s), long_err, rng)[:lens[i]]
-        else:
-            s = s.copy()
-            sub = rng.random(len(s)) < short_sub
-            shift = rng.integers(1, 4, size=len(s), dtype=np.uint8)
-            s[sub] = ((s[sub] - 1 + shift[sub]) % 4) + 1
-        out.append(s)
+        out[i] = _mutate(np.ascontiguousarray(s), long_err, rng)[:lens[i]]
     lens = np.array([len(s) for s in out], dtype=np.int64)
     flat = np.concatenate(out).astype(np.uint8) if out else np.zeros(0, np.uint8)
     flat[rng.random(len(flat)) < n_rate] = N

@@ -191,7 +191,9 @@ int hfm_count_batch_noalloc(hfm_index* idx, const uint8_t* d_q, const uint64_t* 
  *              kernel variants and logs the exact work of each read i:
  *              [4i] Occ record touches (backward and forward extension steps, every pass),
  *              [4i+1] MemHits reported, [4i+2] positions reported,
- *              [4i+3] bit 0: the read ran on the warp-per-read kernel. */
+ *              [4i+3] bit 0: the read left the fast per-thread pass (its candidate list
+ *              or an interval set outgrew the fast path, or n_warp routed it); bit 1: it
+ *              ran on the warp-per-read kernel. */
 typedef struct hfm_sched {
   const uint32_t* d_order;
   uint32_t n_warp;
