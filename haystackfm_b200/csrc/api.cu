@@ -85,8 +85,8 @@ struct DevBuf {
 };
 
 struct Counters {                    // device-side counters, one block per handle
-  unsigned long long iv_used, hit_used, touches, steps;
-  uint32_t n_ovf, still_ovf, walk_err, queue, queue2, n_mid, n_wrp, queue3;
+  unsigned long long iv_used, hit_used, touches, steps, seg_used;
+  uint32_t n_ovf, still_ovf, walk_err, queue, queue2, n_mid, n_wrp, queue3, seg_queue, merge_queue;
 };
 
 struct FmDev {
@@ -110,12 +110,15 @@ struct hfm_index {
   // per-call work buffers (grow-only)
   DevBuf q, qoff, counts, nhits, niv, ivoff, status, ovf, ivpool, hitpool, seg_row, seg_off, pos_base, seg_base,
       scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr,
-      mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout, blockmap, blockmap2, ovf2, ovf3;
+      mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout, blockmap, blockmap2, ovf2, ovf3,
+      lflag, lpos, sids, lids, ucount, ubase, uread, uk, ubits, uexit, ust, ucoff, ucnt, segpool;
   uint32_t flags = 0;
+  uint32_t seg_len = 512;  // SMEM reads longer than 2 * seg_len take the segmented sweep
   int mems_variant = 3;   // SMEM fast-kernel variant (see mems_device): 0/1/2 local 32-entry
                           // candidate lists at 5/6/8 blocks per SM; 3 global 1024-entry lists
   int num_sms = 0;
   uint64_t iv_cap = 0, miv_cap = 0, hit_cap = 0;   // pool capacities in elements (uint2 / BIv / hit)
+  uint64_t seg_cap = 0;                            // segment candidate pool capacity (Cand)
   Counters* h_ctr = nullptr;        // pinned
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t evk[4] = {nullptr, nullptr, nullptr, nullptr};   // main search kernel, resolve kernel
@@ -499,8 +502,50 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   else if (variant == 1) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC, 6>, 128, 0));
   else if (variant == 3) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, 0, 8>, 128, 0));
   else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC, 8>, 128, 0));
-  uint64_t threads = (uint64_t)std::max(1, bpsm) * x->num_sms * 128;
-  threads = std::min<uint64_t>(threads, ((uint64_t)nq + 127) / 128 * 128);
+  const uint64_t full_threads = (uint64_t)std::max(1, bpsm) * x->num_sms * 128;
+  uint64_t threads = std::min<uint64_t>(full_threads, ((uint64_t)nq + 127) / 128 * 128);
+  // Long reads (SMEM mode with global candidate lists) take the segmented sweep: the
+  // fast pass gets the other reads, in the same relative order.
+  const uint32_t* fast_ids = order ? order + n_warp : nullptr;
+  uint32_t n_fast = nq - n_warp, n_long = 0;
+  uint64_t n_units = 0;
+  if (mode == 0 && variant == 3 && n_fast > 0) {
+    RET(x->lflag.ensure((size_t)n_fast * 4 + 4));
+    RET(x->lpos.ensure(((size_t)n_fast + 1) * 8));
+    k_long_flags<<<(n_fast + 255) / 256, 256, 0, x->stream>>>(fast_ids, n_fast, d_qoff, 2 * x->seg_len,
+                                                              x->lflag.as<uint32_t>());
+    other++;
+    CK(cudaGetLastError());
+    RET(scan(x, x->lflag.as<uint32_t>(), 1, n_fast, x->lpos.as<uint64_t>(), other));
+    uint64_t nl = 0;
+    RET(read_u64(x, x->lpos.as<uint64_t>() + n_fast, nl));
+    n_long = (uint32_t)nl;
+    if (n_long) {
+      RET(x->sids.ensure((size_t)n_fast * 4 + 4));
+      RET(x->lids.ensure((size_t)n_long * 4 + 4));
+      RET(x->ucount.ensure((size_t)n_long * 4 + 4));
+      k_split_ids<<<(n_fast + 255) / 256, 256, 0, x->stream>>>(fast_ids, n_fast, x->lflag.as<uint32_t>(),
+                                                               x->lpos.as<uint64_t>(), x->sids.as<uint32_t>(),
+                                                               x->lids.as<uint32_t>(), x->ucount.as<uint32_t>(), d_qoff,
+                                                               x->seg_len);
+      other++;
+      CK(cudaGetLastError());
+      RET(x->ubase.ensure(((size_t)n_long + 1) * 8));
+      RET(scan(x, x->ucount.as<uint32_t>(), 1, n_long, x->ubase.as<uint64_t>(), other));
+      RET(read_u64(x, x->ubase.as<uint64_t>() + n_long, n_units));
+      RET(x->uread.ensure(n_units * 4)); RET(x->uk.ensure(n_units * 4));
+      RET(x->ubits.ensure(n_units * (x->seg_len / 32) * 4)); RET(x->uexit.ensure(n_units * 4));
+      RET(x->ust.ensure(n_units * 4)); RET(x->ucoff.ensure(n_units * 8)); RET(x->ucnt.ensure(n_units * 4));
+      k_unit_fill<<<(n_long + 255) / 256, 256, 0, x->stream>>>(x->lids.as<uint32_t>(), n_long, x->ubase.as<uint64_t>(),
+                                                               x->uread.as<uint32_t>(), x->uk.as<uint32_t>());
+      other++;
+      CK(cudaGetLastError());
+      fast_ids = x->sids.as<uint32_t>();
+      n_fast -= n_long;
+      x->seg_cap = std::max<uint64_t>(x->seg_cap, n_units * 24 + 65536);
+      threads = std::max<uint64_t>(threads, std::min<uint64_t>(full_threads, (n_units + 127) / 128 * 128));
+    }
+  }
   RET(x->memwork.ensure(std::max<uint64_t>(threads, 32) * 4 * MEM_SET_CAP * 16));
   // variant 3: candidate lists in global memory (FAST_CAND_CAP per thread), so long reads
   // stay on the fast pass instead of overflowing a 32-entry local list
@@ -508,6 +553,7 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   bool done = false;
   for (int attempt = 0; attempt < 8 && !done; attempt++) {
     RET(x->mivpool.ensure(x->miv_cap * 16)); x->miv_cap = x->mivpool.cap / 16;
+    if (n_long) { RET(x->segpool.ensure(x->seg_cap * sizeof(Cand))); x->seg_cap = x->segpool.cap / sizeof(Cand); }
     RET(x->hitpool.ensure(x->hit_cap * 32)); x->hit_cap = x->hitpool.cap / 32;
     CK(cudaMemsetAsync(x->ctr.p, 0, sizeof(Counters), x->stream));
     if (wlog && nq) CK(cudaMemsetAsync(wlog, 0, (size_t)nq * 16, x->stream));
@@ -518,13 +564,12 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       CK(cudaMemcpyAsync(x->ovf.p, order, (size_t)n_warp * 4, cudaMemcpyDeviceToDevice, x->stream));
       CK(cudaMemcpyAsync(&dctr(x)->n_ovf, &n_warp, 4, cudaMemcpyHostToDevice, x->stream));
     }
-    if (nq > n_warp) {
+    if (n_fast > 0 || n_long > 0) cudaEventRecord(x->evk[0], x->stream);
+    if (n_fast > 0) {
       MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, variant == 3 ? x->cwork.as<Cand>() : nullptr,
-                 variant == 3 ? FAST_CAND_CAP : 0u, &dctr(x)->queue, order ? order + n_warp : nullptr,
-                 nq - n_warp, &dctr(x)->still_ovf, 0u, wlog};
+                 variant == 3 ? FAST_CAND_CAP : 0u, &dctr(x)->queue, fast_ids, n_fast, &dctr(x)->still_ovf, 0u, wlog};
       unsigned grid = (unsigned)(threads / 128);
       if (x->memwork.cap < (size_t)grid * 128 * 4 * MEM_SET_CAP * 16) return set_error(HFM_E_ARG, "internal: work area too small");
-      cudaEventRecord(x->evk[0], x->stream);
       if (counting && variant == 3) {
         if (x->cwork.cap < (size_t)grid * 128 * FAST_CAND_CAP * sizeof(Cand)) return set_error(HFM_E_ARG, "internal: candidate area too small");
         k_mems<true, 32, 0, 5><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
@@ -546,10 +591,39 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       else
         k_mems<false, 32, MEM_KC, 8><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                                  d_q, d_qoff, P, ivp, hp, o, W);
-      cudaEventRecord(x->evk[1], x->stream);
-      x->k_search_rec = true;
       launches++;
       CK(cudaGetLastError());
+    }
+    if (n_long > 0) {
+      // segmented sweep of the long reads, then the merge along each read's true chain
+      SegWork G{x->seg_len, x->seg_len / 32, x->uread.as<uint32_t>(), x->uk.as<uint32_t>(), (uint32_t)n_units, x->ubits.as<uint32_t>(),
+                x->uexit.as<uint32_t>(), x->ust.as<uint32_t>(), x->ucoff.as<uint64_t>(), x->ucnt.as<uint32_t>(),
+                x->segpool.as<Cand>(), &dctr(x)->seg_used, x->seg_cap, x->lids.as<uint32_t>(),
+                x->ubase.as<uint64_t>(), n_long, &dctr(x)->merge_queue, &dctr(x)->touches};
+      MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), FAST_CAND_CAP, &dctr(x)->seg_queue, nullptr,
+                 0u, &dctr(x)->still_ovf, 0u, wlog};
+      uint64_t ts = std::min<uint64_t>(threads / 128 * 128, (n_units + 127) / 128 * 128);
+      uint64_t tmg = std::min<uint64_t>(threads / 128 * 128, ((uint64_t)n_long + 127) / 128 * 128);
+      unsigned gs = (unsigned)std::max<uint64_t>(1, ts / 128), gm = (unsigned)std::max<uint64_t>(1, tmg / 128);
+      if (x->memwork.cap < (size_t)gs * 128 * 4 * MEM_SET_CAP * 16 || x->cwork.cap < (size_t)gs * 128 * FAST_CAND_CAP * sizeof(Cand))
+        return set_error(HFM_E_ARG, "internal: work area too small");
+      if (counting) {
+        k_mems_seg<true, 32, 5><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                           d_q, d_qoff, P, ivp, W, G);
+        k_mems_merge<true, 32, 5><<<gm, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                             d_q, d_qoff, P, ivp, hp, o, W, G);
+      } else {
+        k_mems_seg<false, 32, 8><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                            d_q, d_qoff, P, ivp, W, G);
+        k_mems_merge<false, 32, 8><<<gm, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                              d_q, d_qoff, P, ivp, hp, o, W, G);
+      }
+      launches += 2;
+      CK(cudaGetLastError());
+    }
+    if (n_fast > 0 || n_long > 0) {
+      cudaEventRecord(x->evk[1], x->stream);
+      x->k_search_rec = true;
     }
     RET(read_ctr(x));
     uint32_t n_ovf = x->h_ctr->n_ovf;
@@ -623,9 +697,11 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
         set_cap *= 4; cand_cap *= 4;
       }
     }
-    if (x->h_ctr->iv_used <= x->miv_cap && x->h_ctr->hit_used <= x->hit_cap) { done = true; break; }
+    if (x->h_ctr->iv_used <= x->miv_cap && x->h_ctr->hit_used <= x->hit_cap &&
+        (n_long == 0 || x->h_ctr->seg_used <= x->seg_cap)) { done = true; break; }
     x->miv_cap = std::max(x->miv_cap, (uint64_t)(x->h_ctr->iv_used * 3 / 2 + 4096));
     x->hit_cap = std::max(x->hit_cap, (uint64_t)(x->h_ctr->hit_used * 3 / 2 + 4096));
+    if (n_long) x->seg_cap = std::max(x->seg_cap, (uint64_t)(x->h_ctr->seg_used * 3 / 2 + 65536));
   }
   if (!done) return set_error(HFM_E_OVERFLOW, "MEM pools did not converge");
   x->stats.occ_touches += x->h_ctr->touches;
@@ -769,6 +845,10 @@ int hfm_index_load(const uint8_t* bytes, size_t len, int kind, const hfm_opts* o
   std::unique_ptr<hfm_index> x(new hfm_index());
   x->device = dev; x->kind = kind; x->flags = opts ? opts->flags : 0;
   if (const char* v = std::getenv("HFM_MEMS_VARIANT")) x->mems_variant = std::atoi(v);
+  if (const char* v = std::getenv("HFM_SEG_LEN")) {
+    int sl = std::atoi(v);
+    if (sl >= 64 && sl <= (int)SEG_MAX && sl % 32 == 0) x->seg_len = (uint32_t)sl;
+  }
   CK(cudaDeviceGetAttribute(&x->num_sms, cudaDevAttrMultiProcessorCount, dev));
   CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
   for (auto& e : x->ev) CK(cudaEventCreate(&e));
@@ -792,7 +872,9 @@ void hfm_index_free(hfm_index* x) {
                     &x->seg_base, &x->scan_tmp, &x->out_pairs, &x->ref_bounds, &x->hit_start, &x->hit_count,
                     &x->hit_base, &x->hits, &x->npos_scan, &x->work, &x->cwork, &x->ctr, &x->mivpool, &x->bswork, &x->memwork,
                     &x->hkeys, &x->hslot, &x->hflags, &x->huid, &x->urow, &x->ulen, &x->uoff, &x->uout,
-                    &x->blockmap, &x->blockmap2, &x->ovf2, &x->ovf3})
+                    &x->blockmap, &x->blockmap2, &x->ovf2, &x->ovf3, &x->lflag, &x->lpos, &x->sids, &x->lids,
+                    &x->ucount, &x->ubase, &x->uread, &x->uk, &x->ubits, &x->uexit, &x->ust, &x->ucoff, &x->ucnt,
+                    &x->segpool})
     b->release();
   for (auto& e : x->ev) if (e) cudaEventDestroy(e);
   for (auto& e : x->evk) if (e) cudaEventDestroy(e);

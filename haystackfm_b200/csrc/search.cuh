@@ -334,7 +334,7 @@ __device__ __forceinline__ bool any_extend(const DevFm& X, const SmemFm& S, uint
   return false;
 }
 
-struct Cand { uint32_t qs, qe, count, nivs; uint64_t ivoff; };
+struct Cand { uint32_t qs, qe, count, nivs; uint64_t ivoff; uint32_t pivot, _pad; };
 
 struct MemsOut {
   uint64_t* hit_start;      // per read: offset of its hits in the hit pool
@@ -359,6 +359,91 @@ __device__ __forceinline__ void sort_by_flo(BIv* a, uint32_t n) {
     }
 }
 
+// The full interval (the empty pattern) as a one-element two-list set.
+template <class SR>
+__device__ __forceinline__ void start_full(TwoList<SR>& t, const BIv& full, uint32_t set_cap) {
+  if (full.fhi - full.flo == 1) { t.s[0] = full; t.n1 = 1; t.nb = 0; }
+  else { t.s[set_cap - 1] = full; t.n1 = 0; t.nb = 1; }
+}
+
+__device__ __forceinline__ uint32_t qmask(const SmemFm& S, uint8_t c) { return c < 16 ? S.compat_mask[c] : 0u; }
+
+// One pivot of the SMEM sweep (collect_smem_candidates loop body,
+// src/fm_index/smem.rs:154-222): forward extension from `pivot`, every right-maximal prefix
+// extended left maximally (extend_left_maximally, smem.rs:227-243), candidates passed to
+// emit(qs, qe, count, set, pivot).  Returns the next pivot, max(reach, pivot + 1), or ~0u
+// on overflow (flags in st).  The sweep is a chain pivot -> next(pivot) that depends only
+// on the read, which is what lets a long read be cut into independently swept segments.
+template <bool COUNT_TOUCH, class SR, class Emit>
+__device__ __forceinline__ uint32_t smem_pivot(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf, const SmemFm& Sr,
+                                               const uint8_t* q, uint32_t n, uint32_t pivot, const MemsParams& P,
+                                               const SR& curr, const SR& nxt, const SR& wa, const SR& wb,
+                                               uint32_t set_cap, uint32_t& st, uint64_t& touches, Emit& emit) {
+  using TL = TwoList<SR>;
+  const BIv full = {0, Fw.text_len, 0, Fw.text_len};
+  bool ovf = false;
+  TL c{curr, 0, 0}, x{nxt, 0, 0};
+  start_full(x, full, set_cap);
+  uint32_t cov;
+  extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[pivot]), x, c, set_cap, cov, ovf, touches);
+  if (ovf) { st |= ST_SET_OVF; return ~0u; }
+  if (c.size() == 0) return pivot + 1;
+  uint32_t j = pivot + 1, reach = pivot + 1;
+  for (;;) {
+    uint32_t end, ncov = 0;
+    bool next_empty, record;
+    x.n1 = x.nb = 0;
+    if (j == n) { end = n; next_empty = true; record = true; }
+    else {
+      extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, x, set_cap, ncov, ovf, touches);
+      if (ovf) { st |= ST_SET_OVF; return ~0u; }
+      end = j; next_empty = x.size() == 0; record = ncov != cov;
+    }
+    if (record) {
+      // right-maximal prefix [pivot, end): extend_left_maximally (smem.rs:227-243)
+      reach = end;
+      TL b = c;
+      uint32_t start = pivot, bcov = cov;
+      TL bufs[2] = {TL{wa, 0, 0}, TL{wb, 0, 0}};
+      int t = 0;
+      while (start > 0) {
+        uint32_t lcov;
+        extend_set<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[start - 1]), b, bufs[t], set_cap, lcov, ovf, touches);
+        if (ovf) { st |= ST_SET_OVF; return ~0u; }
+        if (bufs[t].size() == 0) break;
+        b = bufs[t]; bcov = lcov; t ^= 1; start--;
+      }
+      if (end - start >= P.min_len) {
+        // right-maximality (smem.rs:202-207); with no left extension it is next_empty
+        bool rmax = end == n ||
+                    (start == pivot ? next_empty : !any_extend<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[end]), b, set_cap, touches));
+        if (rmax && !emit(start, end, bcov, b, pivot)) return ~0u;
+      }
+    }
+    if (j == n || x.size() == 0) break;
+    TL tt = c; c = x; x = tt; cov = ncov; j++;
+  }
+  return max(reach, pivot + 1);
+}
+
+// Appends candidates (with their interval sets copied to the interval pool) to a list.
+template <class SR>
+struct CandSink {
+  Cand* cands; uint32_t nc, cap; Pool* ivpool; uint32_t* st; uint32_t set_cap;
+  __device__ __forceinline__ bool operator()(uint32_t qs, uint32_t qe, uint32_t count, const TwoList<SR>& ivs,
+                                             uint32_t pivot) {
+    if (nc >= cap) { *st |= ST_CAND_OVF; return false; }
+    uint32_t niv = ivs.size();
+    uint64_t off = thread_reserve(*ivpool, niv);
+    if (off == ~0ull) { *st |= ST_POOL_OVF; return false; }
+    BIv* dst = (BIv*)ivpool->base + off;
+    for (uint32_t k = 0; k < ivs.n1; k++) dst[k] = ivs.s[k];
+    for (uint32_t k = 0; k < ivs.nb; k++) dst[ivs.n1 + k] = ivs.s[set_cap - 1 - k];
+    cands[nc++] = Cand{qs, qe, count, niv, off, pivot, 0u};
+    return true;
+  }
+};
+
 // Candidate search for one read.  Returns the number of candidates, or ~0u on overflow
 // of a set, the candidate list or the interval pool (flags in st).
 template <bool COUNT_TOUCH, class SR>
@@ -367,32 +452,15 @@ __device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf,
                              const SR& wa, const SR& wb, uint32_t set_cap, Cand* cands, uint32_t cand_cap,
                              Pool& ivpool, uint32_t& st, uint64_t& touches) {
   using TL = TwoList<SR>;
-  uint32_t nc = 0;
   if (n == 0 || P.min_len == 0) return 0;
   const BIv full = {0, Fw.text_len, 0, Fw.text_len};
   bool ovf = false;
-  auto qmask = [&](const SmemFm& S, uint8_t c) -> uint32_t { return c < 16 ? S.compat_mask[c] : 0u; };
-  auto emit = [&](uint32_t qs, uint32_t qe, uint32_t count, const TL& ivs) -> bool {
-    if (nc >= cand_cap) { st |= ST_CAND_OVF; return false; }
-    uint32_t niv = ivs.size();
-    uint64_t off = thread_reserve(ivpool, niv);
-    if (off == ~0ull) { st |= ST_POOL_OVF; return false; }
-    BIv* dst = (BIv*)ivpool.base + off;
-    for (uint32_t k = 0; k < ivs.n1; k++) dst[k] = ivs.s[k];
-    for (uint32_t k = 0; k < ivs.nb; k++) dst[ivs.n1 + k] = ivs.s[set_cap - 1 - k];
-    cands[nc++] = Cand{qs, qe, count, niv, off};
-    return true;
-  };
-  // the full interval (the empty pattern) as a one-element list
-  auto start_full = [&](TL& t) {
-    if (full.fhi - full.flo == 1) { t.s[0] = full; t.n1 = 1; t.nb = 0; }
-    else { t.s[set_cap - 1] = full; t.n1 = 0; t.nb = 1; }
-  };
+  CandSink<SR> sink{cands, 0, cand_cap, &ivpool, &st, set_cap};
   if (P.mode == 1) {
     // find_mems: raw_mem_from(i) for every start (src/fm_index/smem.rs:250-295)
     for (uint32_t i = 0; i < n; i++) {
       TL c{curr, 0, 0}, x{nxt, 0, 0};
-      start_full(c);
+      start_full(c, full, set_cap);
       uint32_t cov = 0, j = i;
       bool matched = false;
       while (j < n) {
@@ -405,57 +473,17 @@ __device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf,
       if (!matched || j - i < P.min_len) continue;
       bool lmax = i == 0 || !any_extend<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[i - 1]), c, set_cap, touches);
       if (!lmax) continue;
-      if (!emit(i, j, cov, c)) return ~0u;
+      if (!sink(i, j, cov, c, i)) return ~0u;
     }
-    return nc;
+    return sink.nc;
   }
   // find_smems: collect_smem_candidates (src/fm_index/smem.rs:154-222)
   uint32_t pivot = 0;
   while (pivot < n) {
-    TL c{curr, 0, 0}, x{nxt, 0, 0};
-    start_full(x);
-    uint32_t cov;
-    extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[pivot]), x, c, set_cap, cov, ovf, touches);
-    if (ovf) { st |= ST_SET_OVF; return ~0u; }
-    if (c.size() == 0) { pivot++; continue; }
-    uint32_t j = pivot + 1, reach = pivot + 1;
-    for (;;) {
-      uint32_t end, ncov = 0;
-      bool next_empty, record;
-      x.n1 = x.nb = 0;
-      if (j == n) { end = n; next_empty = true; record = true; }
-      else {
-        extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, x, set_cap, ncov, ovf, touches);
-        if (ovf) { st |= ST_SET_OVF; return ~0u; }
-        end = j; next_empty = x.size() == 0; record = ncov != cov;
-      }
-      if (record) {
-        // right-maximal prefix [pivot, end): extend_left_maximally (smem.rs:227-243)
-        reach = end;
-        TL b = c;
-        uint32_t start = pivot, bcov = cov;
-        TL bufs[2] = {TL{wa, 0, 0}, TL{wb, 0, 0}};
-        int t = 0;
-        while (start > 0) {
-          uint32_t lcov;
-          extend_set<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[start - 1]), b, bufs[t], set_cap, lcov, ovf, touches);
-          if (ovf) { st |= ST_SET_OVF; return ~0u; }
-          if (bufs[t].size() == 0) break;
-          b = bufs[t]; bcov = lcov; t ^= 1; start--;
-        }
-        if (end - start >= P.min_len) {
-          // right-maximality (smem.rs:202-207); with no left extension it is next_empty
-          bool rmax = end == n ||
-                      (start == pivot ? next_empty : !any_extend<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[end]), b, set_cap, touches));
-          if (rmax && !emit(start, end, bcov, b)) return ~0u;
-        }
-      }
-      if (j == n || x.size() == 0) break;
-      TL tt = c; c = x; x = tt; cov = ncov; j++;
-    }
-    pivot = max(reach, pivot + 1);
+    pivot = smem_pivot<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q, n, pivot, P, curr, nxt, wa, wb, set_cap, st, touches, sink);
+    if (pivot == ~0u) return ~0u;
   }
-  return nc;
+  return sink.nc;
 }
 
 // Sort candidates by (qs, qe) (stable), drop duplicates, keep the containment-maximal ones
@@ -584,6 +612,197 @@ __global__ void __launch_bounds__(128, MINB) k_mems(DevFm Fw, DevFm Rv, const ui
   if (COUNT_TOUCH && touches) atomicAdd(out.touches, (unsigned long long)touches);
 }
 
+
+// =====================================================================================
+// Long reads: the SMEM sweep of a read cut into segments.
+//
+// The sweep visits a chain of pivots, next = max(reach(pivot), pivot + 1), and the next
+// pivot depends only on the read and the current pivot.  k_mems_seg gives one thread to
+// each seg_len-position segment of a long read and sweeps the chain as if a pivot started
+// at the segment's first position, recording the pivots it visits, the first pivot past
+// the segment, and its candidates tagged with their pivots.  k_mems_merge follows the
+// read's true chain across the segments: where it lands on a pivot the segment visited,
+// both chains agree from there to the segment's end, so the segment's candidates from that
+// pivot on are exactly the true chain's; elsewhere the merge sweeps the true chain itself
+// until it meets the segment's chain or leaves the segment.  The candidate set, and so
+// every result, is the one the unsegmented sweep produces; the critical path of a 10 kbp
+// read becomes one segment plus the merge instead of the whole read.
+// =====================================================================================
+constexpr uint32_t SEG_MAX = 4096;   // longest segment (pivot bitmap of SEG_MAX / 32 words)
+
+struct SegWork {
+  uint32_t seg_len, seg_words;    // positions per segment (multiple of 32, <= SEG_MAX)
+  const uint32_t* unit_read;      // read of each unit (segment)
+  const uint32_t* unit_k;         // segment index within its read
+  uint32_t n_units;
+  uint32_t* bits;                 // seg_words per unit: pivots the segment's chain visited
+  uint32_t* exit_pivot;           // per unit: first pivot past the segment, ~0u on failure
+  uint32_t* unit_st;              // per unit: status bits of a failed sweep
+  uint64_t* cand_off;             // per unit: first candidate in the unit pool
+  uint32_t* cand_cnt;             // per unit
+  Cand* pool; unsigned long long* pool_used; uint64_t pool_cap;
+  const uint32_t* long_ids;       // merge: long reads, in queue order
+  const uint64_t* unit_base;      // merge: first unit of each long read (n_long + 1)
+  uint32_t n_long;
+  unsigned int* merge_queue;
+  unsigned long long* touches;
+};
+
+// flags[k] = 1 when read ids[k] (k itself without ids) is longer than min_len.
+__global__ void k_long_flags(const uint32_t* __restrict__ ids, uint32_t n, const uint64_t* __restrict__ qoff,
+                             uint32_t min_len, uint32_t* __restrict__ flags) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  uint32_t i = ids ? ids[k] : k;
+  flags[k] = (qoff[i + 1] - qoff[i]) > min_len ? 1u : 0u;
+}
+
+// Stable split of ids by flag (lpos = exclusive scan of flags).
+__global__ void k_split_ids(const uint32_t* __restrict__ ids, uint32_t n, const uint32_t* __restrict__ flags,
+                            const uint64_t* __restrict__ lpos, uint32_t* __restrict__ short_ids,
+                            uint32_t* __restrict__ long_ids, uint32_t* __restrict__ seg_count,
+                            const uint64_t* __restrict__ qoff, uint32_t seg_len) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  uint32_t i = ids ? ids[k] : k;
+  uint32_t l = (uint32_t)lpos[k];
+  if (flags[k]) {
+    long_ids[l] = i;
+    uint32_t len = (uint32_t)(qoff[i + 1] - qoff[i]);
+    seg_count[l] = (len + seg_len - 1) / seg_len;
+  } else {
+    short_ids[k - l] = i;
+  }
+}
+
+__global__ void k_unit_fill(const uint32_t* __restrict__ long_ids, uint32_t n_long,
+                            const uint64_t* __restrict__ unit_base, uint32_t* __restrict__ unit_read,
+                            uint32_t* __restrict__ unit_k) {
+  uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_long) return;
+  uint64_t b = unit_base[r], e = unit_base[r + 1];
+  for (uint64_t u = b; u < e; u++) { unit_read[u] = long_ids[r]; unit_k[u] = (uint32_t)(u - b); }
+}
+
+template <bool COUNT_TOUCH, int STRIDE, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_mems_seg(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
+                                                 const uint16_t* __restrict__ compat_rv, const uint8_t* __restrict__ q,
+                                                 const uint64_t* __restrict__ qoff, MemsParams P, Pool ivpool,
+                                                 MemsWork W, SegWork G) {
+  __shared__ SmemFm Sf, Sr;
+  smem_fm_init(Sf, Fw, compat_fw);
+  smem_fm_init(Sr, Rv, compat_rv);
+  __syncthreads();
+  using SR = SetRef<BIv, STRIDE>;
+  SR s0 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 0), s1 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 1);
+  SR s2 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 2), s3 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 3);
+  uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  Cand* cands = W.cands + tid * W.cand_cap;
+  uint64_t touches = 0;
+  uint32_t u;
+  while (next_read(W.queue, G.n_units, nullptr, u)) {
+    uint32_t i = G.unit_read[u], k = G.unit_k[u];
+    uint64_t o = qoff[i];
+    uint32_t n = (uint32_t)(qoff[i + 1] - o);
+    uint32_t s = k * G.seg_len, e = min(n, s + G.seg_len);
+    uint32_t st = ST_OK;
+    uint64_t t0 = touches;
+    CandSink<SR> sink{cands, 0, W.cand_cap, &ivpool, &st, W.set_cap};
+    uint32_t* bits = G.bits + (size_t)u * G.seg_words;
+    for (uint32_t w = 0; w < G.seg_words; w++) bits[w] = 0;
+    uint32_t p = s;
+    while (p < e) {
+      uint32_t d = p - s;
+      bits[d >> 5] |= 1u << (d & 31);
+      p = smem_pivot<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
+      if (p == ~0u) break;
+    }
+    uint32_t nc = sink.nc;
+    if (p != ~0u && nc) {
+      unsigned long long off = atomicAdd(G.pool_used, (unsigned long long)nc);
+      if (off + nc > G.pool_cap) { st |= ST_POOL_OVF; p = ~0u; }
+      else {
+        for (uint32_t c = 0; c < nc; c++) G.pool[off + c] = cands[c];
+        G.cand_off[u] = off;
+      }
+    }
+    if (p == ~0u || nc == 0) G.cand_off[u] = 0;
+    G.cand_cnt[u] = p == ~0u ? 0u : nc;
+    G.exit_pivot[u] = p;
+    G.unit_st[u] = st;
+    if (COUNT_TOUCH && W.work_log) atomicAdd(W.work_log + 4 * (size_t)i, (uint32_t)(touches - t0));
+  }
+  if (COUNT_TOUCH && touches) atomicAdd(G.touches, (unsigned long long)touches);
+}
+
+template <bool COUNT_TOUCH, int STRIDE, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_mems_merge(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
+                                                   const uint16_t* __restrict__ compat_rv,
+                                                   const uint8_t* __restrict__ q, const uint64_t* __restrict__ qoff,
+                                                   MemsParams P, Pool ivpool, Pool hitpool, MemsOut out, MemsWork W,
+                                                   SegWork G) {
+  __shared__ SmemFm Sf, Sr;
+  smem_fm_init(Sf, Fw, compat_fw);
+  smem_fm_init(Sr, Rv, compat_rv);
+  __syncthreads();
+  using SR = SetRef<BIv, STRIDE>;
+  SR s0 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 0), s1 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 1);
+  SR s2 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 2), s3 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 3);
+  uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  Cand* cands = W.cands + tid * W.cand_cap;
+  uint64_t touches = 0;
+  uint32_t r;
+  while (next_read(G.merge_queue, G.n_long, nullptr, r)) {
+    uint32_t i = G.long_ids[r];
+    uint64_t o = qoff[i];
+    uint32_t n = (uint32_t)(qoff[i + 1] - o);
+    uint64_t u0 = G.unit_base[r], u1 = G.unit_base[r + 1];
+    uint32_t st = ST_OK;
+    uint64_t t0 = touches;
+    CandSink<SR> sink{cands, 0, W.cand_cap, &ivpool, &st, W.set_cap};
+    bool fail = false;
+    uint32_t t = 0;                                   // the true chain's next pivot
+    for (uint64_t u = u0; u < u1 && !fail; u++) {
+      uint32_t s = (uint32_t)(u - u0) * G.seg_len, e = min(n, s + G.seg_len);
+      if (t >= e) continue;                           // the chain jumps over this segment
+      if (G.exit_pivot[u] == ~0u) { st |= G.unit_st[u]; fail = true; break; }
+      uint32_t p = t;
+      const uint32_t* bits = G.bits + u * G.seg_words;
+      while (p < e && !((bits[(p - s) >> 5] >> ((p - s) & 31)) & 1u)) {
+        p = smem_pivot<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
+        if (p == ~0u) { fail = true; break; }
+      }
+      if (fail) break;
+      if (p < e) {                                    // met the segment's chain at p
+        const Cand* src = G.pool + G.cand_off[u];
+        uint32_t cnt = G.cand_cnt[u];
+        for (uint32_t c = 0; c < cnt; c++) {
+          Cand cd = src[c];
+          if (cd.pivot < p) continue;
+          if (sink.nc >= sink.cap) { st |= ST_CAND_OVF; fail = true; break; }
+          cands[sink.nc++] = cd;
+        }
+        t = G.exit_pivot[u];
+      } else {
+        t = p;
+      }
+    }
+    uint64_t hs = 0; uint32_t hc = 0;
+    if (!fail) {
+      uint32_t nc = P.mode == 0 ? finalize_smems(cands, sink.nc) : sink.nc;
+      if (!write_hits(cands, nc, P, ivpool, hitpool, hs, hc)) st |= ST_POOL_OVF;
+    }
+    if (st) { hs = 0; hc = 0; }
+    out.hit_start[i] = hs; out.hit_count[i] = hc; out.status[i] = st;
+    bool ovf = st & (ST_SET_OVF | ST_CAND_OVF);
+    if (COUNT_TOUCH && W.work_log) {
+      atomicAdd(W.work_log + 4 * (size_t)i, (uint32_t)(touches - t0));
+      if (ovf) atomicOr(W.work_log + 4 * (size_t)i + 3, 1u);
+    }
+    if (ovf) out.ovf_list[atomicAdd(out.n_ovf, 1u)] = i;
+  }
+  if (COUNT_TOUCH && touches) atomicAdd(out.touches, (unsigned long long)touches);
+}
 }  // namespace hfm
 
 // =====================================================================================

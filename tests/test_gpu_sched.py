@@ -81,3 +81,24 @@ def test_bad_order_rejected(mixed_case):
     with pytest.raises(FmIndexError):
         h.mems_sched_packed(flat, off, 19, 0, bounds, 64, order=None, n_warp=3)
     _same(h.mems_sched_packed(flat, off, 19, 0, bounds, 64), want)   # handle still usable
+
+
+def test_long_reads_segmented_sweep_repeats(oracle):
+    """Reads of 1-10 kbp on an ACGT genome with repeat families and tandem repeats take the
+    segmented SMEM sweep (256-position segments merged along the true pivot chain): bytes
+    equal the oracle's whole-read sweep, in both index alphabets' ACGT case."""
+    ref = synth.repeat_reference(total=3_000_000, n_contigs=6, seed=41)
+    flat, off, lens = synth.sample_mixed_reads(ref, n_reads=120, short_frac=0.3, long_median=2500, seed=42,
+                                               n_rate=0.0)
+    assert (lens > 1024).sum() >= 40
+    for tag in (1, 0):
+        b = _build([al.DnaSequence(c) for c in ref.contigs], FmIndexConfig(sa_sample_rate=32, lookup_depth=8),
+                   tag, KIND_BIDIR)
+        idx = BidirFmIndex.from_bytes(b)
+        bounds = idx.seq_boundaries()
+        want = oracle.OracleIndex(b, KIND_BIDIR).mems_packed(flat, off, 19, 0, bounds, 256, threads=8)
+        got = idx.handle.mems_packed(flat, off, 19, 0, bounds, 256)
+        for g, w in zip(got, want):
+            assert np.array_equal(g, w)
+        # and under a schedule that puts the long reads first
+        _same(idx.handle.mems_sched_packed(flat, off, 19, 0, bounds, 256, order=np.argsort(-lens)), want)
