@@ -86,7 +86,7 @@ struct DevBuf {
 
 struct Counters {                    // device-side counters, one block per handle
   unsigned long long iv_used, hit_used, touches, steps, seg_used;
-  uint32_t n_ovf, still_ovf, walk_err, queue, queue2, n_mid, n_wrp, queue3, seg_queue, merge_queue;
+  uint32_t n_ovf, still_ovf, walk_err, queue, queue2, n_mid, n_wrp, queue3, seg_queue, merge_queue, fix_queue, _pad;
 };
 
 struct FmDev {
@@ -111,7 +111,8 @@ struct hfm_index {
   DevBuf q, qoff, counts, nhits, niv, ivoff, status, ovf, ivpool, hitpool, seg_row, seg_off, pos_base, seg_base,
       scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr,
       mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout, blockmap, blockmap2, ovf2, ovf3,
-      lflag, lpos, sids, lids, ucount, ubase, uread, uk, ubits, uexit, ust, ucoff, ucnt, segpool;
+      lflag, lpos, sids, lids, ucount, ubase, uread, uk, ubits, uexit, ust, ucoff, ucnt, segpool, fxe, fxc, fxx,
+      fxo, fxn;
   uint32_t flags = 0;
   uint32_t seg_len = 512;  // SMEM reads longer than 2 * seg_len take the segmented sweep
   int mems_variant = 3;   // SMEM fast-kernel variant (see mems_device): 0/1/2 local 32-entry
@@ -536,6 +537,8 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       RET(x->uread.ensure(n_units * 4)); RET(x->uk.ensure(n_units * 4));
       RET(x->ubits.ensure(n_units * (x->seg_len / 32) * 4)); RET(x->uexit.ensure(n_units * 4));
       RET(x->ust.ensure(n_units * 4)); RET(x->ucoff.ensure(n_units * 8)); RET(x->ucnt.ensure(n_units * 4));
+      RET(x->fxe.ensure(n_units * 4)); RET(x->fxc.ensure(n_units * 4)); RET(x->fxx.ensure(n_units * 4));
+      RET(x->fxo.ensure(n_units * 8)); RET(x->fxn.ensure(n_units * 4));
       k_unit_fill<<<(n_long + 255) / 256, 256, 0, x->stream>>>(x->lids.as<uint32_t>(), n_long, x->ubase.as<uint64_t>(),
                                                                x->uread.as<uint32_t>(), x->uk.as<uint32_t>());
       other++;
@@ -599,9 +602,12 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       SegWork G{x->seg_len, x->seg_len / 32, x->uread.as<uint32_t>(), x->uk.as<uint32_t>(), (uint32_t)n_units, x->ubits.as<uint32_t>(),
                 x->uexit.as<uint32_t>(), x->ust.as<uint32_t>(), x->ucoff.as<uint64_t>(), x->ucnt.as<uint32_t>(),
                 x->segpool.as<Cand>(), &dctr(x)->seg_used, x->seg_cap, x->lids.as<uint32_t>(),
-                x->ubase.as<uint64_t>(), n_long, &dctr(x)->merge_queue, &dctr(x)->touches};
+                x->ubase.as<uint64_t>(), n_long, &dctr(x)->merge_queue, &dctr(x)->touches, x->fxe.as<uint32_t>(),
+                x->fxc.as<uint32_t>(), x->fxx.as<uint32_t>(), x->fxo.as<uint64_t>(), x->fxn.as<uint32_t>()};
       MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), FAST_CAND_CAP, &dctr(x)->seg_queue, nullptr,
                  0u, &dctr(x)->still_ovf, 0u, wlog};
+      MemsWork Wf = W;
+      Wf.queue = &dctr(x)->fix_queue;
       uint64_t ts = std::min<uint64_t>(threads / 128 * 128, (n_units + 127) / 128 * 128);
       uint64_t tmg = std::min<uint64_t>(threads / 128 * 128, ((uint64_t)n_long + 127) / 128 * 128);
       unsigned gs = (unsigned)std::max<uint64_t>(1, ts / 128), gm = (unsigned)std::max<uint64_t>(1, tmg / 128);
@@ -610,15 +616,19 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       if (counting) {
         k_mems_seg<true, 32, 5><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                            d_q, d_qoff, P, ivp, W, G);
+        k_mems_fix<true, 32, 5><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                           d_q, d_qoff, P, ivp, Wf, G);
         k_mems_merge<true, 32, 5><<<gm, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                              d_q, d_qoff, P, ivp, hp, o, W, G);
       } else {
         k_mems_seg<false, 32, 8><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                             d_q, d_qoff, P, ivp, W, G);
+        k_mems_fix<false, 32, 8><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
+                                                            d_q, d_qoff, P, ivp, Wf, G);
         k_mems_merge<false, 32, 8><<<gm, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                               d_q, d_qoff, P, ivp, hp, o, W, G);
       }
-      launches += 2;
+      launches += 3;
       CK(cudaGetLastError());
     }
     if (n_fast > 0 || n_long > 0) {
@@ -874,7 +884,7 @@ void hfm_index_free(hfm_index* x) {
                     &x->hkeys, &x->hslot, &x->hflags, &x->huid, &x->urow, &x->ulen, &x->uoff, &x->uout,
                     &x->blockmap, &x->blockmap2, &x->ovf2, &x->ovf3, &x->lflag, &x->lpos, &x->sids, &x->lids,
                     &x->ucount, &x->ubase, &x->uread, &x->uk, &x->ubits, &x->uexit, &x->ust, &x->ucoff, &x->ucnt,
-                    &x->segpool})
+                    &x->segpool, &x->fxe, &x->fxc, &x->fxx, &x->fxo, &x->fxn})
     b->release();
   for (auto& e : x->ev) if (e) cudaEventDestroy(e);
   for (auto& e : x->evk) if (e) cudaEventDestroy(e);

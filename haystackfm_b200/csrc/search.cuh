@@ -646,6 +646,13 @@ struct SegWork {
   uint32_t n_long;
   unsigned int* merge_queue;
   unsigned long long* touches;
+  // fix-up pass: segment j swept again from the previous segment's exit pivot (the true
+  // chain's entry whenever the previous segment's chain met the true one)
+  uint32_t* fx_entry;             // entry pivot used, ~0u when not computed
+  uint32_t* fx_conv;              // pivot where it met the segment's chain, ~0u if it did not
+  uint32_t* fx_exit;              // first pivot past the segment when it did not meet it
+  uint64_t* fx_off;               // its own candidates (pivots before fx_conv) in the pool
+  uint32_t* fx_cnt;
 };
 
 // flags[k] = 1 when read ids[k] (k itself without ids) is longer than min_len.
@@ -735,6 +742,60 @@ __global__ void __launch_bounds__(128, MINB) k_mems_seg(DevFm Fw, DevFm Rv, cons
   if (COUNT_TOUCH && touches) atomicAdd(G.touches, (unsigned long long)touches);
 }
 
+// Fix-up pass, one thread per segment after the first: sweeps from the previous segment's
+// exit pivot until the chain meets this segment's chain (usually within a few pivots), so
+// the merge below only has to check that the entry it assumed is the true one.
+template <bool COUNT_TOUCH, int STRIDE, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_mems_fix(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
+                                                 const uint16_t* __restrict__ compat_rv, const uint8_t* __restrict__ q,
+                                                 const uint64_t* __restrict__ qoff, MemsParams P, Pool ivpool,
+                                                 MemsWork W, SegWork G) {
+  __shared__ SmemFm Sf, Sr;
+  smem_fm_init(Sf, Fw, compat_fw);
+  smem_fm_init(Sr, Rv, compat_rv);
+  __syncthreads();
+  using SR = SetRef<BIv, STRIDE>;
+  SR s0 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 0), s1 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 1);
+  SR s2 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 2), s3 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 3);
+  uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  Cand* cands = W.cands + tid * W.cand_cap;
+  uint64_t touches = 0;
+  uint32_t u;
+  while (next_read(W.queue, G.n_units, nullptr, u)) {
+    uint32_t i = G.unit_read[u], k = G.unit_k[u];
+    G.fx_entry[u] = ~0u; G.fx_conv[u] = ~0u; G.fx_exit[u] = ~0u; G.fx_off[u] = 0; G.fx_cnt[u] = 0;
+    if (k == 0 || G.exit_pivot[u - 1] == ~0u || G.exit_pivot[u] == ~0u) continue;
+    uint64_t o = qoff[i];
+    uint32_t n = (uint32_t)(qoff[i + 1] - o);
+    uint32_t s = k * G.seg_len, e = min(n, s + G.seg_len);
+    uint32_t entry = G.exit_pivot[u - 1];
+    if (entry >= e) { G.fx_entry[u] = entry; G.fx_exit[u] = entry; continue; }
+    const uint32_t* bits = G.bits + (size_t)u * G.seg_words;
+    uint32_t st = ST_OK;
+    uint64_t t0 = touches;
+    CandSink<SR> sink{cands, 0, W.cand_cap, &ivpool, &st, W.set_cap};
+    uint32_t p = entry;
+    while (p < e && !((bits[(p - s) >> 5] >> ((p - s) & 31)) & 1u)) {
+      p = smem_pivot<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
+      if (p == ~0u) break;
+    }
+    if (COUNT_TOUCH && W.work_log) atomicAdd(W.work_log + 4 * (size_t)i, (uint32_t)(touches - t0));
+    if (p == ~0u) continue;                       // the merge sweeps this segment itself
+    uint32_t nc = sink.nc;
+    if (nc) {
+      unsigned long long off = atomicAdd(G.pool_used, (unsigned long long)nc);
+      if (off + nc > G.pool_cap) continue;        // pool exhausted: counted, regrown by the host
+      for (uint32_t c = 0; c < nc; c++) G.pool[off + c] = cands[c];
+      G.fx_off[u] = off;
+      G.fx_cnt[u] = nc;
+    }
+    if (p < e) { G.fx_conv[u] = p; G.fx_exit[u] = G.exit_pivot[u]; }
+    else G.fx_exit[u] = p;
+    G.fx_entry[u] = entry;
+  }
+  if (COUNT_TOUCH && touches) atomicAdd(G.touches, (unsigned long long)touches);
+}
+
 template <bool COUNT_TOUCH, int STRIDE, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_mems_merge(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
                                                    const uint16_t* __restrict__ compat_rv,
@@ -766,6 +827,30 @@ __global__ void __launch_bounds__(128, MINB) k_mems_merge(DevFm Fw, DevFm Rv, co
       uint32_t s = (uint32_t)(u - u0) * G.seg_len, e = min(n, s + G.seg_len);
       if (t >= e) continue;                           // the chain jumps over this segment
       if (G.exit_pivot[u] == ~0u) { st |= G.unit_st[u]; fail = true; break; }
+      if (u > u0 && G.fx_entry[u] == t) {             // the fix-up pass started where the chain enters
+        const Cand* fx = G.pool + G.fx_off[u];
+        uint32_t fcnt = G.fx_cnt[u];
+        for (uint32_t c = 0; c < fcnt && !fail; c++) {
+          if (sink.nc >= sink.cap) { st |= ST_CAND_OVF; fail = true; break; }
+          cands[sink.nc++] = fx[c];
+        }
+        if (fail) break;
+        uint32_t cv = G.fx_conv[u];
+        if (cv != ~0u) {
+          const Cand* src = G.pool + G.cand_off[u];
+          uint32_t cnt = G.cand_cnt[u];
+          for (uint32_t c = 0; c < cnt; c++) {
+            Cand cd = src[c];
+            if (cd.pivot < cv) continue;
+            if (sink.nc >= sink.cap) { st |= ST_CAND_OVF; fail = true; break; }
+            cands[sink.nc++] = cd;
+          }
+          t = G.exit_pivot[u];
+        } else {
+          t = G.fx_exit[u];
+        }
+        continue;
+      }
       uint32_t p = t;
       const uint32_t* bits = G.bits + u * G.seg_words;
       while (p < e && !((bits[(p - s) >> 5] >> ((p - s) & 31)) & 1u)) {

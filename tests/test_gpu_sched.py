@@ -15,8 +15,10 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def mixed_case(oracle):
-    """2 Mbp IUPAC reference; 240 mixed-length reads (150 bp and 100 bp .. 10 kbp)."""
-    ref = synth.iupac_reference(total=2_000_000, n_contigs=20, seed=31)
+    """2 Mbp IUPAC reference (N runs of mean 60 bp: a reference N matches every query base,
+    and reads longer than the longest N run make the SMEM sweep quadratic in it); 240
+    mixed-length reads (150 bp and 100 bp .. 10 kbp)."""
+    ref = synth.iupac_reference(total=2_000_000, n_contigs=20, n_run_mean=60, seed=31)
     flat, off, lens = synth.sample_mixed_reads(ref, n_reads=240, seed=32)
     b = _build([al.DnaSequence(c) for c in ref.contigs], FmIndexConfig(sa_sample_rate=32, lookup_depth=10), 0,
                KIND_BIDIR)
