@@ -283,6 +283,7 @@ def mixed_workload(args, device, torch):
     ls = LearnedSmem(h, device, seed=1)
     qt = torch.from_numpy(flat_t).to(dev)
     ot = torch.from_numpy(off_t.view(np.int64)).to(dev)
+    tuning = h.autotune_mems(qt, ot, m, 19, 0, bounds, 1024, reps=1)     # on the training reads
     losses, _, _ = ls.fit(qt, ot, m, 19, 0, bounds, 1024, epochs=8, batch=4096, lr=1e-3)
     del qt, ot
     ev_log = ls.log_work(q, o, m, 19, 0, bounds, 1024)
@@ -315,7 +316,7 @@ def mixed_workload(args, device, torch):
         res[name] = e0.elapsed_time(e1) / args.steps
     return {"workload": "mixed_length_repeats_locate_smem", "reads": m, "read_mbp": round(len(flat) / 1e6, 1),
             "genome": f"{args.ref_len // 1_000_000} Mbp ACGT, 40% interspersed repeats, 5% tandem repeats",
-            "alphabet": "ExactDna", "setup_s": round(setup_s, 1),
+            "alphabet": "ExactDna", "setup_s": round(setup_s, 1), "autotuned": tuning,
             "plain_ms_per_step": res["plain"], "plain_reads_per_s": m / (res["plain"] / 1000),
             "learned_ms_per_step": res["learned"], "learned_reads_per_s": m / (res["learned"] / 1000),
             "learned_enabled": bool(ls.enabled), "calibration": ls.calibration,
@@ -366,12 +367,13 @@ def main():
     stream = torch.cuda.ExternalStream(h.stream(), device=dev)
 
     # learned cost model: trained on the logged work of a separate seeded read sample
-    learned, learned_info = None, None
+    learned, learned_info, tuning_main = None, None, None
     if not args.no_learned:
         from haystackfm_b200.cost_model import LearnedSmem, prediction_error, work_targets
         tr = synth.sample_reads(ref, n_reads=args.train_reads, seed=1000 + rank)
         tr_d = torch.from_numpy(tr.reshape(-1)).to(dev)
         tr_off = torch.arange(0, (args.train_reads + 1) * 150, 150, dtype=torch.int64, device=dev)
+        tuning_main = h.autotune_mems(tr_d, tr_off, args.train_reads, 19, 0, bounds, 1024, reps=1)
         learned = LearnedSmem(h, local, seed=1)
         t0 = time.perf_counter()
         losses, _, _ = learned.fit(tr_d, tr_off, args.train_reads, 19, 0, bounds, 1024, epochs=args.train_epochs,
@@ -594,7 +596,7 @@ def main():
                        "index_build_s": round(build_s, 1), "index_cached": not built,
                        "locate_positions": int(loc_total), "mem_hits": int(n_hits), "mem_positions": int(n_pos),
                        "distinct_rows_walked": int(rows_walked(c_mem) + rows_walked(c_loc)),
-                       "parallelism": f"replicas{world}" if world > 1 else "single"},
+                       "parallelism": f"replicas{world}" if world > 1 else "single", "autotuned": tuning_main},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "plain": plain_info, "learned": learned_info, "serving": serving, "mixed": mixed,
             "clocks": clk,

@@ -64,6 +64,10 @@ class HfmSched(C.Structure):
     _fields_ = [("d_order", C.c_void_p), ("n_warp", C.c_uint32), ("_pad", C.c_uint32), ("d_work_log", C.c_void_p)]
 
 
+class HfmTuning(C.Structure):
+    _fields_ = [("mems_variant", C.c_uint32), ("seg_len", C.c_uint32)]
+
+
 class HfmStats(C.Structure):
     _fields_ = [("ms_search", C.c_float), ("ms_resolve", C.c_float), ("ms_total", C.c_float),
                 ("ms_search_kernel", C.c_float), ("ms_resolve_kernel", C.c_float),
@@ -112,6 +116,11 @@ SIGNATURES = {
                                 C.c_float, C.c_uint64, C.POINTER(C.c_float)]),
     "hfm_mlp_schedule": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_float, C.c_void_p,
                                    C.POINTER(C.c_uint32)]),
+    "hfm_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(HfmTuning)]),
+    "hfm_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(HfmTuning)]),
+    "hfm_autotune_mems": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, u32p,
+                                    C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(HfmTuning),
+                                    C.POINTER(C.c_float)]),
     "hfm_free": (None, [C.c_void_p]),
     "hfm_last_error": (C.c_char_p, []),
     "hfm_index_stream": (C.c_void_p, [C.c_void_p]),

@@ -910,6 +910,55 @@ int hfm_last_stats(const hfm_index* x, hfm_stats* o) {
   return HFM_OK;
 }
 
+int hfm_get_tuning(const hfm_index* x, hfm_tuning* t) {
+  if (!x || !t) return set_error(HFM_E_ARG, "NULL argument");
+  t->mems_variant = (uint32_t)x->mems_variant;
+  t->seg_len = x->seg_len;
+  return HFM_OK;
+}
+
+int hfm_set_tuning(hfm_index* x, const hfm_tuning* t) {
+  if (!x || !t) return set_error(HFM_E_ARG, "NULL argument");
+  if (t->mems_variant > 3) return set_error(HFM_E_ARG, "mems_variant must be 0..3");
+  if (t->seg_len < 64 || t->seg_len > SEG_MAX || t->seg_len % 32) return set_error(HFM_E_ARG, "seg_len must be a multiple of 32 in 64..4096");
+  std::lock_guard<std::mutex> lk(x->mu);
+  x->mems_variant = (int)t->mems_variant;
+  x->seg_len = t->seg_len;
+  return HFM_OK;
+}
+
+int hfm_autotune_mems(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t min_len,
+                      uint32_t mode, const uint32_t* ref_bounds, uint32_t nb, uint32_t cap, uint32_t reps,
+                      hfm_tuning* best, float* times_ms) {
+  if (!x || !best || (nq && !d_qoff) || (nb && !ref_bounds)) return set_error(HFM_E_ARG, "NULL argument");
+  if (x->kind != HFM_KIND_BIDIR) return set_error(HFM_E_ARG, "MEM/SMEM search needs a bidirectional index");
+  reps = std::max(1u, reps);
+  Guard g(x);
+  const hfm_tuning cands[] = {{3, 512}, {3, 256}, {3, 1024}, {2, 512}};
+  const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
+  int saved_v = x->mems_variant;
+  uint32_t saved_s = x->seg_len;
+  float best_ms = 0.f;
+  int best_k = -1;
+  for (int k = 0; k < nc; k++) {
+    x->mems_variant = (int)cands[k].mems_variant;
+    x->seg_len = cands[k].seg_len;
+    float t = 0.f;
+    for (uint32_t r = 0; r <= reps; r++) {       // first run warms the pools
+      hfm_dev_mems out;
+      int rc = mems_device(x, d_q, d_qoff, nq, min_len, mode, ref_bounds, nb, cap, &out);
+      if (rc) { x->mems_variant = saved_v; x->seg_len = saved_s; return rc; }
+      if (r > 0) t = r == 1 ? x->stats.ms_total : std::min(t, x->stats.ms_total);
+    }
+    if (times_ms) times_ms[k] = t;
+    if (best_k < 0 || t < best_ms) { best_ms = t; best_k = k; }
+  }
+  x->mems_variant = (int)cands[best_k].mems_variant;
+  x->seg_len = cands[best_k].seg_len;
+  *best = cands[best_k];
+  return HFM_OK;
+}
+
 int hfm_set_counters(hfm_index* x, int enable) {
   if (!x) return set_error(HFM_E_ARG, "NULL argument");
   x->count_work = enable != 0;

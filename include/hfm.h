@@ -249,6 +249,25 @@ void* hfm_index_stream(hfm_index* idx);    /* the handle's cudaStream_t (for eve
 int hfm_last_stats(const hfm_index* idx, hfm_stats* out);
 int hfm_set_counters(hfm_index* idx, int enable);  /* per-read work counters on/off (default off) */
 
+/* Tunable parameters of the SMEM/MEM search and their autotuner (no counterpart in the
+ * reference).  mems_variant: fast pass with 32-entry candidate lists in local memory at 5,
+ * 6 or 8 resident blocks per SM (0, 1, 2) or 1024-entry lists in global memory at 8 blocks
+ * (3, default).  seg_len: SMEM reads longer than 2*seg_len are swept in seg_len-position
+ * segments (multiple of 32 in 64..4096, default 512).  Results never depend on them.
+ * hfm_autotune_mems times the search of a sample batch under each candidate setting
+ * (variant 3 with seg_len 512, 256, 1024; variant 2), best of `reps` runs after a warm-up
+ * run, by CUDA events on the handle's stream; it keeps the fastest on the handle, writes it
+ * to *best, and the candidates' times to times_ms[4] when non-NULL. */
+typedef struct hfm_tuning {
+  uint32_t mems_variant;
+  uint32_t seg_len;
+} hfm_tuning;
+int hfm_get_tuning(const hfm_index* idx, hfm_tuning* out);
+int hfm_set_tuning(hfm_index* idx, const hfm_tuning* t);
+int hfm_autotune_mems(hfm_index* idx, const uint8_t* d_q, const uint64_t* d_q_off, uint32_t nq, uint32_t min_len,
+                      uint32_t mode, const uint32_t* ref_bounds, uint32_t n_bounds, uint32_t max_hits,
+                      uint32_t reps, hfm_tuning* best, float* times_ms);
+
 #ifdef __cplusplus
 }
 #endif

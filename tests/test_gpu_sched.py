@@ -104,3 +104,31 @@ def test_long_reads_segmented_sweep_repeats(oracle):
             assert np.array_equal(g, w)
         # and under a schedule that puts the long reads first
         _same(idx.handle.mems_sched_packed(flat, off, 19, 0, bounds, 256, order=np.argsort(-lens)), want)
+
+
+def test_autotune_keeps_results(oracle):
+    """The autotuner picks one of its candidate settings by measurement and results stay
+    byte-identical under every setting."""
+    import torch
+    ref = synth.repeat_reference(total=2_000_000, n_contigs=4, seed=51)
+    flat, off, lens = synth.sample_mixed_reads(ref, n_reads=80, short_frac=0.5, long_median=2000, seed=52,
+                                               n_rate=0.0)
+    b = _build([al.DnaSequence(c) for c in ref.contigs], FmIndexConfig(sa_sample_rate=32, lookup_depth=8), 1,
+               KIND_BIDIR)
+    idx = BidirFmIndex.from_bytes(b)
+    h = idx.handle
+    bounds = idx.seq_boundaries()
+    want = oracle.OracleIndex(b, KIND_BIDIR).mems_packed(flat, off, 19, 0, bounds, 128, threads=8)
+    q = torch.from_numpy(flat).cuda()
+    o = torch.from_numpy(off.view(np.int64)).cuda()
+    res = h.autotune_mems(q, o, len(off) - 1, 19, 0, bounds, 128, reps=1)
+    assert (res["mems_variant"], res["seg_len"]) in [(3, 512), (3, 256), (3, 1024), (2, 512)]
+    assert h.tuning() == {"mems_variant": res["mems_variant"], "seg_len": res["seg_len"]}
+    assert len(res["candidates_ms"]) == 4 and all(v > 0 for v in res["candidates_ms"].values())
+    for v, sl in [(3, 64), (3, 4096), (2, 512), (0, 512)]:
+        h.set_tuning(v, sl)
+        _same(h.mems_sched_packed(flat, off, 19, 0, bounds, 128), want)
+    with pytest.raises(FmIndexError):
+        h.set_tuning(4, 512)
+    with pytest.raises(FmIndexError):
+        h.set_tuning(3, 100)
