@@ -11,6 +11,7 @@
 // therefore no cap on interval-set size, as in the reference CPU
 // (src/fm_index/query.rs:248-274, src/fm_index/smem.rs:332-357).
 #pragma once
+#include <type_traits>
 #include "dev_index.cuh"
 
 namespace hfm {
@@ -38,16 +39,56 @@ struct SetRef {
   __device__ __forceinline__ T& operator[](uint32_t i) const { return p[(size_t)i * STRIDE]; }
 };
 
+// Interval sets of the SMEM path store a bidirectional interval as three u32 planes
+// (flo, rlo, size): fhi - flo == rhi - rlo always holds, so 12 bytes carry the 16 of a BIv
+// and the sets' traffic (most DRAM writes of the search) drops by a quarter.  Single-row
+// intervals (the front list of a TwoList) store only (flo, rlo): their size is 1.
+template <int STRIDE>
+struct SetRef<BIv, STRIDE> {
+  uint32_t* p;          // this thread's slot: field f of element i at p[(f * cap + i) * STRIDE]
+  uint32_t plane;       // cap * STRIDE
+  struct Ref {
+    uint32_t* a; uint32_t plane;
+    __device__ __forceinline__ operator BIv() const {
+      uint32_t f = a[0], r = a[plane], z = a[2 * plane];
+      return BIv{f, f + z, r, r + z};
+    }
+    __device__ __forceinline__ Ref& operator=(const BIv& v) {
+      a[0] = v.flo; a[plane] = v.rlo; a[2 * plane] = v.fhi - v.flo;
+      return *this;
+    }
+  };
+  __device__ __forceinline__ Ref operator[](uint32_t i) const { return Ref{p + (size_t)i * STRIDE, plane}; }
+  __device__ __forceinline__ BIv single(uint32_t i) const {
+    const uint32_t* a = p + (size_t)i * STRIDE;
+    uint32_t f = a[0], r = a[plane];
+    return BIv{f, f + 1, r, r + 1};
+  }
+  __device__ __forceinline__ void set_single(uint32_t i, uint32_t flo, uint32_t rlo) const {
+    uint32_t* a = p + (size_t)i * STRIDE;
+    a[0] = flo; a[plane] = rlo;
+  }
+};
+
 // Set s (of NS) of the calling thread inside `work`, `cap` elements each.
 // STRIDE 32: warp-interleaved slices (fast path); STRIDE 1: contiguous per-thread slices.
 template <class T, int STRIDE>
 __device__ __forceinline__ SetRef<T, STRIDE> thread_set(T* work, uint32_t cap, int NS, int s) {
   uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (STRIDE == 32) {
-    uint64_t warp = tid >> 5, lane = tid & 31;
-    return SetRef<T, STRIDE>{work + ((warp * NS + s) * cap) * 32 + lane};
+  if constexpr (std::is_same<T, BIv>::value) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(work);           // 3 planes of cap u32 per set
+    if (STRIDE == 32) {
+      uint64_t warp = tid >> 5, lane = tid & 31;
+      return SetRef<T, STRIDE>{w + ((warp * NS + s) * cap * 3) * 32 + lane, cap * STRIDE};
+    }
+    return SetRef<T, STRIDE>{w + (tid * NS + s) * cap * 3, cap * STRIDE};
+  } else {
+    if (STRIDE == 32) {
+      uint64_t warp = tid >> 5, lane = tid & 31;
+      return SetRef<T, STRIDE>{work + ((warp * NS + s) * cap) * 32 + lane};
+    }
+    return SetRef<T, STRIDE>{work + (tid * NS + s) * cap};
   }
-  return SetRef<T, STRIDE>{work + (tid * NS + s) * cap};
 }
 
 // Next read from the device queue: reads are ids[k] (or k itself when ids is null).
@@ -268,17 +309,15 @@ __device__ __forceinline__ void extend_set(const DevFm& X, const SmemFm& S, uint
                                            uint64_t& touches) {
   out.n1 = 0; out.nb = 0; cov = 0;
   for (uint32_t i = 0; i < in.n1; i++) {
-    BIv iv = in.s[i];
+    BIv iv = in.s.single(i);
     uint32_t a = DIR == 0 ? iv.rlo : iv.flo, base = DIR == 0 ? iv.flo : iv.rlo;
     uint32_t s0, rk;
     row_symbol_rank(X, a, s0, rk);
     if (COUNT_TOUCH) touches += 1;
     if ((mask >> s0) & 1) {
       if (out.n1 + out.nb >= cap) { ovf = true; return; }
-      BIv e;
-      if (DIR == 0) { e.flo = base; e.fhi = base + 1; e.rlo = S.C[s0] + rk; e.rhi = S.C[s0] + rk + 1; }
-      else { e.flo = S.C[s0] + rk; e.fhi = S.C[s0] + rk + 1; e.rlo = base; e.rhi = base + 1; }
-      out.s[out.n1++] = e;
+      if (DIR == 0) out.s.set_single(out.n1++, base, S.C[s0] + rk);
+      else out.s.set_single(out.n1++, S.C[s0] + rk, base);
       cov += 1;
     }
   }
@@ -299,7 +338,7 @@ __device__ __forceinline__ void extend_set(const DevFm& X, const SmemFm& S, uint
         BIv e;
         if (DIR == 0) { e.flo = base + run; e.fhi = base + run + d; e.rlo = S.C[s] + rl[s]; e.rhi = S.C[s] + rh[s]; }
         else { e.flo = S.C[s] + rl[s]; e.fhi = S.C[s] + rh[s]; e.rlo = base + run; e.rhi = base + run + d; }
-        if (d == 1) out.s[out.n1++] = e;
+        if (d == 1) out.s.set_single(out.n1++, e.flo, e.rlo);
         else out.s[cap - 1 - out.nb++] = e;
         cov += d;
       }
@@ -314,7 +353,7 @@ __device__ __forceinline__ bool any_extend(const DevFm& X, const SmemFm& S, uint
                                            uint32_t cap, uint64_t& touches) {
   bool any = false;
   for (uint32_t i = 0; i < in.n1; i++) {
-    BIv iv = in.s[i];
+    BIv iv = in.s.single(i);
     uint32_t s0, rk;
     row_symbol_rank(X, DIR == 0 ? iv.rlo : iv.flo, s0, rk);
     if (COUNT_TOUCH) touches += 1;
@@ -362,7 +401,7 @@ __device__ __forceinline__ void sort_by_flo(BIv* a, uint32_t n) {
 // The full interval (the empty pattern) as a one-element two-list set.
 template <class SR>
 __device__ __forceinline__ void start_full(TwoList<SR>& t, const BIv& full, uint32_t set_cap) {
-  if (full.fhi - full.flo == 1) { t.s[0] = full; t.n1 = 1; t.nb = 0; }
+  if (full.fhi - full.flo == 1) { t.s.set_single(0, full.flo, full.rlo); t.n1 = 1; t.nb = 0; }
   else { t.s[set_cap - 1] = full; t.n1 = 0; t.nb = 1; }
 }
 
@@ -437,7 +476,7 @@ struct CandSink {
     uint64_t off = thread_reserve(*ivpool, niv);
     if (off == ~0ull) { *st |= ST_POOL_OVF; return false; }
     BIv* dst = (BIv*)ivpool->base + off;
-    for (uint32_t k = 0; k < ivs.n1; k++) dst[k] = ivs.s[k];
+    for (uint32_t k = 0; k < ivs.n1; k++) dst[k] = ivs.s.single(k);
     for (uint32_t k = 0; k < ivs.nb; k++) dst[ivs.n1 + k] = ivs.s[set_cap - 1 - k];
     cands[nc++] = Cand{qs, qe, count, niv, off, pivot, 0u};
     return true;
