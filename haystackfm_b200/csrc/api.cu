@@ -510,7 +510,7 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   const uint32_t* fast_ids = order ? order + n_warp : nullptr;
   uint32_t n_fast = nq - n_warp, n_long = 0;
   uint64_t n_units = 0;
-  if (mode == 0 && variant == 3 && n_fast > 0) {
+  if (mode == 0 && variant == 3 && n_fast > 0 && min_len > 0) {
     RET(x->lflag.ensure((size_t)n_fast * 4 + 4));
     RET(x->lpos.ensure(((size_t)n_fast + 1) * 8));
     k_long_flags<<<(n_fast + 255) / 256, 256, 0, x->stream>>>(fast_ids, n_fast, d_qoff, 2 * x->seg_len,
@@ -568,7 +568,7 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       CK(cudaMemcpyAsync(&dctr(x)->n_ovf, &n_warp, 4, cudaMemcpyHostToDevice, x->stream));
     }
     if (n_fast > 0 || n_long > 0) cudaEventRecord(x->evk[0], x->stream);
-    if (n_fast > 0) {
+    if (n_fast > 0 && n_long == 0) {     // with long reads, k_mems_seg runs the short reads too
       MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, variant == 3 ? x->cwork.as<Cand>() : nullptr,
                  variant == 3 ? FAST_CAND_CAP : 0u, &dctr(x)->queue, fast_ids, n_fast, &dctr(x)->still_ovf, 0u, wlog};
       unsigned grid = (unsigned)(threads / 128);
@@ -601,28 +601,28 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       // segmented sweep of the long reads, then the merge along each read's true chain
       SegWork G{x->seg_len, x->seg_len / 32, x->uread.as<uint32_t>(), x->uk.as<uint32_t>(), (uint32_t)n_units, x->ubits.as<uint32_t>(),
                 x->uexit.as<uint32_t>(), x->ust.as<uint32_t>(), x->ucoff.as<uint64_t>(), x->ucnt.as<uint32_t>(),
-                x->segpool.as<Cand>(), &dctr(x)->seg_used, x->seg_cap, x->lids.as<uint32_t>(),
+                x->segpool.as<Cand>(), &dctr(x)->seg_used, x->seg_cap, fast_ids, n_fast, x->lids.as<uint32_t>(),
                 x->ubase.as<uint64_t>(), n_long, &dctr(x)->merge_queue, &dctr(x)->touches, x->fxe.as<uint32_t>(),
                 x->fxc.as<uint32_t>(), x->fxx.as<uint32_t>(), x->fxo.as<uint64_t>(), x->fxn.as<uint32_t>()};
       MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), FAST_CAND_CAP, &dctr(x)->seg_queue, nullptr,
                  0u, &dctr(x)->still_ovf, 0u, wlog};
       MemsWork Wf = W;
       Wf.queue = &dctr(x)->fix_queue;
-      uint64_t ts = std::min<uint64_t>(threads / 128 * 128, (n_units + 127) / 128 * 128);
+      uint64_t ts = std::min<uint64_t>(threads / 128 * 128, (n_units + n_fast + 127) / 128 * 128);
       uint64_t tmg = std::min<uint64_t>(threads / 128 * 128, ((uint64_t)n_long + 127) / 128 * 128);
       unsigned gs = (unsigned)std::max<uint64_t>(1, ts / 128), gm = (unsigned)std::max<uint64_t>(1, tmg / 128);
       if (x->memwork.cap < (size_t)gs * 128 * 4 * MEM_SET_CAP * 16 || x->cwork.cap < (size_t)gs * 128 * FAST_CAND_CAP * sizeof(Cand))
         return set_error(HFM_E_ARG, "internal: work area too small");
       if (counting) {
         k_mems_seg<true, 32, 5><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                           d_q, d_qoff, P, ivp, W, G);
+                                                           d_q, d_qoff, P, ivp, hp, o, W, G);
         k_mems_fix<true, 32, 5><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                            d_q, d_qoff, P, ivp, Wf, G);
         k_mems_merge<true, 32, 5><<<gm, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                              d_q, d_qoff, P, ivp, hp, o, W, G);
       } else {
         k_mems_seg<false, 32, 8><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                            d_q, d_qoff, P, ivp, W, G);
+                                                            d_q, d_qoff, P, ivp, hp, o, W, G);
         k_mems_fix<false, 32, 8><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
                                                             d_q, d_qoff, P, ivp, Wf, G);
         k_mems_merge<false, 32, 8><<<gm, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),

@@ -680,6 +680,8 @@ struct SegWork {
   uint64_t* cand_off;             // per unit: first candidate in the unit pool
   uint32_t* cand_cnt;             // per unit
   Cand* pool; unsigned long long* pool_used; uint64_t pool_cap;
+  const uint32_t* short_ids;      // k_mems_seg also runs these whole reads after the segments
+  uint32_t n_short;
   const uint32_t* long_ids;       // merge: long reads, in queue order
   const uint64_t* unit_base;      // merge: first unit of each long read (n_long + 1)
   uint32_t n_long;
@@ -730,11 +732,13 @@ __global__ void k_unit_fill(const uint32_t* __restrict__ long_ids, uint32_t n_lo
   for (uint64_t u = b; u < e; u++) { unit_read[u] = long_ids[r]; unit_k[u] = (uint32_t)(u - b); }
 }
 
+// One persistent queue over the segments of the long reads followed by the whole short
+// reads of the batch (the longest jobs first; the short reads fill the tail).
 template <bool COUNT_TOUCH, int STRIDE, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_mems_seg(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
                                                  const uint16_t* __restrict__ compat_rv, const uint8_t* __restrict__ q,
                                                  const uint64_t* __restrict__ qoff, MemsParams P, Pool ivpool,
-                                                 MemsWork W, SegWork G) {
+                                                 Pool hitpool, MemsOut out, MemsWork W, SegWork G) {
   __shared__ SmemFm Sf, Sr;
   smem_fm_init(Sf, Fw, compat_fw);
   smem_fm_init(Sr, Rv, compat_rv);
@@ -745,38 +749,65 @@ __global__ void __launch_bounds__(128, MINB) k_mems_seg(DevFm Fw, DevFm Rv, cons
   uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   Cand* cands = W.cands + tid * W.cand_cap;
   uint64_t touches = 0;
+  const uint32_t njobs = G.n_units + G.n_short;
   uint32_t u;
-  while (next_read(W.queue, G.n_units, nullptr, u)) {
-    uint32_t i = G.unit_read[u], k = G.unit_k[u];
+  while (next_read(W.queue, njobs, nullptr, u)) {
+    const bool unit = u < G.n_units;
+    uint32_t i, s, e;
+    uint32_t* bits = nullptr;
+    if (unit) i = G.unit_read[u];
+    else i = G.short_ids[u - G.n_units];
     uint64_t o = qoff[i];
     uint32_t n = (uint32_t)(qoff[i + 1] - o);
-    uint32_t s = k * G.seg_len, e = min(n, s + G.seg_len);
+    if (unit) {
+      s = G.unit_k[u] * G.seg_len;
+      e = min(n, s + G.seg_len);
+      bits = G.bits + (size_t)u * G.seg_words;
+      for (uint32_t w = 0; w < G.seg_words; w++) bits[w] = 0;
+    } else {
+      s = 0;
+      e = n;
+    }
     uint32_t st = ST_OK;
     uint64_t t0 = touches;
     CandSink<SR> sink{cands, 0, W.cand_cap, &ivpool, &st, W.set_cap};
-    uint32_t* bits = G.bits + (size_t)u * G.seg_words;
-    for (uint32_t w = 0; w < G.seg_words; w++) bits[w] = 0;
     uint32_t p = s;
     while (p < e) {
-      uint32_t d = p - s;
-      bits[d >> 5] |= 1u << (d & 31);
+      if (unit) { uint32_t d = p - s; bits[d >> 5] |= 1u << (d & 31); }
       p = smem_pivot<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
       if (p == ~0u) break;
     }
     uint32_t nc = sink.nc;
-    if (p != ~0u && nc) {
-      unsigned long long off = atomicAdd(G.pool_used, (unsigned long long)nc);
-      if (off + nc > G.pool_cap) { st |= ST_POOL_OVF; p = ~0u; }
-      else {
-        for (uint32_t c = 0; c < nc; c++) G.pool[off + c] = cands[c];
-        G.cand_off[u] = off;
+    if (unit) {
+      if (p != ~0u && nc) {
+        unsigned long long off = atomicAdd(G.pool_used, (unsigned long long)nc);
+        if (off + nc > G.pool_cap) { st |= ST_POOL_OVF; p = ~0u; }
+        else {
+          for (uint32_t c = 0; c < nc; c++) G.pool[off + c] = cands[c];
+          G.cand_off[u] = off;
+        }
       }
+      if (p == ~0u || nc == 0) G.cand_off[u] = 0;
+      G.cand_cnt[u] = p == ~0u ? 0u : nc;
+      G.exit_pivot[u] = p;
+      G.unit_st[u] = st;
+      if (COUNT_TOUCH && W.work_log) atomicAdd(W.work_log + 4 * (size_t)i, (uint32_t)(touches - t0));
+    } else {
+      // a whole short read: the same sweep as the fast pass, then its hits
+      uint64_t hs = 0; uint32_t hc = 0;
+      if (p != ~0u) {
+        nc = finalize_smems(cands, nc);
+        if (!write_hits(cands, nc, P, ivpool, hitpool, hs, hc)) st |= ST_POOL_OVF;
+      }
+      if (st) { hs = 0; hc = 0; }
+      out.hit_start[i] = hs; out.hit_count[i] = hc; out.status[i] = st;
+      bool ovf = st & (ST_SET_OVF | ST_CAND_OVF);
+      if (COUNT_TOUCH && W.work_log) {
+        W.work_log[4 * (size_t)i] += (uint32_t)(touches - t0);
+        if (ovf) W.work_log[4 * (size_t)i + 3] |= 1u;
+      }
+      if (ovf) out.ovf_list[atomicAdd(out.n_ovf, 1u)] = i;
     }
-    if (p == ~0u || nc == 0) G.cand_off[u] = 0;
-    G.cand_cnt[u] = p == ~0u ? 0u : nc;
-    G.exit_pivot[u] = p;
-    G.unit_st[u] = st;
-    if (COUNT_TOUCH && W.work_log) atomicAdd(W.work_log + 4 * (size_t)i, (uint32_t)(touches - t0));
   }
   if (COUNT_TOUCH && touches) atomicAdd(G.touches, (unsigned long long)touches);
 }
