@@ -387,7 +387,7 @@ def main():
                         "train_mse": [round(float(v), 5) for v in losses],
                         "holdout_error": learned.holdout_error.as_dict() if learned.holdout_error else None,
                         "eval_error": prediction_error(y_ev, work_targets(ev_log)).as_dict(),
-                        "enabled": bool(learned.enabled)}
+                        "calibration": learned.calibration, "enabled": bool(learned.enabled)}
         del ev_log
 
     def step(stats_out=None, plain=False):
@@ -590,6 +590,8 @@ def main():
                        "ref_len": args.ref_len, "contigs": args.contigs, "sa_sample_rate": 32, "lookup_depth": 10,
                        "min_len": 19, "max_hits_per_mem": 1024, "locate_kmer": 32,
                        "path": ("learned-binned" if learned is not None and learned.enabled else
+                                "plain order (learned order not faster on held-out reads)"
+                                if learned is not None and learned.calibration is not None else
                                 "plain order (cost model not predictive on held-out reads)" if learned is not None
                                 else "plain"),
                        "l2": "no flush: index (0.7 GB device layout) + reads (150 MB) + outputs exceed the 126 MB L2",

@@ -2,9 +2,9 @@
 drives (no counterpart in the reference; the reference runs reads in input order).
 
 The exact SMEM kernel logs each read's work (hfm_sched.d_work_log: Occ touches, MemHits,
-positions).  ReadCostModel is a 257 -> 128 -> 128 -> 3 MLP over 4-mer composition and
-length that predicts log1p of those three counters; it is trained on the GPU by the
-library's own forward / backward kernels (hfm_mlp_*).  LearnedSmem bins reads by
+positions).  ReadCostModel is a 258 -> 128 -> 128 -> 3 MLP over 4-mer composition, the
+share of ambiguous 4-mers and length that predicts log1p of those three counters; it is
+trained on the GPU by the library's own forward / backward kernels (hfm_mlp_*).  LearnedSmem bins reads by
 predicted cost (costliest first, warp-uniform runs of similar cost) and sends reads
 predicted to report many MemHits straight to the warp-per-read kernel.  The schedule only
 reorders work: results are byte-identical to the plain path for any model, which is its
@@ -29,6 +29,10 @@ IN_PAD = 272
 def _torch():
     import torch
     return torch
+
+
+def torch_ones_like(t):
+    return _torch().ones_like(t)
 
 
 def work_targets(log) -> "torch.Tensor":
@@ -181,7 +185,8 @@ class LearnedSmem:
     def fit(self, q_d, off_d, nq, min_len, mode, bounds, max_hits, epochs=4, batch=8192, lr=1e-3, seed=0,
             holdout: float = 0.1, calibrate: bool = True):
         """Log the exact kernel's work on the training reads, train on the first
-        (1 - holdout) of them, and judge the model on the rest: the learned order is used
+        (1 - holdout) of them (MSE of standardised targets; per-epoch losses are in those
+        units), and judge the model on the rest: the learned order is used
         only when its predicted Occ touches rank the held-out reads' true touches with
         Spearman >= min_spearman and (calibrate) the learned order runs the held-out reads
         at least 2% faster than the plain order; otherwise run() keeps the plain order."""
@@ -189,8 +194,20 @@ class LearnedSmem:
         t = work_targets(log).to(q_d.device)
         x = self.model.features(q_d, off_d, nq)
         ntr = nq - int(nq * holdout) if nq > 10 else nq
-        self.model.init_output_bias(t[:ntr])
-        losses = self.model.train(x[:ntr].contiguous(), t[:ntr].contiguous(), epochs, batch, lr, seed)
+        # train on standardised targets, then fold the scale into the output layer
+        mu = t[:ntr].mean(dim=0)
+        sd = t[:ntr].std(dim=0).clamp_min(1e-3) if ntr > 1 else torch_ones_like(mu)
+        tz = ((t - mu) / sd).contiguous()
+        p = self.model.get_params()
+        p[NPARAM - 3:] = 0.0
+        self.model.set_params(p)
+        losses = self.model.train(x[:ntr].contiguous(), tz[:ntr].contiguous(), epochs, batch, lr, seed)
+        p = self.model.get_params()
+        sd_h, mu_h = sd.cpu().numpy().astype(np.float32), mu.cpu().numpy().astype(np.float32)
+        w3 = p[NPARAM - 3 - 3 * 128:NPARAM - 3].reshape(3, 128)
+        w3 *= sd_h[:, None]
+        p[NPARAM - 3:] = p[NPARAM - 3:] * sd_h + mu_h
+        self.model.set_params(p)
         if ntr < nq:
             self.holdout_error = prediction_error(self.model.forward(x[ntr:].contiguous()), t[ntr:])
             self.enabled = self.holdout_error.spearman_touches >= self.min_spearman

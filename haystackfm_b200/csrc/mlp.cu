@@ -1,11 +1,12 @@
 // mlp.cu — the learned read-cost model behind the SMEM scheduler (include/hfm.h,
-// hfm_mlp_*): per-read features, a 257 -> 128 -> 128 -> 3 ReLU MLP with its forward and
+// hfm_mlp_*): per-read features, a 258 -> 128 -> 128 -> 3 ReLU MLP with its forward and
 // backward passes on the tensor cores (BF16 operands, FP32 accumulation,
 // mma.sync.m16n8k16), Adam, and the binning of reads by predicted cost.
 //
 // Features of read q (length L): x[f] = 256 * c_f / V - 1 for the 256 4-mers f over ACGT
 // (c_f occurrences, V = 4-mers without an ambiguity code; all 0 when V == 0), x[256] =
-// (log2(L + 1) - 10) / 4, x[257..271] = 0 (padding to the MMA K step).  Outputs predict
+// (log2(L + 1) - 10) / 4, x[257] = (L - 3 - V) / (L - 3), the share of 4-mers holding an
+// ambiguity code (0 when L < 4), x[258..271] = 0 (padding to the MMA K step).  Outputs predict
 // log1p of the exact kernel's per-read work log: Occ touches, MemHits, positions.
 //
 // One CTA owns a tile of 128 reads; each of its 8 warps owns 16 rows and computes all 128
@@ -29,7 +30,7 @@
 namespace hfm {
 namespace mlp {
 
-constexpr int IN = 257, INP = HFM_MLP_IN_PAD, HID = HFM_MLP_HIDDEN, OUT = HFM_MLP_OUT;
+constexpr int IN = 258, INP = HFM_MLP_IN_PAD, HID = HFM_MLP_HIDDEN, OUT = HFM_MLP_OUT;
 constexpr int TILE = 128, THREADS = 256;
 constexpr int XS = 280;   // shared row stride (bf16) of 272-wide tiles: conflict-free fragment loads
 constexpr int HS = 136;   // shared row stride (bf16) of 128-wide tiles
@@ -423,6 +424,7 @@ __global__ void __launch_bounds__(FEAT_WARPS * 32) k_features(const uint8_t* __r
         int c = 2 * k + e;
         if (c < 256) f[e] = valid ? (float)(256u * hw[c]) / (float)valid - 1.f : 0.f;
         else if (c == 256) f[e] = (log2f((float)len + 1.f) - 10.f) * 0.25f;
+        else if (c == 257) f[e] = len >= 4 ? (float)(len - 3 - valid) / (float)(len - 3) : 0.f;
         else f[e] = 0.f;
       }
       reinterpret_cast<uint32_t*>(xr)[k] = pack2(f2bf(f[0]), f2bf(f[1]));

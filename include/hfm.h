@@ -205,13 +205,13 @@ int hfm_mems_batch_device_sched(hfm_index* idx, const uint8_t* d_q, const uint64
                                 uint32_t max_hits, const hfm_sched* sched, hfm_dev_mems* out);
 
 /* ---- learned read-cost model (no counterpart in the reference) -------------
- * A 257 -> 128 -> 128 -> 3 ReLU MLP (BF16 weights and activations, FP32 accumulation)
+ * A 258 -> 128 -> 128 -> 3 ReLU MLP (BF16 weights and activations, FP32 accumulation)
  * predicting, per read, log1p of the exact SMEM kernel's work log (hfm_sched.d_work_log):
  * Occ touches, MemHits, positions.  Input row (HFM_MLP_IN_PAD BF16 values): 256 4-mer
  * frequencies x[f] = 256*c_f/V - 1 (V = 4-mers without an ambiguity code; all 0 when
- * V == 0), x[256] = (log2(len+1) - 10)/4, zeros to the end.  Parameters (FP32, in this
- * order): W1[128][272], b1[128], W2[128][128], b2[128], W3[3][128], b3[3]; W1 columns
- * 257..271 multiply zero inputs.  Training runs the model's own forward and backward CUDA
+ * V == 0), x[256] = (log2(len+1) - 10)/4, x[257] = (len-3-V)/(len-3) (0 when len < 4),
+ * zeros to the end.  Parameters (FP32, in this order): W1[128][272], b1[128],
+ * W2[128][128], b2[128], W3[3][128], b3[3]; W1 columns 258..271 multiply zero inputs.  Training runs the model's own forward and backward CUDA
  * kernels and Adam (lr as given, betas 0.9 / 0.999, eps 1e-8) on the MSE of the outputs.
  * Every call completes its work before returning; device arrays must be 16-byte aligned. */
 #define HFM_MLP_IN_PAD 272

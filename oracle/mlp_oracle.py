@@ -16,7 +16,7 @@ from __future__ import annotations
 
 import numpy as np
 
-IN, INP, HID, OUT = 257, 272, 128, 3
+IN, INP, HID, OUT = 258, 272, 128, 3
 P_W1 = 0
 P_B1 = P_W1 + HID * INP
 P_W2 = P_B1 + HID
@@ -66,6 +66,8 @@ def features(flat: np.ndarray, off: np.ndarray) -> np.ndarray:
         if v:
             x[i, :256] = np.float32(256) * c / np.float32(v) - np.float32(1)
         x[i, 256] = (np.log2(np.float32(L + 1)) - np.float32(10)) * np.float32(0.25)
+        if L >= 4:
+            x[i, 257] = np.float32(L - 3 - v) / np.float32(L - 3)
     return bf16(x)
 
 

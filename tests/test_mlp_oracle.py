@@ -63,6 +63,8 @@ def test_features_direct_count():
         if v:
             want[:256] = np.float32(256) * cnt.astype(np.float32) / np.float32(v) - np.float32(1)
         want[256] = (np.log2(np.float32(len(r) + 1)) - 10) * 0.25
+        if len(r) >= 4:
+            want[257] = np.float32(len(r) - 3 - v) / np.float32(len(r) - 3)
         assert np.array_equal(x[i], M.bf16(want))
     assert (x[:, M.IN:] == 0).all()
 
