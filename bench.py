@@ -567,10 +567,10 @@ def main():
            "d2h_bytes_per_step": int(d2h), "chunk_reads": ch, "handles": args.e2e_streams}
 
     serving = None
-    if not args.no_serving and rank == 0:
+    if not args.no_serving and rank == 0 and world == 1:      # single-GPU measurements
         serving = serving_latency(h, lib, L, kp, rp, bounds, n, args.serving_batches)
     mixed = None
-    if not args.no_mixed and rank == 0:
+    if not args.no_mixed and rank == 0 and world == 1:
         del handles
         mixed = mixed_workload(args, local, torch)
 
