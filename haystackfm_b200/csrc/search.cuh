@@ -527,11 +527,30 @@ __device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf,
 
 // Sort candidates by (qs, qe) (stable), drop duplicates, keep the containment-maximal ones
 // (find_smems, src/fm_index/smem.rs:84-103).  Returns the survivors compacted in place.
+template <bool LONG_LISTS = false>
 __device__ __forceinline__ uint32_t finalize_smems(Cand* c, uint32_t n) {
-  for (uint32_t i = 1; i < n; i++) {           // stable insertion sort
-    Cand t = c[i]; uint32_t j = i;
-    while (j > 0 && (c[j - 1].qs > t.qs || (c[j - 1].qs == t.qs && c[j - 1].qe > t.qe))) { c[j] = c[j - 1]; j--; }
-    c[j] = t;
+  if (LONG_LISTS && n > 128) {
+    // Shell sort (Ciura's gaps) for the long lists of long reads.  Candidates with equal
+    // (qs, qe) name the same pattern, so the same count and interval set: which of them
+    // the dedup below keeps does not matter, and the sort need not be stable.
+    const uint32_t gaps[8] = {701, 301, 132, 57, 23, 10, 4, 1};
+    for (int gi = 0; gi < 8; gi++) {
+      uint32_t g = gaps[gi];
+      if (g >= n) continue;
+      for (uint32_t i = g; i < n; i++) {
+        Cand t = c[i];
+        uint64_t k = ((uint64_t)t.qs << 32) | t.qe;
+        uint32_t j = i;
+        while (j >= g && ((((uint64_t)c[j - g].qs) << 32) | c[j - g].qe) > k) { c[j] = c[j - g]; j -= g; }
+        c[j] = t;
+      }
+    }
+  } else {
+    for (uint32_t i = 1; i < n; i++) {         // insertion sort
+      Cand t = c[i]; uint32_t j = i;
+      while (j > 0 && (c[j - 1].qs > t.qs || (c[j - 1].qs == t.qs && c[j - 1].qe > t.qe))) { c[j] = c[j - 1]; j--; }
+      c[j] = t;
+    }
   }
   uint32_t w = 0;
   for (uint32_t i = 0; i < n; i++)
@@ -944,7 +963,7 @@ __global__ void __launch_bounds__(128, MINB) k_mems_merge(DevFm Fw, DevFm Rv, co
     }
     uint64_t hs = 0; uint32_t hc = 0;
     if (!fail) {
-      uint32_t nc = P.mode == 0 ? finalize_smems(cands, sink.nc) : sink.nc;
+      uint32_t nc = P.mode == 0 ? finalize_smems<true>(cands, sink.nc) : sink.nc;
       if (!write_hits(cands, nc, P, ivpool, hitpool, hs, hc)) st |= ST_POOL_OVF;
     }
     if (st) { hs = 0; hc = 0; }
@@ -1305,7 +1324,7 @@ __global__ void __launch_bounds__(128) k_mems_warp(DevFm Fw, DevFm Rv, const uin
     if (lane == 0) {
       uint64_t hs = 0; uint32_t hc = 0;
       if (nc != ~0u) {
-        if (P.mode == 0) nc = finalize_smems(cands, nc);
+        if (P.mode == 0) nc = finalize_smems<true>(cands, nc);
         if (!write_hits(cands, nc, P, ivpool, hitpool, hs, hc)) st |= ST_POOL_OVF;
       }
       if (st) { hs = 0; hc = 0; }
