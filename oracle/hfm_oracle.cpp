@@ -519,36 +519,42 @@ struct Bidir {
     return ivs;
   }
 
-  // collect_smem_candidates (src/fm_index/smem.rs:154-222)
+  // collect_smem_candidates (src/fm_index/smem.rs:154-222), one pivot of its loop:
+  // appends the pivot's candidates (and, when piv is given, the pivot of each) and returns
+  // the next pivot.
+  size_t pivot_step(const uint8_t* q, size_t n, size_t min_len, size_t pivot, std::vector<RawMem>& out,
+                    std::vector<size_t>* piv) const {
+    std::vector<BIv> curr = multi_right({full()}, q[pivot]);
+    if (curr.empty()) return pivot + 1;
+    uint32_t cov = coverage(curr);
+    std::vector<std::pair<std::vector<BIv>, size_t>> prefixes;
+    size_t j = pivot + 1;
+    for (;;) {
+      if (j == n) { prefixes.push_back({curr, n}); break; }
+      std::vector<BIv> nx = multi_right(curr, q[j]);
+      uint32_t ncov = coverage(nx);
+      if (ncov != cov) prefixes.push_back({curr, j});
+      if (nx.empty()) break;
+      curr.swap(nx); cov = ncov; j++;
+    }
+    size_t reach = prefixes.empty() ? pivot + 1 : prefixes.back().second;
+    for (auto& pr : prefixes) {
+      size_t start;
+      std::vector<BIv> b = left_max(pr.first, q, pivot, start);
+      size_t end = pr.second;
+      if (end - start < min_len) continue;
+      bool rmax = end == n || multi_right(b, q[end]).empty();
+      if (!rmax) continue;
+      out.push_back({(uint32_t)start, (uint32_t)end, coverage(b), std::move(b)});
+      if (piv) piv->push_back(pivot);
+    }
+    return std::max(reach, pivot + 1);
+  }
+
   std::vector<RawMem> smem_candidates(const uint8_t* q, size_t n, size_t min_len) const {
     std::vector<RawMem> out;
     size_t pivot = 0;
-    while (pivot < n) {
-      std::vector<BIv> curr = multi_right({full()}, q[pivot]);
-      if (curr.empty()) { pivot++; continue; }
-      uint32_t cov = coverage(curr);
-      std::vector<std::pair<std::vector<BIv>, size_t>> prefixes;
-      size_t j = pivot + 1;
-      for (;;) {
-        if (j == n) { prefixes.push_back({curr, n}); break; }
-        std::vector<BIv> nx = multi_right(curr, q[j]);
-        uint32_t ncov = coverage(nx);
-        if (ncov != cov) prefixes.push_back({curr, j});
-        if (nx.empty()) break;
-        curr.swap(nx); cov = ncov; j++;
-      }
-      size_t reach = prefixes.empty() ? pivot + 1 : prefixes.back().second;
-      for (auto& pr : prefixes) {
-        size_t start;
-        std::vector<BIv> b = left_max(pr.first, q, pivot, start);
-        size_t end = pr.second;
-        if (end - start < min_len) continue;
-        bool rmax = end == n || multi_right(b, q[end]).empty();
-        if (!rmax) continue;
-        out.push_back({(uint32_t)start, (uint32_t)end, coverage(b), std::move(b)});
-      }
-      pivot = std::max(reach, pivot + 1);
-    }
+    while (pivot < n) pivot = pivot_step(q, n, min_len, pivot, out, nullptr);
     return out;
   }
 
@@ -580,7 +586,9 @@ struct Bidir {
   // find_smems without positions (src/fm_index/smem.rs:71-104)
   std::vector<RawMem> find_smems(const uint8_t* q, size_t n, size_t min_len) const {
     if (n == 0 || min_len == 0) return {};
-    std::vector<RawMem> raws = smem_candidates(q, n, min_len);
+    return filter_smems(smem_candidates(q, n, min_len));
+  }
+  static std::vector<RawMem> filter_smems(std::vector<RawMem> raws) {
     sort_dedup(raws);
     std::vector<RawMem> out;
     for (size_t i = 0; i < raws.size(); i++) {
@@ -955,6 +963,97 @@ int orc_mems_native(void* hv, const uint8_t* q, uint64_t n, uint32_t min_len, ui
     mem.insert(mem.end(), {m.qs, m.qe, m.count, np});
   }
   *mems_out = dup_out(mem); *nmems_out = ms.size(); *pos_out = dup_out(pos); *npos_out = pos.size() / 2;
+  return 0;
+}
+
+// ---- check of the library's segmented SMEM sweep (no counterpart in the reference) ----
+// The library cuts reads longer than 2 * seg_len into seg_len-position segments, sweeps
+// the pivot chain of each segment from its first position, sweeps each segment again from
+// the previous segment's exit pivot until that chain meets the segment's own, and merges
+// along the true chain (haystackfm_b200/csrc/search.cuh, k_mems_seg / k_mems_fix /
+// k_mems_merge).  This restates those three steps on the oracle's own pivot step so that
+// the CPU suite can show the candidate set equals the whole-read sweep's.
+static std::vector<RawMem> segmented_candidates(const Bidir& bd, const uint8_t* q, size_t n, size_t min_len,
+                                                size_t seg) {
+  const size_t NONE = ~(size_t)0;
+  size_t U = (n + seg - 1) / seg;
+  struct Unit {
+    std::vector<char> seen; size_t exit = 0;
+    std::vector<RawMem> c; std::vector<size_t> piv;
+    size_t fx_entry = NONE, fx_conv = NONE, fx_exit = NONE; std::vector<RawMem> fc;
+  };
+  std::vector<Unit> u(U);
+  for (size_t k = 0; k < U; k++) {                 // segment sweeps
+    size_t s = k * seg, e = std::min(n, s + seg);
+    u[k].seen.assign(e - s, 0);
+    size_t p = s;
+    while (p < e) { u[k].seen[p - s] = 1; p = bd.pivot_step(q, n, min_len, p, u[k].c, &u[k].piv); }
+    u[k].exit = p;
+  }
+  for (size_t k = 1; k < U; k++) {                 // fix-up sweeps from the previous exit
+    size_t s = k * seg, e = std::min(n, s + seg), entry = u[k - 1].exit;
+    u[k].fx_entry = entry;
+    if (entry >= e) { u[k].fx_exit = entry; continue; }
+    size_t p = entry;
+    while (p < e && !u[k].seen[p - s]) p = bd.pivot_step(q, n, min_len, p, u[k].fc, nullptr);
+    if (p < e) { u[k].fx_conv = p; u[k].fx_exit = u[k].exit; } else u[k].fx_exit = p;
+  }
+  std::vector<RawMem> out;                          // merge along the true chain
+  size_t t = 0;
+  auto take = [&](const Unit& x, size_t from) {
+    for (size_t i = 0; i < x.c.size(); i++) if (x.piv[i] >= from) out.push_back(x.c[i]);
+  };
+  for (size_t k = 0; k < U; k++) {
+    size_t s = k * seg, e = std::min(n, s + seg);
+    if (t >= e) continue;
+    if (k > 0 && u[k].fx_entry == t) {
+      out.insert(out.end(), u[k].fc.begin(), u[k].fc.end());
+      if (u[k].fx_conv != NONE) { take(u[k], u[k].fx_conv); t = u[k].exit; } else t = u[k].fx_exit;
+      continue;
+    }
+    size_t p = t;
+    while (p < e && !u[k].seen[p - s]) p = bd.pivot_step(q, n, min_len, p, out, nullptr);
+    if (p < e) { take(u[k], p); t = u[k].exit; } else t = p;
+  }
+  return out;
+}
+
+static bool same_mems(std::vector<RawMem> a, std::vector<RawMem> b) {
+  if (a.size() != b.size()) return false;
+  auto by_lo = [](const BIv& x, const BIv& y) { return x.fwd_lo < y.fwd_lo; };
+  for (size_t i = 0; i < a.size(); i++) {
+    if (a[i].qs != b[i].qs || a[i].qe != b[i].qe || a[i].count != b[i].count || a[i].ivs.size() != b[i].ivs.size())
+      return false;
+    std::sort(a[i].ivs.begin(), a[i].ivs.end(), by_lo);
+    std::sort(b[i].ivs.begin(), b[i].ivs.end(), by_lo);
+    for (size_t j = 0; j < a[i].ivs.size(); j++)
+      if (a[i].ivs[j].fwd_lo != b[i].ivs[j].fwd_lo || a[i].ivs[j].fwd_hi != b[i].ivs[j].fwd_hi ||
+          a[i].ivs[j].rev_lo != b[i].ivs[j].rev_lo || a[i].ivs[j].rev_hi != b[i].ivs[j].rev_hi)
+        return false;
+  }
+  return true;
+}
+
+// For each read longer than seg_len: find_smems through the segmented sweep equals the
+// whole-read sweep.  *mismatch = reads that differ, *checked = reads compared.
+int orc_smem_segment_check(void* hv, const uint8_t* q, const uint64_t* off, uint32_t nq, uint32_t min_len,
+                           uint32_t seg_len, uint32_t* mismatch, uint32_t* checked) {
+  Handle* h = (Handle*)hv;
+  if (h->kind != 1) { g_err = "mems need a bidirectional index"; return -4; }
+  if (seg_len == 0 || min_len == 0) { g_err = "seg_len and min_len must be > 0"; return -4; }
+  const Bidir& bd = h->bd;
+  uint32_t bad = 0, n_checked = 0;
+  for (uint32_t r = 0; r < nq; r++) {
+    const uint8_t* qq = q + off[r];
+    size_t n = off[r + 1] - off[r];
+    if (n <= seg_len) continue;
+    n_checked++;
+    auto whole = bd.find_smems(qq, n, min_len);
+    auto segd = Bidir::filter_smems(segmented_candidates(bd, qq, n, min_len, seg_len));
+    if (!same_mems(whole, segd)) bad++;
+  }
+  *mismatch = bad;
+  *checked = n_checked;
   return 0;
 }
 

@@ -57,6 +57,8 @@ def lib():
         L.orc_mems_native.argtypes = [C.c_void_p, u8p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_int,
                                       C.POINTER(u32p), u64p, C.POINTER(u32p), u64p]
         L.orc_extend.argtypes = [C.c_void_p, C.c_int, u32p, C.c_uint8, u32p]
+        L.orc_smem_segment_check.argtypes = [C.c_void_p, u8p, u64p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                             u32p, u32p]
         L.orc_suffix_array.argtypes = [u8p, C.c_uint64, u32p]
         _lib = L
     return _lib
@@ -247,6 +249,17 @@ class OracleIndex:
 
     def find_mems(self, query, min_len: int, locate: bool = False):
         return self.mems_native(query, min_len, 1, locate)
+
+    def smem_segment_check(self, flat: np.ndarray, off: np.ndarray, min_len: int, seg_len: int):
+        """-> (reads whose segmented SMEM sweep differs from the whole-read one, reads checked)."""
+        flat = np.ascontiguousarray(flat if len(flat) else np.zeros(1, np.uint8), dtype=np.uint8)
+        off = np.ascontiguousarray(off, dtype=np.uint64)
+        bad, n = np.zeros(1, np.uint32), np.zeros(1, np.uint32)
+        rc = lib().orc_smem_segment_check(self.h, _p(flat, u8p), _p(off, u64p), len(off) - 1, min_len, seg_len,
+                                          _p(bad, u32p), _p(n, u32p))
+        if rc:
+            raise RuntimeError(lib().orc_last_error().decode())
+        return int(bad[0]), int(n[0])
 
     def extend(self, direction: int, iv, c: int):
         a = np.ascontiguousarray(iv, dtype=np.uint32)
