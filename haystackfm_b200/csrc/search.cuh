@@ -6,10 +6,13 @@
 // ~|read| dependent rank steps, so throughput comes from keeping ~10^5 reads in flight,
 // not from spreading one read over a warp.  Interval sets live in per-thread slices of a
 // global work area, interleaved across the 32 lanes of a warp (element i of every lane is
-// one 512-byte run) with a fixed capacity; a read whose set, candidate list or output
-// outgrows it is queued for a fallback pass with much larger per-thread slices.  There is
-// therefore no cap on interval-set size, as in the reference CPU
-// (src/fm_index/query.rs:248-274, src/fm_index/smem.rs:332-357).
+// one contiguous run: 256 B per u32 plane of the SMEM sets, 256 B per uint2 of the backward
+// search sets) with a fixed capacity; a read whose set, candidate list or output outgrows
+// it is queued for a fallback pass with much larger slices (a per-thread rerun for long
+// candidate lists, then one warp per read).  There is therefore no cap on interval-set
+// size, as in the reference CPU (src/fm_index/query.rs:248-274,
+// src/fm_index/smem.rs:332-357).  SMEM reads longer than 2 * seg_len are swept in
+// segments whose pivot chains are merged (below), so no single read is a long serial chain.
 #pragma once
 #include <type_traits>
 #include "dev_index.cuh"
