@@ -6,7 +6,7 @@
 // ~|read| dependent rank steps, so throughput comes from keeping ~10^5 reads in flight,
 // not from spreading one read over a warp.  Interval sets live in per-thread slices of a
 // global work area, interleaved across the 32 lanes of a warp (element i of every lane is
-// one contiguous run: 256 B per u32 plane of the SMEM sets, 256 B per uint2 of the backward
+// one contiguous run: 128 B per u32 plane of the SMEM sets, 256 B per uint2 of the backward
 // search sets) with a fixed capacity; a read whose set, candidate list or output outgrows
 // it is queued for a fallback pass with much larger slices (a per-thread rerun for long
 // candidate lists, then one warp per read).  There is therefore no cap on interval-set
