@@ -95,3 +95,29 @@ def test_build_rejects_bad_input():
         _build([], FmIndexConfig(), 0, KIND_FM)
     with pytest.raises(Exception):
         _build([al.DnaSequence(np.array([1, 0, 2], np.uint8))], FmIndexConfig(), 0, KIND_FM)
+
+
+def test_null_arguments_rejected_without_a_gpu():
+    """The scheduling, tuning and cost-model entry points reject missing handles and
+    outputs with HFM_E_ARG and a message, before touching a device."""
+    import ctypes as C
+    from haystackfm_b200 import _lib as L
+    lib = L.lib()
+    E_ARG = -4
+    dm = L.HfmDevMems()
+    sc = L.HfmSched(None, 0, 0, None)
+    t = L.HfmTuning(3, 512)
+    assert lib.hfm_mems_batch_device_sched(None, None, None, 0, 19, 0, None, 0, 64, C.byref(sc), C.byref(dm)) == E_ARG
+    assert lib.hfm_get_tuning(None, C.byref(t)) == E_ARG
+    assert lib.hfm_set_tuning(None, C.byref(t)) == E_ARG
+    assert lib.hfm_autotune_mems(None, None, None, 0, 19, 0, None, 0, 64, 1, C.byref(t), None) == E_ARG
+    assert lib.hfm_mlp_create(0, 1, None) == E_ARG
+    assert lib.hfm_mlp_set_params(None, None) == E_ARG
+    assert lib.hfm_mlp_get_params(None, None) == E_ARG
+    assert lib.hfm_mlp_forward(None, None, 0, None) == E_ARG
+    assert lib.hfm_mlp_train(None, None, None, 0, 1, 1, 1e-3, 0, None) == E_ARG
+    nw = C.c_uint32()
+    assert lib.hfm_mlp_schedule(None, None, 0, 0.0, None, C.byref(nw)) == E_ARG
+    assert lib.hfm_last_error()                               # a message was set
+    lib.hfm_mlp_free(None)                                    # no-ops
+    assert lib.hfm_mlp_stream(None) in (None, 0)
