@@ -578,9 +578,11 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, ns, dt = cpu_reference(args, data, reads, bounds, args.cpu_seconds, threads)
+        v1, ns1, dt1 = cpu_reference(args, data, reads, bounds, min(4.0, args.cpu_seconds / 3), 1)
         cpu = {"value": v, "unit": "reads/s", "cores": threads, "kind": "port",
                "sample": f"first {ns} reads of the workload ({dt:.1f} s): locate of the 32-mer + find_smems, "
-                         f"oracle/hfm_oracle.cpp, {threads} threads"}
+                         f"oracle/hfm_oracle.cpp, {threads} threads",
+               "single_core": {"value": v1, "sample": f"first {ns1} reads ({dt1:.1f} s), 1 thread"}}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
