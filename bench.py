@@ -12,10 +12,13 @@ min_len 19 and max_hits_per_mem 1024, positions mapped to the reference boundari
 
 `value` is device-resident throughput (reads in HBM before the timed region, results left
 in HBM); `e2e` goes through the C ABI with host buffers (H2D of the reads from pinned
-memory and D2H of every result inside the timed region).  --impl reference times the
-CPU restatement of the reference path on the host cores (the Rust reference cannot be
-built here).  Multi-GPU: one process per GPU, each with its own index replica and its own
-1M reads (weak scaling, no collective on the data path).
+memory and D2H of every result inside the timed region).  After timing, the outputs of the
+timed calls for the first PARITY_READS reads are compared byte for byte with the CPU
+oracle (`parity` in the line; a mismatch exits non-zero).  --impl reference times the CPU
+restatement of the reference path on the host cores (the Rust reference cannot be built
+here) on an index the oracle builds itself, without loading libhfm.so.  Both arms time the
+same CPU_SAMPLE reads.  Multi-GPU: one process per GPU, each with its own index replica and
+its own 1M reads (weak scaling, no collective on the data path).
 """
 from __future__ import annotations
 
@@ -36,6 +39,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "SMEM+locate reads/s on 1 B200, learned-binned vs plain (bit-exact); p99 latency"
+PARITY_READS = 65_536      # timed outputs of these reads are byte-compared with the oracle
+CPU_SAMPLE = 8_192         # reads both CPU legs time (the reference arm: one pass per step)
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -52,7 +57,6 @@ def parse():
     ap.add_argument("--e2e-chunk", type=int, default=125_000)
     ap.add_argument("--e2e-streams", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="time the plain order only")
     ap.add_argument("--train-reads", type=int, default=1_000_000,
@@ -67,29 +71,55 @@ def parse():
     return ap.parse_args()
 
 
+def bench_config(args, world):
+    """The workload's config dict: identical, key for key, in both arms."""
+    return {"workload": "iupac_batch_locate_smem", "reads_per_step_per_gpu": args.reads, "read_len": 150,
+            "ref_len": args.ref_len, "contigs": args.contigs, "alphabet": "IupacDna", "sa_sample_rate": 32,
+            "lookup_depth": 10, "min_len": 19, "max_hits_per_mem": 1024, "locate_kmer": 32,
+            "seeds": {"reference": 2, "reads": 3}, "parallelism": f"replicas{world}" if world > 1 else "single",
+            "l2": "no flush: index (0.7 GB device layout) + reads (150 MB) + outputs exceed the 126 MB L2"}
+
+
+def iupac_inputs(args, rank=0):
+    """Seeded reference and reads of the workload (numpy only: loads no native library)."""
+    from haystackfm_b200 import synth
+    ref = synth.iupac_reference(total=args.ref_len, n_contigs=args.contigs, seed=2)
+    reads = synth.sample_reads(ref, n_reads=args.reads, seed=3 + rank)
+    return ref, reads
+
+
 def workload(args, rank=0):
-    from haystackfm_b200 import alphabet as al, synth
+    from haystackfm_b200 import alphabet as al
     from haystackfm_b200.fm_index import FmIndexConfig, KIND_BIDIR, _build
     key = hashlib.sha1(f"iupac-v1-{args.ref_len}-{args.contigs}-2-rate32-lut10".encode()).hexdigest()[:16]
     cache_dir = os.path.join(tempfile.gettempdir(), "hfm_bench_cache")
     os.makedirs(cache_dir, exist_ok=True)
     path = os.path.join(cache_dir, key + ".bin")
-    ref = synth.iupac_reference(total=args.ref_len, n_contigs=args.contigs, seed=2)
+    ref, reads = iupac_inputs(args, rank)
     t0 = time.time()
     if os.path.exists(path):
         data = open(path, "rb").read()
         built = False
     else:
         data = _build([al.DnaSequence(c) for c in ref.contigs],
-                      FmIndexConfig(sa_sample_rate=32, lookup_depth=10, build_threads=2), 0, KIND_BIDIR)
+                      FmIndexConfig(sa_sample_rate=32, lookup_depth=10, build_threads=os.cpu_count() or 1), 0,
+                      KIND_BIDIR)
         tmp = path + f".{os.getpid()}"
         with open(tmp, "wb") as f:
             f.write(data)
         os.replace(tmp, path)
         built = True
     build_s = time.time() - t0
-    reads = synth.sample_reads(ref, n_reads=args.reads, seed=3 + rank)
     return ref, data, reads, build_s, built
+
+
+def native_libs_loaded():
+    """Shared objects of this repository mapped into the process (from /proc/self/maps)."""
+    try:
+        maps = open("/proc/self/maps").read()
+    except OSError:
+        return None
+    return sorted({ln.split()[-1] for ln in maps.splitlines() if ln.endswith(".so") and ROOT in ln})
 
 
 class Clocks:
@@ -137,57 +167,123 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def cpu_reference(args, data, reads, bounds, seconds, threads):
-    """Oracle (C++ restatement of the reference CPU path) on a bounded read sample."""
+def cpu_time(o, reads, bounds, threads):
+    """Oracle (C++ restatement of the reference CPU path) over `reads`: locate of the first
+    32-mer (cap 1024) + find_smems (min_len 19, max_hits 1024).  -> (seconds, outputs)."""
     from haystackfm_b200 import synth
-    from oracle import oracle as orc
-    orc.build()
-    o = orc.OracleIndex(data, 1)
-    n = 256
-    while True:
-        sub = reads[:n]
-        t0 = time.perf_counter()
-        f32, o32 = synth.pack_rows(sub, 32)
-        o.locate_packed(f32, o32, 1024, threads)
-        fr, orr = synth.pack_rows(sub)
-        o.mems_packed(fr, orr, 19, 0, bounds, 1024, threads)
-        dt = time.perf_counter() - t0
-        if dt >= seconds * 0.5 or n >= len(reads):
-            return n / dt, n, dt
-        n = min(len(reads), int(n * max(2.0, seconds * 0.6 / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    f32, o32 = synth.pack_rows(reads, 32)
+    loc = o.locate_packed(f32, o32, 1024, threads)
+    fr, orr = synth.pack_rows(reads)
+    mems = o.mems_packed(fr, orr, 19, 0, bounds, 1024, threads)
+    return time.perf_counter() - t0, loc, mems
 
 
 def run_reference(args):
+    """The reference arm: the oracle builds its own index (prefix-doubling suffix sort, no
+    code of libhfm.so) and times CPU_SAMPLE reads per step on every host core."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    _, data, reads, _, _ = workload(args)
-    from haystackfm_b200.fm_index import _header_fields
-    bounds = _header_fields(data, 4)[2]
+    from oracle import oracle as orc
+    orc.build()
     threads = os.cpu_count() or 1
-    per_step = max(2.0, args.cpu_seconds / max(1, args.steps))
+    ref, reads = iupac_inputs(args)
+    t0 = time.time()
+    orc.set_build_threads(threads)
+    data = orc.build_index_bytes(ref.contigs, rate=32, lookup_depth=10, tag=0, kind=1)
+    build_s = time.time() - t0
+    o = orc.OracleIndex(data, 1)
+    bounds = _bounds_of(data)
+    sample = reads[:CPU_SAMPLE]
     for _ in range(args.warmup):
-        cpu_reference(args, data, reads, bounds, per_step / 4, threads)
-    vals = []
+        cpu_time(o, sample[:max(256, CPU_SAMPLE // 8)], bounds, threads)
+    tot_t = 0.0
     for _ in range(args.steps):
-        v, n, dt = cpu_reference(args, data, reads, bounds, per_step, threads)
-        vals.append((v, n, dt))
-    tot_n = sum(x[1] for x in vals)
-    tot_t = sum(x[2] for x in vals)
-    value = tot_n / tot_t
+        dt, _, _ = cpu_time(o, sample, bounds, threads)
+        tot_t += dt
+    value = len(sample) * args.steps / tot_t
+    libs = native_libs_loaded()
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * tot_t / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
-        "config": {"workload": "iupac_batch_locate_smem", "reads_per_step": args.reads, "read_len": 150,
-                   "ref_len": args.ref_len, "contigs": args.contigs, "sa_sample_rate": 32, "lookup_depth": 10,
-                   "min_len": 19, "max_hits_per_mem": 1024, "locate_kmer": 32, "path": "cpu_reference"},
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic (seeded generators, haystackfm_b200/synth.py)",
+        "config": bench_config(args, world),
         "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads, "kind": "port",
-                         "sample": f"{vals[-1][1]} reads of the 1M-read workload per step, oracle/hfm_oracle.cpp "
-                                   f"(Rust reference not buildable here), {threads} threads"},
+                         "sample": f"the first {len(sample)} reads of the workload each step (locate of the 32-mer "
+                                   f"+ find_smems), oracle/hfm_oracle.cpp (the Rust reference cannot be built "
+                                   f"here), {threads} threads"},
         "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "index": {"builder": "oracle (prefix-doubling suffix sort)", "build_s": round(build_s, 1),
+                  "sha256": hashlib.sha256(data).hexdigest()},
+        "native_libs": libs,
     }
+    if libs and any("libhfm" in x for x in libs):
+        raise SystemExit("reference arm loaded libhfm.so")
     print(json.dumps(line), flush=True)
+
+
+def _bounds_of(data):
+    """seq_boundaries of the forward index inside BidirFmIndex bincode (struct only)."""
+    import struct
+    o = 4 + 64 + 2 + 32
+    (n,) = struct.unpack_from("<Q", data, o); o += 8 + 4 * n
+    (n,) = struct.unpack_from("<Q", data, o); o += 8 + n
+    o += 16
+    (n,) = struct.unpack_from("<Q", data, o); o += 8 + n
+    (n,) = struct.unpack_from("<Q", data, o); o += 8 + 4 * n
+    o += 16
+    (n,) = struct.unpack_from("<Q", data, o); o += 8
+    return np.frombuffer(data, dtype="<u4", count=n, offset=o).copy()
+
+
+def gpu_prefix_outputs(h, lib, L, dev, k32_d, off32_d, reads_d, off_d, n, bounds, npre):
+    """Runs the timed step's two calls once more and copies the outputs of the first `npre`
+    reads (a prefix of each CSR) to the host, in the oracle's array format."""
+    from haystackfm_b200.fm_index import device_to_host as d2h
+    nb = len(bounds)
+    dh = L.HfmDevHits()
+    L.check(lib.hfm_locate_batch_device(h.h, k32_d.data_ptr(), off32_d.data_ptr(), n, 1024, C.byref(dh)))
+    offs = d2h(dh.d_offsets, npre + 1, "<i8", dev).view(np.uint64)
+    counts = d2h(dh.d_counts, npre, "<i4", dev).view(np.uint32)
+    pairs = d2h(dh.d_pairs, 2 * int(offs[-1]), "<i4", dev).view(np.uint32).reshape(-1, 2)
+    dm = L.HfmDevMems()
+    L.check(lib.hfm_mems_batch_device(h.h, reads_d.data_ptr(), off_d.data_ptr(), n, 19, 0, L.ptr(bounds, L.u32p),
+                                      nb, 1024, C.byref(dm)))
+    hoff = d2h(dm.d_hit_offsets, npre + 1, "<i8", dev).view(np.uint64)
+    hits = d2h(dm.d_hits, 8 * int(hoff[-1]), "<i4", dev).view(np.uint32).reshape(-1, 8)
+    npos = 0
+    if len(hits):
+        last = hits[-1]
+        npos = (int(last[6]) | (int(last[7]) << 32)) + int(last[5])
+    pos = d2h(dm.d_positions, 2 * npos, "<i4", dev).view(np.uint32).reshape(-1, 2)
+    return (counts, offs, pairs), (hoff, hits, pos)
+
+
+def device_mems_tensors(torch, dev, dm, n, clone):
+    """hfm_dev_mems outputs as torch views (or copies) of the library's device arrays."""
+    from haystackfm_b200.fm_index import _DeviceArray
+
+    def view(ptr, k, ts):
+        if k == 0:
+            return torch.zeros(0, dtype=torch.int32, device=dev)
+        t = torch.as_tensor(_DeviceArray(int(ptr), int(k), ts), device=dev)
+        return t.clone() if clone else t
+    return (view(dm.d_hit_offsets, n + 1, "<i8"), view(dm.d_hits, 8 * dm.n_hits, "<i4"),
+            view(dm.d_positions, 2 * dm.n_positions, "<i4"))
+
+
+def compare_outputs(got, want):
+    """Byte comparison of (locate, mems) output tuples; -> list of differing arrays."""
+    names = [("locate", ("counts", "offsets", "pairs")), ("mems", ("hit_offsets", "hits", "positions"))]
+    bad = []
+    for (grp, fields), g, w in zip(names, got, want):
+        for f, a, b in zip(fields, g, w):
+            if a.shape != b.shape or not np.array_equal(a, b):
+                bad.append(f"{grp}.{f}")
+    return bad
 
 
 def profile_smem(args):
@@ -460,6 +556,19 @@ def main():
             pms = float(t.item())
         plain_info = {"value": world * n * args.steps / (pms / 1000.0), "ms_per_step": pms / args.steps}
         learned_info["speedup_vs_plain"] = round(plain_info["ms_per_step"] / (ms / args.steps), 4)
+    # learned order vs plain order on the whole batch: every output array byte for byte
+    learned_parity = None
+    if learned is not None:
+        dm_p = L.HfmDevMems()
+        L.check(lib.hfm_mems_batch_device(h.h, reads_d.data_ptr(), off_d.data_ptr(), n, 19, 0, L.ptr(bounds, L.u32p),
+                                          nb, 1024, C.byref(dm_p)))
+        snap = device_mems_tensors(torch, dev, dm_p, n, clone=True)
+        dm_l = learned.run(reads_d, off_d, n, 19, 0, L.ptr(bounds, L.u32p), nb, 1024)
+        now = device_mems_tensors(torch, dev, dm_l, n, clone=False)
+        eq = all(a.shape == b.shape and bool(torch.equal(a, b)) for a, b in zip(snap, now))
+        learned_parity = {"reads_checked": n, "equal": eq, "mem_hits": int(dm_l.n_hits),
+                          "mem_positions": int(dm_l.n_positions)}
+        del snap, now
     # kernel times (CUDA events around each launch, recorded by the library on its stream)
     k_mems_ms = statistics.mean(s2.ms_search_kernel for _, s2, *_ in per)
     k_res_mem_ms = statistics.mean(s2.ms_resolve_kernel for _, s2, *_ in per)
@@ -574,33 +683,53 @@ def main():
         del handles
         mixed = mixed_workload(args, local, torch)
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    # CPU baseline (the same CPU_SAMPLE reads the reference arm times) and parity: the timed
+    # calls' outputs for the first PARITY_READS reads, byte for byte against the oracle
+    cpu, parity = None, None
+    if rank == 0 and not args.no_cpu_baseline:
+        from oracle import oracle as orc
+        orc.build()
+        o = orc.OracleIndex(data, 1)
         threads = os.cpu_count() or 1
-        v, ns, dt = cpu_reference(args, data, reads, bounds, args.cpu_seconds, threads)
-        v1, ns1, dt1 = cpu_reference(args, data, reads, bounds, min(4.0, args.cpu_seconds / 3), 1)
-        cpu = {"value": v, "unit": "reads/s", "cores": threads, "kind": "port",
-               "sample": f"first {ns} reads of the workload ({dt:.1f} s): locate of the 32-mer + find_smems, "
-                         f"oracle/hfm_oracle.cpp, {threads} threads",
-               "single_core": {"value": v1, "sample": f"first {ns1} reads ({dt1:.1f} s), 1 thread"}}
+        dt, _, _ = cpu_time(o, reads[:CPU_SAMPLE], bounds, threads)
+        dt1, _, _ = cpu_time(o, reads[:1024], bounds, 1)
+        cpu = {"value": CPU_SAMPLE / dt, "unit": "reads/s", "cores": threads, "kind": "port",
+               "sample": f"the first {CPU_SAMPLE} reads of the workload ({dt:.1f} s): locate of the 32-mer + "
+                         f"find_smems, oracle/hfm_oracle.cpp, {threads} threads (the reference arm times the same "
+                         f"reads)",
+               "single_core": {"value": 1024 / dt1, "sample": f"the first 1024 reads ({dt1:.1f} s), 1 thread"}}
+        npre = min(PARITY_READS, n)
+        t0 = time.perf_counter()
+        got = gpu_prefix_outputs(h, lib, L, dev, k32_d, off32_d, reads_d, off_d, n, bounds, npre)
+        _, wloc, wmem = cpu_time(o, reads[:npre], bounds, threads)
+        bad = compare_outputs(got, (wloc, wmem))
+        parity = {"reads_checked": npre, "equal": not bad, "mismatched": bad,
+                  "locate_positions": int(len(wloc[2])), "mem_hits": int(len(wmem[1])),
+                  "mem_positions": int(len(wmem[2])), "oracle_s": round(time.perf_counter() - t0, 1),
+                  "what": "outputs of the timed device calls (locate CSR, MemHit CSR, positions) for the first "
+                          f"{npre} reads vs oracle/hfm_oracle.cpp on the same index bytes"}
+        del o
+    if learned is not None and learned_parity is not None:
+        if parity is None:
+            parity = {}
+        parity["learned_vs_plain"] = learned_parity
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generators, haystackfm_b200/synth.py)",
-            "config": {"workload": "iupac_batch_locate_smem", "reads_per_step_per_gpu": n, "read_len": 150,
-                       "ref_len": args.ref_len, "contigs": args.contigs, "sa_sample_rate": 32, "lookup_depth": 10,
-                       "min_len": 19, "max_hits_per_mem": 1024, "locate_kmer": 32,
-                       "path": ("learned-binned" if learned is not None and learned.enabled else
-                                "plain order (learned order not faster on held-out reads)"
-                                if learned is not None and learned.calibration is not None else
-                                "plain order (cost model not predictive on held-out reads)" if learned is not None
-                                else "plain"),
-                       "l2": "no flush: index (0.7 GB device layout) + reads (150 MB) + outputs exceed the 126 MB L2",
-                       "index_build_s": round(build_s, 1), "index_cached": not built,
-                       "locate_positions": int(loc_total), "mem_hits": int(n_hits), "mem_positions": int(n_pos),
-                       "distinct_rows_walked": int(rows_walked(c_mem) + rows_walked(c_loc)),
-                       "parallelism": f"replicas{world}" if world > 1 else "single", "autotuned": tuning_main},
+            "config": bench_config(args, world),
+            "run": {"path": ("learned-binned" if learned is not None and learned.enabled else
+                             "plain order (learned order not faster on held-out reads)"
+                             if learned is not None and learned.calibration is not None else
+                             "plain order (cost model not predictive on held-out reads)" if learned is not None
+                             else "plain"),
+                    "index_build_s": round(build_s, 1), "index_cached": not built,
+                    "index_sha256": hashlib.sha256(data).hexdigest(),
+                    "locate_positions": int(loc_total), "mem_hits": int(n_hits), "mem_positions": int(n_pos),
+                    "distinct_rows_walked": int(rows_walked(c_mem) + rows_walked(c_loc)),
+                    "autotuned": tuning_main},
+            "parity": parity,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "plain": plain_info, "learned": learned_info, "serving": serving, "mixed": mixed,
             "clocks": clk,
@@ -609,6 +738,9 @@ def main():
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+    if parity and (not parity.get("equal", True) or
+                   (parity.get("learned_vs_plain") and not parity["learned_vs_plain"]["equal"])):
+        raise SystemExit("parity mismatch: " + json.dumps(parity))
 
 
 if __name__ == "__main__":

@@ -86,6 +86,8 @@ class HfmBuildOpts(C.Structure):
 SIGNATURES = {
     "hfm_build_index": (C.c_int, [u8p, u64p, C.c_uint32, C.POINTER(C.c_char_p), C.POINTER(HfmBuildOpts), C.c_int,
                                   C.POINTER(u8p), C.POINTER(C.c_size_t)]),
+    "hfm_build_index_gpu": (C.c_int, [u8p, u64p, C.c_uint32, C.POINTER(C.c_char_p), C.POINTER(HfmBuildOpts),
+                                      C.c_int, C.c_int, C.POINTER(u8p), C.POINTER(C.c_size_t)]),
     "hfm_index_load": (C.c_int, [u8p, C.c_size_t, C.c_int, C.POINTER(HfmOpts), C.POINTER(C.c_void_p)]),
     "hfm_index_free": (None, [C.c_void_p]),
     "hfm_index_info_get": (C.c_int, [C.c_void_p, C.POINTER(HfmIndexInfo)]),
@@ -126,6 +128,7 @@ SIGNATURES = {
     "hfm_index_stream": (C.c_void_p, [C.c_void_p]),
     "hfm_last_stats": (C.c_int, [C.c_void_p, C.POINTER(HfmStats)]),
     "hfm_set_counters": (C.c_int, [C.c_void_p, C.c_int]),
+    "hfm_set_timeout": (C.c_int, [C.c_void_p, C.c_uint32]),
 }
 
 _lib = None

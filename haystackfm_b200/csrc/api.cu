@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -18,6 +19,7 @@
 #include <mutex>
 #include <unordered_map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "dev_index.cuh"
@@ -43,6 +45,14 @@ int set_error(int status, const std::string& msg) {
   } while (0)
 
 #define RET(x) do { int _r = (x); if (_r != HFM_OK) return _r; } while (0)
+
+// Runs the statement block with FM bound to the index's Occ record format as a
+// compile-time constant (the SMEM kernels are specialised per format).
+#define WITH_FMT(fmt, ...)                                                                        \
+  do {                                                                                            \
+    if ((fmt) == OCC_NARROW) { constexpr uint32_t FM = OCC_NARROW; __VA_ARGS__ }                   \
+    else { constexpr uint32_t FM = OCC_WIDE; __VA_ARGS__ }                                        \
+  } while (0)
 
 // compatible_symbols / ExactDna::compatible (src/alphabet.rs:174-193,286-294) as bit masks
 static void compat_masks(uint32_t tag, uint16_t out[16]) {
@@ -91,10 +101,10 @@ struct Counters {                    // device-side counters, one block per hand
 
 struct FmDev {
   DevFm d{};
-  DevBuf occ, ssa, sa_vals, lut, bounds, compat;
-  uint32_t text_len = 0, num_seqs = 0, lookup_depth = 0, tag = 0, num_lanes = 0, encoding = 0, rate = 0;
+  DevBuf occ, sb, ssa, sa_vals, lut, bounds, compat;
+  uint32_t text_len = 0, num_seqs = 0, lookup_depth = 0, tag = 0, num_lanes = 0, encoding = 0, rate = 0, fmt = 0;
   std::vector<uint32_t> seq_boundaries;
-  size_t bytes() const { return occ.cap + ssa.cap + sa_vals.cap + lut.cap + bounds.cap + compat.cap; }
+  size_t bytes() const { return occ.cap + sb.cap + ssa.cap + sa_vals.cap + lut.cap + bounds.cap + compat.cap; }
 };
 
 }  // namespace hfm
@@ -112,15 +122,18 @@ struct hfm_index {
       scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr,
       mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout, blockmap, blockmap2, ovf2, ovf3,
       lflag, lpos, sids, lids, ucount, ubase, uread, uk, ubits, uexit, ust, ucoff, ucnt, segpool, fxe, fxc, fxx,
-      fxo, fxn;
+      fxo, fxn, npos;
   uint32_t flags = 0;
   uint32_t seg_len = 512;  // SMEM reads longer than 2 * seg_len take the segmented sweep
-  int mems_variant = 3;   // SMEM fast-kernel variant (see mems_device): 0/1/2 local 32-entry
-                          // candidate lists at 5/6/8 blocks per SM; 3 global 1024-entry lists
+  int mems_variant = 3;   // SMEM fast-kernel variant (see mems_device): 2 local 32-entry
+                          // candidate lists; 3 global 1024-entry lists
   int num_sms = 0;
   uint64_t iv_cap = 0, miv_cap = 0, hit_cap = 0;   // pool capacities in elements (uint2 / BIv / hit)
   uint64_t seg_cap = 0;                            // segment candidate pool capacity (Cand)
   Counters* h_ctr = nullptr;        // pinned
+  uint32_t timeout_ms = 0;          // host-side deadline of every wait on the stream (0: none)
+  std::vector<void*> orphans;       // result blocks of calls that timed out (freed once the stream drains)
+  cudaEvent_t ev_wait = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t evk[4] = {nullptr, nullptr, nullptr, nullptr};   // main search kernel, resolve kernel
   bool k_search_rec = false, k_resolve_rec = false;
@@ -141,15 +154,27 @@ static int upload(DevBuf& b, const void* src, size_t bytes, cudaStream_t s) {
 static int build_device_fm(const HostFm& h, FmDev& f, cudaStream_t s) {
   const uint32_t n = h.text_len, L = h.num_lanes;
   const uint64_t nblk = ((uint64_t)n + 63) / 64;
-  std::vector<uint32_t> occ(nblk * 24, 0);
+  const uint64_t nsb = (nblk + (1u << SB_BLOCK_SHIFT) - 1) >> SB_BLOCK_SHIFT;
+  // symbols absent from the lane map are absent from the text
+  uint16_t sym_mask = 0;
+  for (int sy = 0; sy < 16; sy++) if (h.s2l[sy] != 0xFF) sym_mask |= (uint16_t)(1u << sy);
+  const bool narrow = (sym_mask & ~0x1Fu) == 0;       // codes 0..4 only
+  const uint32_t fmt = narrow ? OCC_NARROW : OCC_WIDE;
+  const uint64_t rec_u32 = narrow ? OCC_NARROW_U4 * 4 : OCC_WIDE_U4 * 4;
+  std::vector<uint32_t> occ(nblk * rec_u32, 0);
+  std::vector<uint32_t> sb(nsb * 16, 0);
   std::vector<uint32_t> ssa(nblk * 4, 0);
   const uint64_t width = h.encoding == 0 ? h.num_planes : L;
-  for (uint64_t b = 0; b < nblk; b++) {
+  // Decode the reference records (compacted lanes, u32 superblock count + u16 delta per
+  // lane) into whole per-symbol counts and 4 symbol-code bitplanes, then re-encode them as
+  // the device records.  Superblocks of the device layout are 1024 records, so every
+  // count within one fits a u16.
+  auto decode = [&](uint64_t b, uint32_t cnt[16], uint64_t planes[4]) {
     const uint8_t* r = h.block_data + b * h.block_stride;
-    uint32_t cnt[16] = {0};
     uint64_t words[16] = {0};
     for (uint64_t w = 0; w < width; w++) std::memcpy(&words[w], r + L * 6 + w * 8, 8);
-    uint64_t planes[4] = {0, 0, 0, 0};
+    for (int c = 0; c < 16; c++) cnt[c] = 0;
+    for (int p = 0; p < 4; p++) planes[p] = 0;
     for (uint32_t l = 0; l < L; l++) {
       uint32_t sbv; uint16_t dv;
       std::memcpy(&sbv, r + l * 4, 4); std::memcpy(&dv, r + L * 4 + l * 2, 2);
@@ -162,19 +187,54 @@ static int build_device_fm(const HostFm& h, FmDev& f, cudaStream_t s) {
       if (b == nblk - 1 && (n & 63)) m &= (1ull << (n & 63)) - 1;   // rows past the text
       for (int p = 0; p < 4; p++) if ((sym >> p) & 1) planes[p] |= m;
     }
-    std::memcpy(&occ[b * 24], cnt, 64);
-    std::memcpy(&occ[b * 24 + 16], planes, 32);
-    // sampled-SA record: bits + rank before (validated equal to the stored sb + delta)
-    uint64_t word; uint32_t sb; uint16_t d;
-    std::memcpy(&word, h.ssa_words + b * 14, 8); std::memcpy(&sb, h.ssa_words + b * 14 + 8, 4);
-    std::memcpy(&d, h.ssa_words + b * 14 + 12, 2);
-    if (b == nblk - 1 && (n & 63)) word &= (1ull << (n & 63)) - 1;
-    ssa[b * 4 + 0] = (uint32_t)word; ssa[b * 4 + 1] = (uint32_t)(word >> 32); ssa[b * 4 + 2] = sb + d;
+  };
+  auto fill = [&](uint64_t b0, uint64_t b1) {
+    uint32_t cnt[16], base[16];
+    uint64_t planes[4];
+    for (uint64_t b = b0; b < b1; b++) {
+      decode(b, cnt, planes);
+      const uint64_t sbi = b >> SB_BLOCK_SHIFT;
+      if ((b & ((1u << SB_BLOCK_SHIFT) - 1)) == 0 || b == b0) {
+        if ((b & ((1u << SB_BLOCK_SHIFT) - 1)) == 0) {
+          std::memcpy(base, cnt, 64);
+          std::memcpy(&sb[sbi * 16], cnt, 64);
+        } else {                                        // a thread's range starts inside a superblock
+          uint32_t c0[16]; uint64_t p0[4];
+          decode(sbi << SB_BLOCK_SHIFT, c0, p0);
+          std::memcpy(base, c0, 64);
+        }
+      }
+      uint32_t* rec = &occ[b * rec_u32];
+      uint32_t d[16];
+      for (int c = 0; c < 16; c++) d[c] = cnt[c] - base[c];
+      if (narrow) {
+        rec[0] = d[1] | (d[2] << 16); rec[1] = d[3] | (d[4] << 16);
+        std::memcpy(rec + 2, &planes[0], 8); std::memcpy(rec + 4, &planes[1], 8); std::memcpy(rec + 6, &planes[2], 8);
+      } else {
+        for (int c = 0; c < 16; c += 2) rec[c / 2] = d[c] | (d[c + 1] << 16);
+        std::memcpy(rec + 8, planes, 32);
+      }
+      // sampled-SA record: bits + rank before (validated equal to the stored sb + delta)
+      uint64_t word; uint32_t sbs; uint16_t dd;
+      std::memcpy(&word, h.ssa_words + b * 14, 8); std::memcpy(&sbs, h.ssa_words + b * 14 + 8, 4);
+      std::memcpy(&dd, h.ssa_words + b * 14 + 12, 2);
+      if (b == nblk - 1 && (n & 63)) word &= (1ull << (n & 63)) - 1;
+      ssa[b * 4 + 0] = (uint32_t)word; ssa[b * 4 + 1] = (uint32_t)(word >> 32); ssa[b * 4 + 2] = sbs + dd;
+    }
+  };
+  {
+    unsigned nt = std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    if (nblk < (1u << 16)) nt = 1;
+    std::vector<std::thread> th;
+    const uint64_t per = (nblk + nt - 1) / nt;
+    for (unsigned t = 0; t < nt; t++) {
+      uint64_t b0 = t * per, b1 = std::min<uint64_t>(nblk, b0 + per);
+      if (b0 < b1) th.emplace_back(fill, b0, b1);
+    }
+    for (auto& x : th) x.join();
   }
-  // symbols absent from the lane map are absent from the text
-  uint16_t sym_mask = 0;
-  for (int sy = 0; sy < 16; sy++) if (h.s2l[sy] != 0xFF) sym_mask |= (uint16_t)(1u << sy);
   RET(upload(f.occ, occ.data(), occ.size() * 4, s));
+  RET(upload(f.sb, sb.data(), sb.size() * 4, s));
   RET(upload(f.ssa, ssa.data(), ssa.size() * 4, s));
   RET(upload(f.sa_vals, h.sa_vals, h.n_sa_vals * 4, s));
   RET(upload(f.bounds, h.seq_boundaries.data(), h.seq_boundaries.size() * 4, s));
@@ -184,18 +244,19 @@ static int build_device_fm(const HostFm& h, FmDev& f, cudaStream_t s) {
   RET(upload(f.compat, cm, sizeof(cm), s));
   CK(cudaStreamSynchronize(s));      // host vectors die at return
   DevFm& d = f.d;
-  d.occ = f.occ.as<uint4>(); d.ssa = f.ssa.as<uint4>();
+  d.occ = f.occ.as<uint4>(); d.sb = f.sb.as<uint32_t>(); d.ssa = f.ssa.as<uint4>();
   d.sa_vals = f.sa_vals.as<uint32_t>(); d.seq_bounds = f.bounds.as<uint32_t>();
   d.lut = h.has_lookup ? f.lut.as<uint2>() : nullptr;
   d.text_len = n; d.num_seqs = (uint32_t)h.seq_boundaries.size(); d.sample_rate = h.sample_rate;
   d.lut_depth = h.has_lookup ? h.lookup_depth : 0; d.tag = h.tag;
-  d.lut_radix = (uint32_t)h.lookup_core.size(); d.num_blocks = (uint32_t)nblk;
+  d.lut_radix = (uint32_t)h.lookup_core.size(); d.num_blocks = (uint32_t)nblk; d.fmt = fmt;
   std::memcpy(d.C, h.C, 64); std::memcpy(d.s2l, h.s2l, 16); std::memcpy(d.l2s, h.l2s, 16);
   std::memset(d.lut_digit, 0xFF, 16);
   for (size_t k = h.lookup_core.size(); k-- > 0;) if (h.lookup_core[k] < 16) d.lut_digit[h.lookup_core[k]] = (uint8_t)k;
   d.sym_mask = sym_mask;
   f.text_len = n; f.num_seqs = h.num_sequences; f.lookup_depth = d.lut_depth; f.tag = h.tag;
   f.num_lanes = L; f.encoding = h.encoding; f.rate = h.sample_rate; f.seq_boundaries = h.seq_boundaries;
+  f.fmt = fmt;
   return HFM_OK;
 }
 
@@ -216,17 +277,39 @@ static int scan(hfm_index* x, const T* in, uint32_t stride, uint64_t n, uint64_t
   return HFM_OK;
 }
 
+// Waits until `ev` has completed.  Without a deadline this is cudaEventSynchronize; with
+// one (hfm_set_timeout) the host polls the event and gives up with HFM_E_TIMEOUT once the
+// deadline has passed.  The abandoned work stays queued on the handle's stream: the next
+// call on the handle runs after it, so the handle remains usable.
+static int wait_event(hfm_index* x, cudaEvent_t ev) {
+  if (!x->timeout_ms) { CK(cudaEventSynchronize(ev)); return HFM_OK; }
+  const auto t0 = std::chrono::steady_clock::now();
+  const auto limit = std::chrono::milliseconds(x->timeout_ms);
+  for (;;) {
+    cudaError_t e = cudaEventQuery(ev);
+    if (e == cudaSuccess) return HFM_OK;
+    if (e != cudaErrorNotReady) CK(e);
+    if (std::chrono::steady_clock::now() - t0 >= limit)
+      return set_error(HFM_E_TIMEOUT, "device work did not finish within " + std::to_string(x->timeout_ms) + " ms");
+    std::this_thread::yield();
+  }
+}
+
+static int wait_stream(hfm_index* x) {
+  CK(cudaEventRecord(x->ev_wait, x->stream));
+  return wait_event(x, x->ev_wait);
+}
+
 static int read_ctr(hfm_index* x) {
   CK(cudaMemcpyAsync(x->h_ctr, x->ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, x->stream));
-  CK(cudaStreamSynchronize(x->stream));
-  return HFM_OK;
+  return wait_stream(x);
 }
 
 static Counters* dctr(hfm_index* x) { return x->ctr.as<Counters>(); }
 
 static int read_u64(hfm_index* x, const uint64_t* dsrc, uint64_t& v) {
   CK(cudaMemcpyAsync(&x->h_ctr->steps, dsrc, 8, cudaMemcpyDeviceToHost, x->stream));
-  CK(cudaStreamSynchronize(x->stream));
+  RET(wait_stream(x));
   v = x->h_ctr->steps;
   return HFM_OK;
 }
@@ -239,6 +322,7 @@ static constexpr int MEM_KC = 32;              // fast-path candidate capacity (
 static constexpr uint32_t MID_CAND_CAP = 1024;  // candidate list of the per-thread rerun (global memory)
 static constexpr uint32_t MID_THREADS_PER_SM = 256;
 static constexpr uint32_t FAST_CAND_CAP = 1024;  // global candidate list of fast-pass variant 3
+static constexpr int MEMS_PLAIN = 4;             // mems_variant of the plain one-thread-per-read launch
 
 // Backward search for a batch.  with_ivs = false: counts only.
 static int run_bsearch(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t cap,
@@ -395,9 +479,9 @@ static void begin_stats(hfm_index* x) {
   x->k_search_rec = x->k_resolve_rec = false;
   cudaEventRecord(x->ev[0], x->stream);
 }
-static void end_stats(hfm_index* x) {
+static int end_stats(hfm_index* x) {
   cudaEventRecord(x->ev[2], x->stream);
-  cudaEventSynchronize(x->ev[2]);
+  RET(wait_event(x, x->ev[2]));
   float a = 0, b = 0;
   cudaEventElapsedTime(&a, x->ev[0], x->ev[1]);
   cudaEventElapsedTime(&b, x->ev[1], x->ev[2]);
@@ -406,6 +490,7 @@ static void end_stats(hfm_index* x) {
   if (x->k_search_rec) cudaEventElapsedTime(&ks, x->evk[0], x->evk[1]);
   if (x->k_resolve_rec) cudaEventElapsedTime(&kr, x->evk[2], x->evk[3]);
   x->stats.ms_search_kernel = ks; x->stats.ms_resolve_kernel = kr;
+  return HFM_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -416,7 +501,7 @@ static int count_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff
   uint32_t launches = 0;
   RET(run_bsearch(x, d_q, d_qoff, nq, 0, false, d_counts, launches));
   cudaEventRecord(x->ev[1], x->stream);
-  end_stats(x);
+  RET(end_stats(x));
   x->stats.search_launches = launches;
   return HFM_OK;
 }
@@ -451,7 +536,7 @@ static int locate_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qof
   RET(resolve_segments(x, x->fwd, x->seg_row.as<uint32_t>(), 1, x->seg_off.as<uint64_t>(), nseg, total,
               x->fwd.bounds.as<uint32_t>(), (uint32_t)x->fwd.seq_boundaries.size(), x->out_pairs.as<uint32_t>(), rl, other));
   RET(read_ctr(x));
-  end_stats(x);
+  RET(end_stats(x));
   x->stats.search_launches = launches; x->stats.resolve_launches = rl; x->stats.other_launches = other;
   x->stats.rows_resolved = total; x->stats.lf_calls = x->h_ctr->steps;
   if (x->h_ctr->walk_err) return set_error(HFM_E_WALK, "LF walk exceeded sample_rate steps: index inconsistent");
@@ -494,15 +579,17 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   MemsParams P{min_len, mode, cap, nb ? 1u : 0u};
   const FmDev& Fw = x->fwd; const FmDev& Rv = x->rev;
   // persistent fast pass: one wave of resident threads, MEM_SET_CAP intervals per set.
-  // Variants 0-2: 5, 6 or 8 resident blocks of 128 threads per SM with a 32-entry
-  // candidate list in local memory; variant 3 (default): 8 blocks per SM with a 1024-entry
-  // list per thread in global memory, so reads up to ~10 kbp finish in this pass.
+  // Variant 2: 8 resident blocks of 128 threads per SM with a 32-entry candidate list in
+  // local memory; variant 3 (default): 8 blocks per SM with a 1024-entry list per thread
+  // in global memory, so reads up to ~10 kbp finish in this pass.  The kernels are
+  // specialised for the index's Occ record format (narrow or wide).
   int variant = x->mems_variant;
   int bpsm = 0;
-  if (variant == 0) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC, 5>, 128, 0));
-  else if (variant == 1) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC, 6>, 128, 0));
-  else if (variant == 3) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, 0, 8>, 128, 0));
-  else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC, 8>, 128, 0));
+  const uint32_t fmt = Fw.fmt;
+  WITH_FMT(fmt, {
+    if (variant == 3) CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, 0, 8, FM>, 128, 0));
+    else CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, MEM_KC, 8, FM>, 128, 0));
+  });
   const uint64_t full_threads = (uint64_t)std::max(1, bpsm) * x->num_sms * 128;
   uint64_t threads = std::min<uint64_t>(full_threads, ((uint64_t)nq + 127) / 128 * 128);
   // Long reads (SMEM mode with global candidate lists) take the segmented sweep: the
@@ -549,10 +636,44 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       threads = std::max<uint64_t>(threads, std::min<uint64_t>(full_threads, (n_units + 127) / 128 * 128));
     }
   }
-  RET(x->memwork.ensure(std::max<uint64_t>(threads, 32) * 4 * MEM_SET_CAP * 16));
-  // variant 3: candidate lists in global memory (FAST_CAND_CAP per thread), so long reads
-  // stay on the fast pass instead of overflowing a 32-entry local list
-  if (variant == 3) RET(x->cwork.ensure((size_t)std::max<uint64_t>(threads, 128) * FAST_CAND_CAP * sizeof(Cand)));
+  const bool plain = variant == MEMS_PLAIN;
+  if (plain && (order || n_warp)) return set_error(HFM_E_ARG, "the plain launch takes no schedule");
+  if (!plain) {
+    RET(x->memwork.ensure(std::max<uint64_t>(threads, 32) * 4 * MEM_SET_CAP * 16));
+    // variant 3: candidate lists in global memory (FAST_CAND_CAP per thread), so long reads
+    // stay on the fast pass instead of overflowing a 32-entry local list
+    if (variant == 3) RET(x->cwork.ensure((size_t)std::max<uint64_t>(threads, 128) * FAST_CAND_CAP * sizeof(Cand)));
+  } else if (nq) {
+    // plain launch, count pass: every read's MemHits and positions counted by a full
+    // search, read back and prefix-summed to size the outputs before the write pass
+    RET(x->npos.ensure((size_t)nq * 4 + 4));
+    CK(cudaMemsetAsync(x->ctr.p, 0, sizeof(Counters), x->stream));
+    MemsOut oc{x->hit_start.as<uint64_t>(), x->hit_count.as<uint32_t>(), x->status.as<uint32_t>(),
+               x->ovf.as<uint32_t>(), &dctr(x)->n_ovf, &dctr(x)->touches};
+    Pool none{nullptr, &dctr(x)->iv_used, 0};
+    cudaEventRecord(x->evk[0], x->stream);
+    WITH_FMT(fmt, {
+      if (counting)
+        k_mems_plain<true, 0, FM><<<(nq + 127) / 128, 128, 0, x->stream>>>(
+            Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, P, nq, none, none, oc,
+            x->npos.as<uint32_t>(), &dctr(x)->seg_used);
+      else
+        k_mems_plain<false, 0, FM><<<(nq + 127) / 128, 128, 0, x->stream>>>(
+            Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, P, nq, none, none, oc,
+            x->npos.as<uint32_t>(), &dctr(x)->seg_used);
+    });
+    launches++;
+    CK(cudaGetLastError());
+    RET(read_ctr(x));
+    const uint64_t ivs_need = x->h_ctr->seg_used;
+    x->stats.occ_touches += x->h_ctr->touches;
+    RET(x->hit_base.ensure(((size_t)nq + 1) * 8));
+    RET(scan(x, x->hit_count.as<uint32_t>(), 1, nq, x->hit_base.as<uint64_t>(), other));
+    uint64_t counted = 0;
+    RET(read_u64(x, x->hit_base.as<uint64_t>() + nq, counted));
+    x->hit_cap = counted + 4096;             // exact for the reads the write pass completes
+    x->miv_cap = ivs_need + 4096;
+  }
   bool done = false;
   for (int attempt = 0; attempt < 8 && !done; attempt++) {
     RET(x->mivpool.ensure(x->miv_cap * 16)); x->miv_cap = x->mivpool.cap / 16;
@@ -567,33 +688,47 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       CK(cudaMemcpyAsync(x->ovf.p, order, (size_t)n_warp * 4, cudaMemcpyDeviceToDevice, x->stream));
       CK(cudaMemcpyAsync(&dctr(x)->n_ovf, &n_warp, 4, cudaMemcpyHostToDevice, x->stream));
     }
-    if (n_fast > 0 || n_long > 0) cudaEventRecord(x->evk[0], x->stream);
-    if (n_fast > 0 && n_long == 0) {     // with long reads, k_mems_seg runs the short reads too
+    if (plain && nq) {
+      // plain launch, write pass: the same search again, writing into the counted pools
+      WITH_FMT(fmt, {
+        if (counting)
+          k_mems_plain<true, 1, FM><<<(nq + 127) / 128, 128, 0, x->stream>>>(
+              Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, P, nq, ivp, hp, o,
+              x->npos.as<uint32_t>(), &dctr(x)->seg_used);
+        else
+          k_mems_plain<false, 1, FM><<<(nq + 127) / 128, 128, 0, x->stream>>>(
+              Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff, P, nq, ivp, hp, o,
+              x->npos.as<uint32_t>(), &dctr(x)->seg_used);
+      });
+      launches++;
+      CK(cudaGetLastError());
+      cudaEventRecord(x->evk[1], x->stream);
+      x->k_search_rec = true;
+    }
+    if (!plain && (n_fast > 0 || n_long > 0)) cudaEventRecord(x->evk[0], x->stream);
+    if (!plain && n_fast > 0 && n_long == 0) {     // with long reads, k_mems_seg runs the short reads too
       MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, variant == 3 ? x->cwork.as<Cand>() : nullptr,
                  variant == 3 ? FAST_CAND_CAP : 0u, &dctr(x)->queue, fast_ids, n_fast, &dctr(x)->still_ovf, 0u, wlog};
       unsigned grid = (unsigned)(threads / 128);
       if (x->memwork.cap < (size_t)grid * 128 * 4 * MEM_SET_CAP * 16) return set_error(HFM_E_ARG, "internal: work area too small");
-      if (counting && variant == 3) {
-        if (x->cwork.cap < (size_t)grid * 128 * FAST_CAND_CAP * sizeof(Cand)) return set_error(HFM_E_ARG, "internal: candidate area too small");
-        k_mems<true, 32, 0, 5><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                           d_q, d_qoff, P, ivp, hp, o, W);
-      } else if (counting)
-        k_mems<true, 32, MEM_KC, 5><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                                d_q, d_qoff, P, ivp, hp, o, W);
-      else if (variant == 0)
-        k_mems<false, 32, MEM_KC, 5><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                                 d_q, d_qoff, P, ivp, hp, o, W);
-      else if (variant == 1)
-        k_mems<false, 32, MEM_KC, 6><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                                 d_q, d_qoff, P, ivp, hp, o, W);
-      else if (variant == 3) {
-        if (x->cwork.cap < (size_t)grid * 128 * FAST_CAND_CAP * sizeof(Cand)) return set_error(HFM_E_ARG, "internal: candidate area too small");
-        k_mems<false, 32, 0, 8><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                            d_q, d_qoff, P, ivp, hp, o, W);
-      }
-      else
-        k_mems<false, 32, MEM_KC, 8><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                                 d_q, d_qoff, P, ivp, hp, o, W);
+      if (variant == 3 && x->cwork.cap < (size_t)grid * 128 * FAST_CAND_CAP * sizeof(Cand))
+        return set_error(HFM_E_ARG, "internal: candidate area too small");
+      WITH_FMT(fmt, {
+        if (counting && variant == 3)
+          k_mems<true, 32, 0, 5, FM><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(),
+                                                                  Rv.compat.as<uint16_t>(), d_q, d_qoff, P, ivp, hp, o, W);
+        else if (counting)
+          k_mems<true, 32, MEM_KC, 5, FM><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(),
+                                                                       Rv.compat.as<uint16_t>(), d_q, d_qoff, P, ivp, hp,
+                                                                       o, W);
+        else if (variant == 3)
+          k_mems<false, 32, 0, 8, FM><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(),
+                                                                   Rv.compat.as<uint16_t>(), d_q, d_qoff, P, ivp, hp, o, W);
+        else
+          k_mems<false, 32, MEM_KC, 8, FM><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(),
+                                                                        Rv.compat.as<uint16_t>(), d_q, d_qoff, P, ivp, hp,
+                                                                        o, W);
+      });
       launches++;
       CK(cudaGetLastError());
     }
@@ -613,25 +748,30 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       unsigned gs = (unsigned)std::max<uint64_t>(1, ts / 128), gm = (unsigned)std::max<uint64_t>(1, tmg / 128);
       if (x->memwork.cap < (size_t)gs * 128 * 4 * MEM_SET_CAP * 16 || x->cwork.cap < (size_t)gs * 128 * FAST_CAND_CAP * sizeof(Cand))
         return set_error(HFM_E_ARG, "internal: work area too small");
-      if (counting) {
-        k_mems_seg<true, 32, 5><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                           d_q, d_qoff, P, ivp, hp, o, W, G);
-        k_mems_fix<true, 32, 5><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                           d_q, d_qoff, P, ivp, Wf, G);
-        k_mems_merge<true, 32, 5><<<gm, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                             d_q, d_qoff, P, ivp, hp, o, W, G);
-      } else {
-        k_mems_seg<false, 32, 8><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                            d_q, d_qoff, P, ivp, hp, o, W, G);
-        k_mems_fix<false, 32, 8><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                            d_q, d_qoff, P, ivp, Wf, G);
-        k_mems_merge<false, 32, 8><<<gm, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                              d_q, d_qoff, P, ivp, hp, o, W, G);
-      }
+      WITH_FMT(fmt, {
+        if (counting) {
+          k_mems_seg<true, 32, 5, FM><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(),
+                                                                 Rv.compat.as<uint16_t>(), d_q, d_qoff, P, ivp, hp, o, W, G);
+          k_mems_fix<true, 32, 5, FM><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(),
+                                                                 Rv.compat.as<uint16_t>(), d_q, d_qoff, P, ivp, Wf, G);
+          k_mems_merge<true, 32, 5, FM><<<gm, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(),
+                                                                   Rv.compat.as<uint16_t>(), d_q, d_qoff, P, ivp, hp, o,
+                                                                   W, G);
+        } else {
+          k_mems_seg<false, 32, 8, FM><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(),
+                                                                  Rv.compat.as<uint16_t>(), d_q, d_qoff, P, ivp, hp, o, W,
+                                                                  G);
+          k_mems_fix<false, 32, 8, FM><<<gs, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(),
+                                                                  Rv.compat.as<uint16_t>(), d_q, d_qoff, P, ivp, Wf, G);
+          k_mems_merge<false, 32, 8, FM><<<gm, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(),
+                                                                    Rv.compat.as<uint16_t>(), d_q, d_qoff, P, ivp, hp, o,
+                                                                    W, G);
+        }
+      });
       launches += 3;
       CK(cudaGetLastError());
     }
-    if (n_fast > 0 || n_long > 0) {
+    if (!plain && (n_fast > 0 || n_long > 0)) {
       cudaEventRecord(x->evk[1], x->stream);
       x->k_search_rec = true;
     }
@@ -665,12 +805,16 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
         MemsOut o2 = o;
         o2.ovf_list = x->ovf2.as<uint32_t>();
         o2.n_ovf = &dctr(x)->n_wrp;
-        if (counting)
-          k_mems<true, 32, 0, 5><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                             d_q, d_qoff, P, ivp, hp, o2, W);
-        else
-          k_mems<false, 32, 0, 8><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(),
-                                                              d_q, d_qoff, P, ivp, hp, o2, W);
+        WITH_FMT(fmt, {
+          if (counting)
+            k_mems<true, 32, 0, 5, FM><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(),
+                                                                    Rv.compat.as<uint16_t>(), d_q, d_qoff, P, ivp, hp, o2,
+                                                                    W);
+          else
+            k_mems<false, 32, 0, 8, FM><<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(),
+                                                                     Rv.compat.as<uint16_t>(), d_q, d_qoff, P, ivp, hp, o2,
+                                                                     W);
+        });
         launches++;
         CK(cudaGetLastError());
         RET(read_ctr(x));
@@ -748,7 +892,7 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   RET(resolve_segments(x, Fw, x->hits.as<uint32_t>() + 4, 8, x->npos_scan.as<uint64_t>(), nh, npos,
               x->ref_bounds.as<uint32_t>(), nb, x->out_pairs.as<uint32_t>(), rl, other));
   RET(read_ctr(x));
-  end_stats(x);
+  RET(end_stats(x));
   x->stats.search_launches = launches; x->stats.resolve_launches = rl; x->stats.other_launches = other;
   x->stats.rows_resolved = npos; x->stats.lf_calls = x->h_ctr->steps; x->stats.hits_out = nh;
   if (x->h_ctr->walk_err) return set_error(HFM_E_WALK, "LF walk exceeded sample_rate steps: index inconsistent");
@@ -816,7 +960,14 @@ static void host_result_free(void* p) {
 struct Guard {
   hfm_index* x;
   std::unique_lock<std::mutex> lk;
-  explicit Guard(hfm_index* i) : x(i), lk(i->mu) { cudaSetDevice(i->device); }
+  explicit Guard(hfm_index* i) : x(i), lk(i->mu) {
+    cudaSetDevice(i->device);
+    if (!i->orphans.empty()) {           // a timed-out call left copies in flight: let them land
+      cudaStreamSynchronize(i->stream);
+      for (void* p : i->orphans) host_result_free(p);
+      i->orphans.clear();
+    }
+  }
 };
 
 }  // namespace hfm
@@ -854,15 +1005,11 @@ int hfm_index_load(const uint8_t* bytes, size_t len, int kind, const hfm_opts* o
   CK(cudaSetDevice(dev));
   std::unique_ptr<hfm_index> x(new hfm_index());
   x->device = dev; x->kind = kind; x->flags = opts ? opts->flags : 0;
-  if (const char* v = std::getenv("HFM_MEMS_VARIANT")) x->mems_variant = std::atoi(v);
-  if (const char* v = std::getenv("HFM_SEG_LEN")) {
-    int sl = std::atoi(v);
-    if (sl >= 64 && sl <= (int)SEG_MAX && sl % 32 == 0) x->seg_len = (uint32_t)sl;
-  }
   CK(cudaDeviceGetAttribute(&x->num_sms, cudaDevAttrMultiProcessorCount, dev));
   CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
   for (auto& e : x->ev) CK(cudaEventCreate(&e));
   for (auto& e : x->evk) CK(cudaEventCreate(&e));
+  CK(cudaEventCreateWithFlags(&x->ev_wait, cudaEventDisableTiming));
   CK(cudaMallocHost((void**)&x->h_ctr, sizeof(Counters)));
   RET(x->ctr.ensure(sizeof(Counters)));
   RET(build_device_fm(hf, x->fwd, x->stream));
@@ -875,7 +1022,8 @@ void hfm_index_free(hfm_index* x) {
   if (!x) return;
   cudaSetDevice(x->device);
   if (x->stream) cudaStreamSynchronize(x->stream);
-  for (DevBuf* b : {&x->fwd.occ, &x->fwd.ssa, &x->fwd.sa_vals, &x->fwd.lut, &x->fwd.bounds,
+  for (void* p : x->orphans) host_result_free(p);
+  for (DevBuf* b : {&x->fwd.occ, &x->fwd.sb, &x->rev.sb, &x->fwd.ssa, &x->fwd.sa_vals, &x->fwd.lut, &x->fwd.bounds,
                     &x->fwd.compat, &x->rev.occ, &x->rev.ssa, &x->rev.sa_vals, &x->rev.lut,
                     &x->rev.bounds, &x->rev.compat, &x->q, &x->qoff, &x->counts, &x->nhits, &x->niv, &x->ivoff,
                     &x->status, &x->ovf, &x->ivpool, &x->hitpool, &x->seg_row, &x->seg_off, &x->pos_base,
@@ -884,10 +1032,11 @@ void hfm_index_free(hfm_index* x) {
                     &x->hkeys, &x->hslot, &x->hflags, &x->huid, &x->urow, &x->ulen, &x->uoff, &x->uout,
                     &x->blockmap, &x->blockmap2, &x->ovf2, &x->ovf3, &x->lflag, &x->lpos, &x->sids, &x->lids,
                     &x->ucount, &x->ubase, &x->uread, &x->uk, &x->ubits, &x->uexit, &x->ust, &x->ucoff, &x->ucnt,
-                    &x->segpool, &x->fxe, &x->fxc, &x->fxx, &x->fxo, &x->fxn})
+                    &x->segpool, &x->fxe, &x->fxc, &x->fxx, &x->fxo, &x->fxn, &x->npos})
     b->release();
   for (auto& e : x->ev) if (e) cudaEventDestroy(e);
   for (auto& e : x->evk) if (e) cudaEventDestroy(e);
+  if (x->ev_wait) cudaEventDestroy(x->ev_wait);
   if (x->h_ctr) cudaFreeHost(x->h_ctr);
   if (x->stream) cudaStreamDestroy(x->stream);
   delete x;
@@ -919,7 +1068,7 @@ int hfm_get_tuning(const hfm_index* x, hfm_tuning* t) {
 
 int hfm_set_tuning(hfm_index* x, const hfm_tuning* t) {
   if (!x || !t) return set_error(HFM_E_ARG, "NULL argument");
-  if (t->mems_variant > 3) return set_error(HFM_E_ARG, "mems_variant must be 0..3");
+  if (t->mems_variant < 2 || t->mems_variant > 4) return set_error(HFM_E_ARG, "mems_variant must be 2, 3 or 4");
   if (t->seg_len < 64 || t->seg_len > SEG_MAX || t->seg_len % 32) return set_error(HFM_E_ARG, "seg_len must be a multiple of 32 in 64..4096");
   std::lock_guard<std::mutex> lk(x->mu);
   x->mems_variant = (int)t->mems_variant;
@@ -956,6 +1105,13 @@ int hfm_autotune_mems(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, 
   x->mems_variant = (int)cands[best_k].mems_variant;
   x->seg_len = cands[best_k].seg_len;
   *best = cands[best_k];
+  return HFM_OK;
+}
+
+int hfm_set_timeout(hfm_index* x, uint32_t ms) {
+  if (!x) return set_error(HFM_E_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(x->mu);
+  x->timeout_ms = ms;
   return HFM_OK;
 }
 
@@ -1000,8 +1156,7 @@ int hfm_count_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint3
   RET(x->counts.ensure((size_t)nq * 4 + 4));
   RET(count_device(x, x->q.as<uint8_t>(), x->qoff.as<uint64_t>(), nq, x->counts.as<uint32_t>()));
   if (nq) CK(cudaMemcpyAsync(counts_out, x->counts.p, (size_t)nq * 4, cudaMemcpyDeviceToHost, x->stream));
-  CK(cudaStreamSynchronize(x->stream));
-  return HFM_OK;
+  return wait_stream(x);
 }
 
 int hfm_locate_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32_t nq, uint32_t cap, hfm_hits** out) {
@@ -1023,8 +1178,12 @@ int hfm_locate_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint
   CK(cudaMemcpyAsync(h->offsets, d.d_offsets, ((size_t)nq + 1) * 8, cudaMemcpyDeviceToHost, x->stream));
   if (d.total) CK(cudaMemcpyAsync(h->pairs, d.d_pairs, (size_t)d.total * 8, cudaMemcpyDeviceToHost, x->stream));
   if (nq) CK(cudaMemcpyAsync(h->counts, d.d_counts, (size_t)nq * 4, cudaMemcpyDeviceToHost, x->stream));
-  cudaError_t e = cudaStreamSynchronize(x->stream);
-  if (e != cudaSuccess) { host_result_free(blk); return set_error(HFM_E_CUDA, cudaGetErrorString(e)); }
+  int rc = wait_stream(x);
+  if (rc != HFM_OK) {
+    if (rc == HFM_E_TIMEOUT) x->orphans.push_back(blk);   // copies may still land in blk
+    else host_result_free(blk);
+    return rc;
+  }
   *out = h;
   return HFM_OK;
 }
@@ -1049,8 +1208,12 @@ int hfm_mems_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32
   CK(cudaMemcpyAsync(m->hit_offsets, d.d_hit_offsets, ((size_t)nq + 1) * 8, cudaMemcpyDeviceToHost, x->stream));
   if (d.n_hits) CK(cudaMemcpyAsync(m->hits, d.d_hits, (size_t)d.n_hits * sizeof(hfm_mem_hit), cudaMemcpyDeviceToHost, x->stream));
   if (d.n_positions) CK(cudaMemcpyAsync(m->positions, d.d_positions, (size_t)d.n_positions * 8, cudaMemcpyDeviceToHost, x->stream));
-  cudaError_t e = cudaStreamSynchronize(x->stream);
-  if (e != cudaSuccess) { host_result_free(blk); return set_error(HFM_E_CUDA, cudaGetErrorString(e)); }
+  int rc = wait_stream(x);
+  if (rc != HFM_OK) {
+    if (rc == HFM_E_TIMEOUT) x->orphans.push_back(blk);   // copies may still land in blk
+    else host_result_free(blk);
+    return rc;
+  }
   *out = m;
   return HFM_OK;
 }

@@ -2,29 +2,41 @@
 // primitives every kernel uses.
 //
 // Device layout (built once by hfm_index_load from the reference's bincode records):
-//   occ   : one 96-byte record per 64 BWT rows: 16 x u32 counts of every symbol code before
-//           the block, then 4 x u64 bitplanes of each row's 4-bit symbol code.  The reference
-//           compacts symbols to lanes and splits counts into superblock + u16 delta; on the
-//           device the lane IS the symbol code and the count is whole, so a rank is one
-//           record read (3 DRAM sectors) and no table lookup.
+//   occ   : one record per 64 BWT rows holding, per symbol code, the count of that code
+//           from the start of the record's superblock (1,024 records = 65,536 rows) to the
+//           start of the record as a u16, and the rows' 4-bit codes as bitplanes:
+//             wide   (64 B, any text): 16 x u16 counts (codes 0..15), 4 x u64 planes;
+//             narrow (32 B, texts of codes 0..4 only — ExactDna and ACGT-only IUPAC
+//                    texts): 4 x u16 counts (codes 1..4), 3 x u64 planes; the count of
+//                    code 0 is the rows before the border minus the other four.
+//           One rank reads one or two 32-byte sectors.
+//   sb    : 16 x u32 per superblock: count of every code before the superblock (a few MB at
+//           3.1 Gbp; it stays in L2).
 //   ssa   : one 16-byte record per 64 rows: u64 "row is sampled" bits + u32 count of
 //           sampled rows before the word (SampledSuffixArray, src/suffix_array/mod.rs:54-63).
 //   sa_vals, seq_boundaries, lookup intervals: as in the reference.
-// rank(c, i) = occ[(i-1)/64].count[c] + popc(rows of code c <= (i-1)%64),
-// identical to OccTable::rank (src/occ/mod.rs:330-363).
+// rank(c, i) = sb[(i-1)/65536][c] + rec[(i-1)/64].count[c] + popc(rows of code c <= (i-1)%64),
+// identical to OccTable::rank (src/occ/mod.rs:330-363), whose records instead hold
+// compacted lanes with a u32 superblock count and a u16 delta per lane (src/occ/mod.rs:144).
 #pragma once
 #include <cstdint>
 
 namespace hfm {
 
+enum : uint32_t { OCC_WIDE = 0, OCC_NARROW = 1 };
+constexpr uint32_t SB_BLOCK_SHIFT = 10;           // records per superblock: 1024 (65,536 rows)
+constexpr uint32_t OCC_WIDE_U4 = 4;               // uint4 per wide record
+constexpr uint32_t OCC_NARROW_U4 = 2;             // uint4 per narrow record
+
 struct DevFm {
-  const uint4* occ;          // 6 x uint4 per block
+  const uint4* occ;          // OCC_WIDE_U4 or OCC_NARROW_U4 uint4 per record
+  const uint32_t* sb;        // 16 x u32 per superblock
   const uint4* ssa;          // 1 x uint4 per block
   const uint32_t* sa_vals;
   const uint2* lut;          // nullptr when the index has no lookup table
   const uint32_t* seq_bounds;
   uint32_t text_len, num_seqs, sample_rate, lut_depth;
-  uint32_t tag, lut_radix, num_blocks, _pad;
+  uint32_t tag, lut_radix, num_blocks, fmt;
   uint32_t C[16];
   uint8_t s2l[16], l2s[16], lut_digit[16];
   uint16_t sym_mask;         // symbols present in the text
@@ -54,69 +66,208 @@ __device__ __forceinline__ uint64_t u2to64(uint32_t lo, uint32_t hi) { return ((
 __device__ __forceinline__ uint32_t sel4(uint4 x, uint32_t i) {
   return (i & 2) ? ((i & 1) ? x.w : x.z) : ((i & 1) ? x.y : x.x);
 }
-__device__ __forceinline__ uint32_t sel16(uint4 a, uint4 b, uint4 c, uint4 d, uint32_t i) {
-  uint4 x = (i & 8) ? ((i & 4) ? d : c) : ((i & 4) ? b : a);
-  return sel4(x, i & 3);
+
+// One record with the rows of a border selected.  A border i (0 <= i <= text_len) is the
+// position between BWT rows i-1 and i: the record of row i-1, rows 0..(i-1)%64 selected
+// (border 0: record 0 with no row selected; its counts and superblock entry are 0).
+template <uint32_t FMT>
+struct Border {
+  uint4 a, b, c, d;       // wide: a, b = counts, c, d = planes; narrow: a = counts + p0, b = p1, p2
+  uint64_t low;           // selected rows
+  uint32_t sbi, i;        // superblock, the border itself
+
+  __device__ __forceinline__ uint64_t plane(int k) const {
+    if (FMT == OCC_WIDE) return k == 0 ? u2to64(c.x, c.y) : k == 1 ? u2to64(c.z, c.w) : k == 2 ? u2to64(d.x, d.y)
+                                                                                                  : u2to64(d.z, d.w);
+    return k == 0 ? u2to64(a.z, a.w) : k == 1 ? u2to64(b.x, b.y) : k == 2 ? u2to64(b.z, b.w) : 0ull;
+  }
+  // rows of code s among the selected ones (s a compile-time constant after unrolling)
+  __device__ __forceinline__ uint64_t eq(int s) const {
+    uint64_t m = low & ((s & 1) ? plane(0) : ~plane(0)) & ((s & 2) ? plane(1) : ~plane(1)) &
+                 ((s & 4) ? plane(2) : ~plane(2));
+    if (FMT == OCC_WIDE) m &= (s & 8) ? plane(3) : ~plane(3);
+    return m;
+  }
+  // count of code s from the superblock start to the record start (narrow: s in 1..4)
+  __device__ __forceinline__ uint32_t delta(int s) const {
+    uint32_t w;
+    if (FMT == OCC_WIDE) w = s < 8 ? sel4(a, (uint32_t)s >> 1) : sel4(b, ((uint32_t)s - 8) >> 1);
+    else w = s <= 2 ? a.x : a.y;
+    const int half = FMT == OCC_WIDE ? (s & 1) : ((s - 1) & 1);
+    return half ? (w >> 16) : (w & 0xFFFFu);
+  }
+  // rank within the superblock: count of code s in rows [superblock start, i)
+  __device__ __forceinline__ uint32_t local(int s) const { return delta(s) + (uint32_t)__popcll(eq(s)); }
+};
+
+template <uint32_t FMT>
+__device__ __forceinline__ Border<FMT> load_border(const DevFm& F, uint32_t i) {
+  Border<FMT> r;
+  uint32_t pos = i ? i - 1 : 0u, blk = pos >> 6;
+  r.low = i ? (2ull << (pos & 63)) - 1ull : 0ull;        // rows 0..pos%64 (pos%64 = 63: all)
+  r.sbi = blk >> SB_BLOCK_SHIFT;
+  r.i = i;
+  if (FMT == OCC_WIDE) {
+    const uint4* p = F.occ + (size_t)blk * OCC_WIDE_U4;
+    r.a = __ldg(p); r.b = __ldg(p + 1); r.c = __ldg(p + 2); r.d = __ldg(p + 3);
+  } else {
+    const uint4* p = F.occ + (size_t)blk * OCC_NARROW_U4;
+    r.a = __ldg(p); r.b = __ldg(p + 1); r.c = make_uint4(0, 0, 0, 0); r.d = r.c;
+  }
+  return r;
 }
 
-struct OccRec { uint4 c0, c1, c2, c3, p0, p1; };
-
-__device__ __forceinline__ OccRec load_occ(const DevFm& F, uint32_t blk) {
-  const uint4* r = F.occ + (size_t)blk * 6;
-  OccRec o;
-  o.c0 = __ldg(r); o.c1 = __ldg(r + 1); o.c2 = __ldg(r + 2); o.c3 = __ldg(r + 3);
-  o.p0 = __ldg(r + 4); o.p1 = __ldg(r + 5);
-  return o;
+__device__ __forceinline__ uint32_t sb_count(const DevFm& F, uint32_t sbi, uint32_t s) {
+  return __ldg(F.sb + (size_t)sbi * 16 + s);
 }
 
-// Rank of every symbol code at position i (counts of code s in bwt[0..i)), absent codes 0.
+// Absolute rank of code s at a border (occ(s, i)).
+template <uint32_t FMT>
+__device__ __forceinline__ uint32_t border_rank(const DevFm& F, const Border<FMT>& B, int s) {
+  if constexpr (FMT == OCC_NARROW) {
+    if (s == 0) {
+      uint32_t t = 0;
+#pragma unroll
+      for (int c = 1; c <= 4; c++) t += sb_count(F, B.sbi, c) + B.local(c);
+      return B.i - t;
+    }
+    return sb_count(F, B.sbi, s) + B.local(s);
+  } else {
+    const uint64_t sel0 = (s & 1) ? 0ull : ~0ull, sel1 = (s & 2) ? 0ull : ~0ull;
+    const uint64_t sel2 = (s & 4) ? 0ull : ~0ull, sel3 = (s & 8) ? 0ull : ~0ull;
+    const uint64_t m = B.low & (B.plane(0) ^ sel0) & (B.plane(1) ^ sel1) & (B.plane(2) ^ sel2) & (B.plane(3) ^ sel3);
+    const uint32_t w = sel4(s < 8 ? B.a : B.b, ((uint32_t)s & 7) >> 1);
+    return sb_count(F, B.sbi, s) + ((s & 1) ? (w >> 16) : (w & 0xFFFFu)) + (uint32_t)__popcll(m);
+  }
+}
+
+// The interval [lo, hi) of the BWT split by symbol: calls f(s, d, r, sbi) for every code s
+// in ascending order (0..4 narrow, 0..last wide), d = occ(s, hi) - occ(s, lo), and the lo
+// border's rank within its superblock r, so that occ(s, lo) = sb_count(F, sbi, s) + r (one
+// L2-resident load, made only for the codes the caller keeps).  No per-symbol arrays: each
+// code's count is formed and consumed in turn.
+template <uint32_t FMT, class Fn>
+__device__ __forceinline__ void split_by_symbol(const DevFm& F, uint32_t lo, uint32_t hi, uint32_t last, Fn&& f) {
+  if constexpr (FMT == OCC_NARROW) {
+    const Border<FMT> L = load_border<FMT>(F, lo), H = load_border<FMT>(F, hi);
+    const bool same_sb = L.sbi == H.sbi;
+    uint32_t d[5], r[5];
+    uint32_t sum = 0, rsum = 0;
+#pragma unroll
+    for (int s = 1; s <= 4; s++) {
+      const uint32_t a = L.local(s);
+      uint32_t v = H.local(s) - a;
+      if (!same_sb) v += sb_count(F, H.sbi, s) - sb_count(F, L.sbi, s);
+      d[s] = v; sum += v; r[s] = a; rsum += a;
+    }
+    d[0] = (hi - lo) - sum;
+    r[0] = (lo - (L.sbi << (SB_BLOCK_SHIFT + 6))) - rsum;   // rows of the superblock before lo, minus codes 1..4
+#pragma unroll
+    for (int s = 0; s <= 4; s++) f(s, d[s], r[s], L.sbi);
+  } else {
+    // Wide records: the codes in a rolled loop up to `last` (the highest code the caller
+    // needs), planes in registers and each count word read again from L1 when used, so
+    // the two borders do not hold 32 registers of counts through the loop.
+    const uint32_t pl = lo ? lo - 1 : 0u, ph = hi ? hi - 1 : 0u;
+    const uint32_t bl = pl >> 6, bh = ph >> 6;
+    const uint32_t* rl = reinterpret_cast<const uint32_t*>(F.occ + (size_t)bl * OCC_WIDE_U4);
+    const uint32_t* rh = reinterpret_cast<const uint32_t*>(F.occ + (size_t)bh * OCC_WIDE_U4);
+    const uint4 l0 = __ldg(F.occ + (size_t)bl * OCC_WIDE_U4 + 2), l1 = __ldg(F.occ + (size_t)bl * OCC_WIDE_U4 + 3);
+    const uint4 h0 = __ldg(F.occ + (size_t)bh * OCC_WIDE_U4 + 2), h1 = __ldg(F.occ + (size_t)bh * OCC_WIDE_U4 + 3);
+    const uint64_t lowl = lo ? (2ull << (pl & 63)) - 1ull : 0ull, lowh = hi ? (2ull << (ph & 63)) - 1ull : 0ull;
+    const uint64_t lp0 = u2to64(l0.x, l0.y), lp1 = u2to64(l0.z, l0.w), lp2 = u2to64(l1.x, l1.y), lp3 = u2to64(l1.z, l1.w);
+    const uint64_t hp0 = u2to64(h0.x, h0.y), hp1 = u2to64(h0.z, h0.w), hp2 = u2to64(h1.x, h1.y), hp3 = u2to64(h1.z, h1.w);
+    const uint32_t sbl = bl >> SB_BLOCK_SHIFT, sbh = bh >> SB_BLOCK_SHIFT;
+#pragma unroll 1
+    for (uint32_t s = 0; s <= last; s++) {
+      const uint64_t sel0 = (s & 1) ? 0ull : ~0ull, sel1 = (s & 2) ? 0ull : ~0ull;
+      const uint64_t sel2 = (s & 4) ? 0ull : ~0ull, sel3 = (s & 8) ? 0ull : ~0ull;
+      const uint64_t ml = lowl & (lp0 ^ sel0) & (lp1 ^ sel1) & (lp2 ^ sel2) & (lp3 ^ sel3);
+      const uint64_t mh = lowh & (hp0 ^ sel0) & (hp1 ^ sel1) & (hp2 ^ sel2) & (hp3 ^ sel3);
+      const uint32_t sh = (s & 1) * 16;
+      const uint32_t dl = (__ldg(rl + (s >> 1)) >> sh) & 0xFFFFu, dh = (__ldg(rh + (s >> 1)) >> sh) & 0xFFFFu;
+      const uint32_t a = dl + (uint32_t)__popcll(ml);
+      uint32_t v = (dh + (uint32_t)__popcll(mh)) - a;
+      if (sbl != sbh) v += sb_count(F, sbh, s) - sb_count(F, sbl, s);
+      f((int)s, v, a, sbl);
+    }
+  }
+}
+
+// The code of BWT row `row` and its rank at that row (LF step of a one-row interval,
+// lane_and_mask_bitplane + rank_at_lane, src/occ/mod.rs:434-480).
+template <uint32_t FMT>
+__device__ __forceinline__ void row_code_rank(const DevFm& F, uint32_t row, uint32_t& code, uint32_t& rank) {
+  Border<FMT> B = load_border<FMT>(F, row + 1);     // the record of `row`, rows 0..row%64
+  const uint32_t off = row & 63;
+  uint32_t c = (uint32_t)((B.plane(0) >> off) & 1) | ((uint32_t)((B.plane(1) >> off) & 1) << 1) |
+               ((uint32_t)((B.plane(2) >> off) & 1) << 2);
+  if (FMT == OCC_WIDE) c |= (uint32_t)((B.plane(3) >> off) & 1) << 3;
+  B.low >>= 1;                                         // rows before `row` only
+  B.i = row;
+  code = c;
+  uint32_t r;
+  if (FMT == OCC_WIDE) {
+    uint64_t m = B.low & ((c & 1) ? B.plane(0) : ~B.plane(0)) & ((c & 2) ? B.plane(1) : ~B.plane(1)) &
+                 ((c & 4) ? B.plane(2) : ~B.plane(2)) & ((c & 8) ? B.plane(3) : ~B.plane(3));
+    uint32_t w = sel4(c < 8 ? B.a : B.b, (c & 7) >> 1);
+    r = sb_count(F, B.sbi, c) + ((c & 1) ? (w >> 16) : (w & 0xFFFFu)) + (uint32_t)__popcll(m);
+  } else if (c == 0) {
+    r = border_rank<FMT>(F, B, 0);
+  } else {
+    uint64_t m = B.low & ((c & 1) ? B.plane(0) : ~B.plane(0)) & ((c & 2) ? B.plane(1) : ~B.plane(1)) &
+                 ((c & 4) ? B.plane(2) : ~B.plane(2));
+    uint32_t w = c <= 2 ? B.a.x : B.a.y;
+    r = sb_count(F, B.sbi, c) + (((c - 1) & 1) ? (w >> 16) : (w & 0xFFFFu)) + (uint32_t)__popcll(m);
+  }
+  rank = r;
+}
+
+// Rank of every symbol code at border i (counts of code s in bwt[0..i)), absent codes 0.
+// Used by the backward search and the warp-per-read kernels.
+template <uint32_t FMT>
+__device__ __forceinline__ void sym_ranks_t(const DevFm& F, uint32_t i, uint32_t r[16]) {
+  const Border<FMT> B = load_border<FMT>(F, i);
+  if (FMT == OCC_NARROW) {
+    uint32_t t = 0;
+#pragma unroll
+    for (int s = 1; s <= 4; s++) { r[s] = sb_count(F, B.sbi, s) + B.local(s); t += r[s]; }
+    r[0] = i - t;
+#pragma unroll
+    for (int s = 5; s < 16; s++) r[s] = 0;
+  } else {
+#pragma unroll
+    for (int s = 0; s < 16; s++) r[s] = sb_count(F, B.sbi, s) + B.local(s);
+  }
+}
+
 __device__ __forceinline__ void sym_ranks(const DevFm& F, const SmemFm& S, uint32_t i, uint32_t r[16]) {
-  if (i == 0) {
-#pragma unroll
-    for (int s = 0; s < 16; s++) r[s] = 0;
-    return;
-  }
-  uint32_t pos = i - 1, off = pos & 63;
-  OccRec o = load_occ(F, pos >> 6);
-  uint64_t low = (2ull << off) - 1ull;          // bits 0..off (off = 63 -> all ones)
-  uint64_t pl[4] = {u2to64(o.p0.x, o.p0.y), u2to64(o.p0.z, o.p0.w), u2to64(o.p1.x, o.p1.y), u2to64(o.p1.z, o.p1.w)};
-  // symbol masks by successive splits on planes 3,2,1,0: m[s] = rows of code s among bits <= off
-  uint64_t m[16];
-  m[0] = low;
-#pragma unroll
-  for (int p = 3; p >= 0; --p) {
-    const int cnt = 1 << (3 - p);
-#pragma unroll
-    for (int k = cnt - 1; k >= 0; --k) { uint64_t v = m[k]; m[2 * k + 1] = v & pl[p]; m[2 * k] = v & ~pl[p]; }
-  }
-  uint32_t cw[16] = {o.c0.x, o.c0.y, o.c0.z, o.c0.w, o.c1.x, o.c1.y, o.c1.z, o.c1.w,
-                     o.c2.x, o.c2.y, o.c2.z, o.c2.w, o.c3.x, o.c3.y, o.c3.z, o.c3.w};
-#pragma unroll
-  for (int s = 0; s < 16; s++) r[s] = cw[s] + (uint32_t)__popcll(m[s]);
+  (void)S;
+  if (F.fmt == OCC_NARROW) sym_ranks_t<OCC_NARROW>(F, i, r);
+  else sym_ranks_t<OCC_WIDE>(F, i, r);
 }
 
 // One LF step with the sampled-SA test (FmIndex::resolve_sa loop body,
 // src/fm_index/query.rs:282-291; lf_step src/occ/mod.rs:456-480).  Returns true with
 // *val = SA value when row `pos` is sampled; otherwise advances pos = LF(pos).
-__device__ __forceinline__ bool lf_or_sample(const DevFm& F, const SmemFm& S, uint32_t& pos, uint32_t& val) {
-  uint32_t blk = pos >> 6, off = pos & 63;
+template <uint32_t FMT>
+__device__ __forceinline__ bool lf_or_sample_t(const DevFm& F, const SmemFm& S, uint32_t& pos, uint32_t& val) {
+  const uint32_t blk = pos >> 6, off = pos & 63;
   uint4 w = __ldg(F.ssa + blk);
-  OccRec o = load_occ(F, blk);            // issued before the sampled test: overlaps its latency
+  uint32_t code, rank;
+  row_code_rank<FMT>(F, pos, code, rank);            // issued before the sampled test: overlaps its latency
   uint64_t word = u2to64(w.x, w.y);
-  uint64_t below = (1ull << off) - 1ull;
   if ((word >> off) & 1ull) {
-    val = __ldg(F.sa_vals + w.z + (uint32_t)__popcll(word & below));
+    val = __ldg(F.sa_vals + w.z + (uint32_t)__popcll(word & ((1ull << off) - 1ull)));
     return true;
   }
-  uint64_t p0 = u2to64(o.p0.x, o.p0.y), p1 = u2to64(o.p0.z, o.p0.w);
-  uint64_t p2 = u2to64(o.p1.x, o.p1.y), p3 = u2to64(o.p1.z, o.p1.w);
-  uint32_t lane = (uint32_t)((p0 >> off) & 1) | ((uint32_t)((p1 >> off) & 1) << 1) |
-                  ((uint32_t)((p2 >> off) & 1) << 2) | ((uint32_t)((p3 >> off) & 1) << 3);
-  uint64_t m = below & ((lane & 1) ? p0 : ~p0) & ((lane & 2) ? p1 : ~p1) & ((lane & 4) ? p2 : ~p2) &
-               ((lane & 8) ? p3 : ~p3);
-  uint32_t rank = sel16(o.c0, o.c1, o.c2, o.c3, lane) + (uint32_t)__popcll(m);
-  pos = S.C[lane] + rank;
+  pos = S.C[code] + rank;
   return false;
+}
+
+__device__ __forceinline__ bool lf_or_sample(const DevFm& F, const SmemFm& S, uint32_t& pos, uint32_t& val) {
+  if (F.fmt == OCC_NARROW) return lf_or_sample_t<OCC_NARROW>(F, S, pos, val);
+  return lf_or_sample_t<OCC_WIDE>(F, S, pos, val);
 }
 
 // partition_point(bounds, b <= p): first index with bounds[idx] > p.

@@ -39,6 +39,31 @@ int parse_fm(const uint8_t* p, uint64_t n, HostFm& f);
 
 void suffix_array(const uint8_t* text, uint32_t n, uint32_t* sa);
 
+// One FmIndex in the reference's record layout, ready for the bincode writer.
+struct BuiltFm {
+  uint32_t C[16];
+  uint8_t num_lanes, num_planes, s2l[16], l2s[16];
+  std::vector<uint32_t> sb;
+  std::vector<uint8_t> block_data;
+  uint64_t block_stride;
+  uint32_t encoding, text_len;
+  std::vector<uint8_t> ssa_words;
+  std::vector<uint32_t> sa_vals;
+  uint32_t rate;
+  uint32_t num_sequences;
+  std::vector<uint32_t> bounds;
+  std::vector<std::string> headers;
+  uint32_t lookup_depth;
+  std::vector<std::pair<uint32_t, uint32_t>> lut;
+  uint8_t tag;
+};
+
+// bincode-1 bytes of one FmIndex (src/fm_index/serialize.rs:55-67).
+void write_fm(const BuiltFm& f, std::vector<uint8_t>& out);
+int concat_text(const uint8_t* codes, const uint64_t* seq_off, uint32_t nseq, const char* const* headers,
+                std::vector<uint8_t>& text, std::vector<uint32_t>& bounds, std::vector<std::string>& hs);
+int emit_bytes(const BuiltFm& fwd, const BuiltFm& rev, int kind, uint8_t** bytes_out, size_t* len_out);
+
 }  // namespace hfm
 
 extern "C" int hfm_suffix_array(const uint8_t* text, uint32_t n, uint32_t* sa_out);

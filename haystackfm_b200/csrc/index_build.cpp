@@ -23,6 +23,8 @@ namespace hfm {
 
 static const uint32_t EMPTY = 0xFFFFFFFFu;
 
+#define RET_STATUS(x) do { int _r = (x); if (_r != HFM_OK) return _r; } while (0)
+
 // ---------------------------------------------------------------------------
 // SA-IS.  T[n-1] must be the unique smallest symbol; symbols are < K.
 // ---------------------------------------------------------------------------
@@ -107,25 +109,7 @@ struct BinWriter {
   void u64(uint64_t v) { put(&v, 8); }
 };
 
-struct BuiltFm {
-  uint32_t C[16];
-  uint8_t num_lanes, num_planes, s2l[16], l2s[16];
-  std::vector<uint32_t> sb;
-  std::vector<uint8_t> block_data;
-  uint64_t block_stride;
-  uint32_t encoding, text_len;
-  std::vector<uint8_t> ssa_words;
-  std::vector<uint32_t> sa_vals;
-  uint32_t rate;
-  uint32_t num_sequences;
-  std::vector<uint32_t> bounds;
-  std::vector<std::string> headers;
-  uint32_t lookup_depth;
-  std::vector<std::pair<uint32_t, uint32_t>> lut;
-  uint8_t tag;
-};
-
-static void write_fm(const BuiltFm& f, std::vector<uint8_t>& out) {
+void write_fm(const BuiltFm& f, std::vector<uint8_t>& out) {
   BinWriter w{out};
   for (int c = 0; c < 16; c++) w.u32(f.C[c]);
   // OccTable field order (src/occ/mod.rs:45-78)
@@ -272,26 +256,20 @@ static void build_fm(const uint8_t* text, uint32_t n, const std::vector<uint32_t
   }
 }
 
-}  // namespace hfm
 
-using namespace hfm;
-
-extern "C" int hfm_build_index(const uint8_t* codes, const uint64_t* seq_off, uint32_t nseq,
-                               const char* const* headers, const hfm_build_opts* opts, int kind,
-                               uint8_t** bytes_out, size_t* len_out) {
-  if (!codes && nseq) return set_error(HFM_E_ARG, "codes is NULL");
-  if (nseq == 0) return set_error(HFM_E_ARG, "empty sequence list");
-  if (!opts || !bytes_out || !len_out) return set_error(HFM_E_ARG, "NULL argument");
-  if (kind != HFM_KIND_FM && kind != HFM_KIND_BIDIR) return set_error(HFM_E_ARG, "kind must be 0 or 1");
-  if (opts->alphabet_tag > 1 || opts->occ_encoding > 1) return set_error(HFM_E_ARG, "bad alphabet tag or encoding");
-  // concatenate_sequences (src/alphabet.rs:375-393)
+// concatenate_sequences (src/alphabet.rs:375-393): codes 1..15 per sequence, a 0 sentinel
+// after each; bounds = exclusive ends; headers default to "seq_{i}".
+int concat_text(const uint8_t* codes, const uint64_t* seq_off, uint32_t nseq, const char* const* headers,
+                std::vector<uint8_t>& text, std::vector<uint32_t>& bounds, std::vector<std::string>& hs) {
   uint64_t total = 0;
   for (uint32_t s = 0; s < nseq; s++) total += seq_off[s + 1] - seq_off[s] + 1;
   if (total > 0xFFFFFFFFull) return set_error(HFM_E_ARG, "text too large: exceeds u32::MAX");
-  uint32_t n = (uint32_t)total;
-  std::vector<uint8_t> text(n);
-  std::vector<uint32_t> bounds(nseq);
-  std::vector<std::string> hs(nseq);
+  const uint32_t n = (uint32_t)total;
+  try {
+    text.assign(n, 0); bounds.assign(nseq, 0); hs.assign(nseq, std::string());
+  } catch (const std::bad_alloc&) {
+    return set_error(HFM_E_OOM, "host allocation failed");
+  }
   uint64_t pos = 0;
   for (uint32_t s = 0; s < nseq; s++) {
     uint64_t len = seq_off[s + 1] - seq_off[s];
@@ -304,6 +282,50 @@ extern "C" int hfm_build_index(const uint8_t* codes, const uint64_t* seq_off, ui
     std::string h = headers && headers[s] ? headers[s] : "";
     hs[s] = h.empty() ? "seq_" + std::to_string(s) : h;
   }
+  return HFM_OK;
+}
+
+// FmIndex bytes (kind 0) or BidirFmIndex bytes, [u32 fwd_len][fwd][rev] (kind 1,
+// src/fm_index/bidir_index.rs:183-192), in one malloc block.
+int emit_bytes(const BuiltFm& fwd, const BuiltFm& rev, int kind, uint8_t** bytes_out, size_t* len_out) {
+  std::vector<uint8_t> out;
+  try {
+    if (kind == HFM_KIND_FM) write_fm(fwd, out);
+    else {
+      std::vector<uint8_t> fb, rb;
+      write_fm(fwd, fb); write_fm(rev, rb);
+      uint32_t fl = (uint32_t)fb.size();
+      out.resize(4); std::memcpy(out.data(), &fl, 4);
+      out.insert(out.end(), fb.begin(), fb.end());
+      out.insert(out.end(), rb.begin(), rb.end());
+    }
+  } catch (const std::bad_alloc&) {
+    return set_error(HFM_E_OOM, "host allocation failed");
+  }
+  uint8_t* p = (uint8_t*)std::malloc(out.size());
+  if (!p) return set_error(HFM_E_OOM, "host allocation failed");
+  std::memcpy(p, out.data(), out.size());
+  *bytes_out = p; *len_out = out.size();
+  return HFM_OK;
+}
+
+}  // namespace hfm
+
+using namespace hfm;
+
+extern "C" int hfm_build_index(const uint8_t* codes, const uint64_t* seq_off, uint32_t nseq,
+                               const char* const* headers, const hfm_build_opts* opts, int kind,
+                               uint8_t** bytes_out, size_t* len_out) {
+  if (!codes && nseq) return set_error(HFM_E_ARG, "codes is NULL");
+  if (nseq == 0) return set_error(HFM_E_ARG, "empty sequence list");
+  if (!opts || !bytes_out || !len_out) return set_error(HFM_E_ARG, "NULL argument");
+  if (kind != HFM_KIND_FM && kind != HFM_KIND_BIDIR) return set_error(HFM_E_ARG, "kind must be 0 or 1");
+  if (opts->alphabet_tag > 1 || opts->occ_encoding > 1) return set_error(HFM_E_ARG, "bad alphabet tag or encoding");
+  std::vector<uint8_t> text;
+  std::vector<uint32_t> bounds;
+  std::vector<std::string> hs;
+  RET_STATUS(concat_text(codes, seq_off, nseq, headers, text, bounds, hs));
+  const uint32_t n = (uint32_t)text.size();
   BuiltFm fwd, rev;
   std::vector<uint8_t> rtext;
   bool par = (opts->threads == 0 || opts->threads > 1) && kind == HFM_KIND_BIDIR;
@@ -325,21 +347,7 @@ extern "C" int hfm_build_index(const uint8_t* codes, const uint64_t* seq_off, ui
   } catch (const std::bad_alloc&) {
     return set_error(HFM_E_OOM, "host allocation failed during index construction");
   }
-  std::vector<uint8_t> out;
-  if (kind == HFM_KIND_FM) write_fm(fwd, out);
-  else {
-    std::vector<uint8_t> fb, rb;
-    write_fm(fwd, fb); write_fm(rev, rb);
-    uint32_t fl = (uint32_t)fb.size();
-    out.resize(4); std::memcpy(out.data(), &fl, 4);
-    out.insert(out.end(), fb.begin(), fb.end());
-    out.insert(out.end(), rb.begin(), rb.end());
-  }
-  uint8_t* p = (uint8_t*)std::malloc(out.size());
-  if (!p) return set_error(HFM_E_OOM, "host allocation failed");
-  std::memcpy(p, out.data(), out.size());
-  *bytes_out = p; *len_out = out.size();
-  return HFM_OK;
+  return emit_bytes(fwd, rev, kind, bytes_out, len_out);
 }
 
 extern "C" int hfm_suffix_array(const uint8_t* text, uint32_t n, uint32_t* sa_out) {

@@ -291,31 +291,18 @@ struct TwoList {
   __device__ __forceinline__ uint32_t size() const { return n1 + nb; }
 };
 
-// One row's symbol and its rank at that row (LF step of a one-row interval).
-__device__ __forceinline__ void row_symbol_rank(const DevFm& F, uint32_t row, uint32_t& sym, uint32_t& rank) {
-  uint32_t off = row & 63;
-  OccRec o = load_occ(F, row >> 6);
-  uint64_t p0 = u2to64(o.p0.x, o.p0.y), p1 = u2to64(o.p0.z, o.p0.w);
-  uint64_t p2 = u2to64(o.p1.x, o.p1.y), p3 = u2to64(o.p1.z, o.p1.w);
-  uint32_t c = (uint32_t)((p0 >> off) & 1) | ((uint32_t)((p1 >> off) & 1) << 1) |
-               ((uint32_t)((p2 >> off) & 1) << 2) | ((uint32_t)((p3 >> off) & 1) << 3);
-  uint64_t m = ((1ull << off) - 1ull) & ((c & 1) ? p0 : ~p0) & ((c & 2) ? p1 : ~p1) & ((c & 4) ? p2 : ~p2) &
-               ((c & 8) ? p3 : ~p3);
-  sym = c;
-  rank = sel16(o.c0, o.c1, o.c2, o.c3, c) + (uint32_t)__popcll(m);
-}
-
 // DIR 0 = right (ranks on the reverse index), 1 = left (ranks on the forward index).
-template <int DIR, bool COUNT_TOUCH, class SR>
+template <int DIR, bool COUNT_TOUCH, uint32_t FMT, class SR>
 __device__ __forceinline__ void extend_set(const DevFm& X, const SmemFm& S, uint32_t mask, const TwoList<SR>& in,
                                            TwoList<SR>& out, uint32_t cap, uint32_t& cov, bool& ovf,
                                            uint64_t& touches) {
   out.n1 = 0; out.nb = 0; cov = 0;
+  const uint32_t top = mask ? 31u - __clz(mask) : 0u;     // highest code that can extend
   for (uint32_t i = 0; i < in.n1; i++) {
     BIv iv = in.s.single(i);
     uint32_t a = DIR == 0 ? iv.rlo : iv.flo, base = DIR == 0 ? iv.flo : iv.rlo;
     uint32_t s0, rk;
-    row_symbol_rank(X, a, s0, rk);
+    row_code_rank<FMT>(X, a, s0, rk);
     if (COUNT_TOUCH) touches += 1;
     if ((mask >> s0) & 1) {
       if (out.n1 + out.nb >= cap) { ovf = true; return; }
@@ -328,37 +315,41 @@ __device__ __forceinline__ void extend_set(const DevFm& X, const SmemFm& S, uint
     BIv iv = in.s[cap - 1 - k];
     uint32_t a = DIR == 0 ? iv.rlo : iv.flo, b = DIR == 0 ? iv.rhi : iv.fhi;
     uint32_t base = DIR == 0 ? iv.flo : iv.rlo;
-    uint32_t rl[16], rh[16];
-    sym_ranks(X, S, a, rl);
-    sym_ranks(X, S, b, rh);
     if (COUNT_TOUCH) touches += (a != 0) + (b != 0);
     uint32_t run = 0;
-#pragma unroll
-    for (int s = 0; s < 16; s++) {
-      uint32_t d = rh[s] - rl[s];
-      if (((mask >> s) & 1) && d) {
+    // count_smaller_than (src/fm_index/bidir.rs:125-143): the new interval of symbol s on
+    // the other strand starts after every code below s, $ included
+    split_by_symbol<FMT>(X, a, b, top, [&](int s, uint32_t d, uint32_t r, uint32_t sbi) {
+      if (!ovf && ((mask >> s) & 1) && d) {
         if (out.n1 + out.nb >= cap) { ovf = true; return; }
-        BIv e;
-        if (DIR == 0) { e.flo = base + run; e.fhi = base + run + d; e.rlo = S.C[s] + rl[s]; e.rhi = S.C[s] + rh[s]; }
-        else { e.flo = S.C[s] + rl[s]; e.fhi = S.C[s] + rh[s]; e.rlo = base + run; e.rhi = base + run + d; }
-        if (d == 1) out.s.set_single(out.n1++, e.flo, e.rlo);
-        else out.s[cap - 1 - out.nb++] = e;
+        const uint32_t lo = S.C[s] + sb_count(X, sbi, s) + r;
+        if (d == 1) {
+          if (DIR == 0) out.s.set_single(out.n1++, base + run, lo);
+          else out.s.set_single(out.n1++, lo, base + run);
+        } else {
+          BIv e;
+          if (DIR == 0) { e.flo = base + run; e.fhi = base + run + d; e.rlo = lo; e.rhi = lo + d; }
+          else { e.flo = lo; e.fhi = lo + d; e.rlo = base + run; e.rhi = base + run + d; }
+          out.s[cap - 1 - out.nb++] = e;
+        }
         cov += d;
       }
       run += d;
-    }
+    });
+    if (ovf) return;
   }
 }
 
 // Does any interval of the set extend by a compatible symbol?
-template <int DIR, bool COUNT_TOUCH, class SR>
+template <int DIR, bool COUNT_TOUCH, uint32_t FMT, class SR>
 __device__ __forceinline__ bool any_extend(const DevFm& X, const SmemFm& S, uint32_t mask, const TwoList<SR>& in,
                                            uint32_t cap, uint64_t& touches) {
   bool any = false;
+  const uint32_t top = mask ? 31u - __clz(mask) : 0u;
   for (uint32_t i = 0; i < in.n1; i++) {
     BIv iv = in.s.single(i);
     uint32_t s0, rk;
-    row_symbol_rank(X, DIR == 0 ? iv.rlo : iv.flo, s0, rk);
+    row_code_rank<FMT>(X, DIR == 0 ? iv.rlo : iv.flo, s0, rk);
     if (COUNT_TOUCH) touches += 1;
     any |= (mask >> s0) & 1;
   }
@@ -366,12 +357,9 @@ __device__ __forceinline__ bool any_extend(const DevFm& X, const SmemFm& S, uint
   for (uint32_t k = 0; k < in.nb; k++) {
     BIv iv = in.s[cap - 1 - k];
     uint32_t a = DIR == 0 ? iv.rlo : iv.flo, b = DIR == 0 ? iv.rhi : iv.fhi;
-    uint32_t rl[16], rh[16];
-    sym_ranks(X, S, a, rl);
-    sym_ranks(X, S, b, rh);
     if (COUNT_TOUCH) touches += (a != 0) + (b != 0);
-#pragma unroll
-    for (int s = 0; s < 16; s++) if (((mask >> s) & 1) && rh[s] != rl[s]) return true;
+    split_by_symbol<FMT>(X, a, b, top, [&](int s, uint32_t d, uint32_t, uint32_t) { any |= ((mask >> s) & 1) && d; });
+    if (any) return true;
   }
   return false;
 }
@@ -416,7 +404,7 @@ __device__ __forceinline__ uint32_t qmask(const SmemFm& S, uint8_t c) { return c
 // emit(qs, qe, count, set, pivot).  Returns the next pivot, max(reach, pivot + 1), or ~0u
 // on overflow (flags in st).  The sweep is a chain pivot -> next(pivot) that depends only
 // on the read, which is what lets a long read be cut into independently swept segments.
-template <bool COUNT_TOUCH, class SR, class Emit>
+template <bool COUNT_TOUCH, uint32_t FMT, class SR, class Emit>
 __device__ __forceinline__ uint32_t smem_pivot(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf, const SmemFm& Sr,
                                                const uint8_t* q, uint32_t n, uint32_t pivot, const MemsParams& P,
                                                const SR& curr, const SR& nxt, const SR& wa, const SR& wb,
@@ -427,7 +415,7 @@ __device__ __forceinline__ uint32_t smem_pivot(const DevFm& Fw, const DevFm& Rv,
   TL c{curr, 0, 0}, x{nxt, 0, 0};
   start_full(x, full, set_cap);
   uint32_t cov;
-  extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[pivot]), x, c, set_cap, cov, ovf, touches);
+  extend_set<0, COUNT_TOUCH, FMT>(Rv, Sr, qmask(Sr, q[pivot]), x, c, set_cap, cov, ovf, touches);
   if (ovf) { st |= ST_SET_OVF; return ~0u; }
   if (c.size() == 0) return pivot + 1;
   uint32_t j = pivot + 1, reach = pivot + 1;
@@ -437,7 +425,7 @@ __device__ __forceinline__ uint32_t smem_pivot(const DevFm& Fw, const DevFm& Rv,
     x.n1 = x.nb = 0;
     if (j == n) { end = n; next_empty = true; record = true; }
     else {
-      extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, x, set_cap, ncov, ovf, touches);
+      extend_set<0, COUNT_TOUCH, FMT>(Rv, Sr, qmask(Sr, q[j]), c, x, set_cap, ncov, ovf, touches);
       if (ovf) { st |= ST_SET_OVF; return ~0u; }
       end = j; next_empty = x.size() == 0; record = ncov != cov;
     }
@@ -450,7 +438,7 @@ __device__ __forceinline__ uint32_t smem_pivot(const DevFm& Fw, const DevFm& Rv,
       int t = 0;
       while (start > 0) {
         uint32_t lcov;
-        extend_set<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[start - 1]), b, bufs[t], set_cap, lcov, ovf, touches);
+        extend_set<1, COUNT_TOUCH, FMT>(Fw, Sf, qmask(Sf, q[start - 1]), b, bufs[t], set_cap, lcov, ovf, touches);
         if (ovf) { st |= ST_SET_OVF; return ~0u; }
         if (bufs[t].size() == 0) break;
         b = bufs[t]; bcov = lcov; t ^= 1; start--;
@@ -458,7 +446,7 @@ __device__ __forceinline__ uint32_t smem_pivot(const DevFm& Fw, const DevFm& Rv,
       if (end - start >= P.min_len) {
         // right-maximality (smem.rs:202-207); with no left extension it is next_empty
         bool rmax = end == n ||
-                    (start == pivot ? next_empty : !any_extend<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[end]), b, set_cap, touches));
+                    (start == pivot ? next_empty : !any_extend<0, COUNT_TOUCH, FMT>(Rv, Sr, qmask(Sr, q[end]), b, set_cap, touches));
         if (rmax && !emit(start, end, bcov, b, pivot)) return ~0u;
       }
     }
@@ -486,18 +474,18 @@ struct CandSink {
   }
 };
 
-// Candidate search for one read.  Returns the number of candidates, or ~0u on overflow
-// of a set, the candidate list or the interval pool (flags in st).
-template <bool COUNT_TOUCH, class SR>
-__device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf, const SmemFm& Sr,
-                             const uint8_t* q, uint32_t n, const MemsParams& P, const SR& curr, const SR& nxt,
-                             const SR& wa, const SR& wb, uint32_t set_cap, Cand* cands, uint32_t cand_cap,
-                             Pool& ivpool, uint32_t& st, uint64_t& touches) {
+// Candidate search for one read into `sink` (find_mems or find_smems candidates).  Returns
+// the number of candidates, or ~0u on overflow of a set, the candidate list or the
+// interval pool (flags in st).
+template <bool COUNT_TOUCH, uint32_t FMT, class SR, class Sink>
+__device__ uint32_t mems_sweep(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf, const SmemFm& Sr,
+                               const uint8_t* q, uint32_t n, const MemsParams& P, const SR& curr, const SR& nxt,
+                               const SR& wa, const SR& wb, uint32_t set_cap, Sink& sink, uint32_t& st,
+                               uint64_t& touches) {
   using TL = TwoList<SR>;
   if (n == 0 || P.min_len == 0) return 0;
   const BIv full = {0, Fw.text_len, 0, Fw.text_len};
   bool ovf = false;
-  CandSink<SR> sink{cands, 0, cand_cap, &ivpool, &st, set_cap};
   if (P.mode == 1) {
     // find_mems: raw_mem_from(i) for every start (src/fm_index/smem.rs:250-295)
     for (uint32_t i = 0; i < n; i++) {
@@ -507,13 +495,13 @@ __device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf,
       bool matched = false;
       while (j < n) {
         uint32_t ncov;
-        extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, x, set_cap, ncov, ovf, touches);
+        extend_set<0, COUNT_TOUCH, FMT>(Rv, Sr, qmask(Sr, q[j]), c, x, set_cap, ncov, ovf, touches);
         if (ovf) { st |= ST_SET_OVF; return ~0u; }
         if (x.size() == 0) break;
         TL t = c; c = x; x = t; cov = ncov; j++; matched = true;
       }
       if (!matched || j - i < P.min_len) continue;
-      bool lmax = i == 0 || !any_extend<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[i - 1]), c, set_cap, touches);
+      bool lmax = i == 0 || !any_extend<1, COUNT_TOUCH, FMT>(Fw, Sf, qmask(Sf, q[i - 1]), c, set_cap, touches);
       if (!lmax) continue;
       if (!sink(i, j, cov, c, i)) return ~0u;
     }
@@ -522,10 +510,19 @@ __device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf,
   // find_smems: collect_smem_candidates (src/fm_index/smem.rs:154-222)
   uint32_t pivot = 0;
   while (pivot < n) {
-    pivot = smem_pivot<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q, n, pivot, P, curr, nxt, wa, wb, set_cap, st, touches, sink);
+    pivot = smem_pivot<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q, n, pivot, P, curr, nxt, wa, wb, set_cap, st, touches, sink);
     if (pivot == ~0u) return ~0u;
   }
   return sink.nc;
+}
+
+template <bool COUNT_TOUCH, uint32_t FMT, class SR>
+__device__ uint32_t mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf, const SmemFm& Sr,
+                             const uint8_t* q, uint32_t n, const MemsParams& P, const SR& curr, const SR& nxt,
+                             const SR& wa, const SR& wb, uint32_t set_cap, Cand* cands, uint32_t cand_cap,
+                             Pool& ivpool, uint32_t& st, uint64_t& touches) {
+  CandSink<SR> sink{cands, 0, cand_cap, &ivpool, &st, set_cap};
+  return mems_sweep<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q, n, P, curr, nxt, wa, wb, set_cap, sink, st, touches);
 }
 
 // Sort candidates by (qs, qe) (stable), drop duplicates, keep the containment-maximal ones
@@ -625,7 +622,7 @@ __global__ void k_split_ovf(const uint32_t* __restrict__ list, uint32_t n, uint3
   else mid[atomicAdd(n_mid, 1u)] = i;
 }
 
-template <bool COUNT_TOUCH, int STRIDE, int KC, int MINB>
+template <bool COUNT_TOUCH, int STRIDE, int KC, int MINB, uint32_t FMT>
 __global__ void __launch_bounds__(128, MINB) k_mems(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
                                              const uint16_t* __restrict__ compat_rv, const uint8_t* __restrict__ q,
                                              const uint64_t* __restrict__ qoff, MemsParams P, Pool ivpool,
@@ -651,7 +648,7 @@ __global__ void __launch_bounds__(128, MINB) k_mems(DevFm Fw, DevFm Rv, const ui
     uint32_t st = ST_OK;
     uint64_t o = qoff[i];
     uint64_t t0 = touches;
-    uint32_t nc = mems_one<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, (uint32_t)(qoff[i + 1] - o), P, s0, s1, s2, s3,
+    uint32_t nc = mems_one<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, (uint32_t)(qoff[i + 1] - o), P, s0, s1, s2, s3,
                                         W.set_cap, cands, cand_cap, ivpool, st, touches);
     uint64_t hs = 0; uint32_t hc = 0;
     if (nc != ~0u) {
@@ -673,6 +670,96 @@ __global__ void __launch_bounds__(128, MINB) k_mems(DevFm Fw, DevFm Rv, const ui
   if (COUNT_TOUCH && touches) atomicAdd(out.touches, (unsigned long long)touches);
 }
 
+
+// =====================================================================================
+// The plain launch: one thread per read over a grid the size of the batch, interval sets
+// and candidate list in the thread's local memory, and a count pass before the write pass
+// whose totals the host reads back to size the outputs — the structure of the reference's
+// GPU search (one invocation per query, count-then-write, host prefix sum;
+// shaders/mem_find.wgsl:179-372, src/gpu/mem_find.rs:213-244) restated with the CPU
+// semantics.  It is the baseline the persistent path is measured against.  Reads whose
+// sets or candidates outgrow the local capacity go to the warp-per-read kernel, so the
+// results are those of every other path.
+// =====================================================================================
+constexpr uint32_t PLAIN_SET_CAP = 64;
+constexpr int PLAIN_KC = 32;
+
+// Count-pass sink: candidates with their MemHit count (nivs) and position count (in
+// ivoff), no interval copies.
+template <class SR>
+struct CountSink {
+  Cand* cands; uint32_t nc, cap; uint32_t* st; uint32_t set_cap; uint32_t max_hits, resolve;
+  unsigned long long ivs_all;       // intervals of every candidate (the write pass's pool need)
+  __device__ __forceinline__ bool operator()(uint32_t qs, uint32_t qe, uint32_t count, const TwoList<SR>& ivs,
+                                             uint32_t pivot) {
+    if (nc >= cap) { *st |= ST_CAND_OVF; return false; }
+    uint64_t npos = 0;
+    if (resolve) {
+      npos = max_hits ? ivs.n1 : 0u;
+      for (uint32_t k = 0; k < ivs.nb; k++) {
+        BIv iv = ivs.s[set_cap - 1 - k];
+        npos += min(iv.fhi - iv.flo, max_hits);
+      }
+    }
+    ivs_all += ivs.size();
+    cands[nc++] = Cand{qs, qe, count, ivs.size(), npos, pivot, 0u};
+    return true;
+  }
+};
+
+template <bool COUNT_TOUCH, int PASS, uint32_t FMT>
+__global__ void __launch_bounds__(128) k_mems_plain(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
+                                                   const uint16_t* __restrict__ compat_rv, const uint8_t* __restrict__ q,
+                                                   const uint64_t* __restrict__ qoff, MemsParams P, uint32_t n,
+                                                   Pool ivpool, Pool hitpool, MemsOut out, uint32_t* pos_count,
+                                                   unsigned long long* ivs_need) {
+  __shared__ SmemFm Sf, Sr;
+  smem_fm_init(Sf, Fw, compat_fw);
+  smem_fm_init(Sr, Rv, compat_rv);
+  __syncthreads();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  using SR = SetRef<BIv, 1>;
+  uint32_t lset[4][3 * PLAIN_SET_CAP];
+  SR s0{lset[0], PLAIN_SET_CAP}, s1{lset[1], PLAIN_SET_CAP}, s2{lset[2], PLAIN_SET_CAP}, s3{lset[3], PLAIN_SET_CAP};
+  Cand cands[PLAIN_KC];
+  uint64_t touches = 0;
+  const uint64_t o = qoff[i];
+  const uint32_t len = (uint32_t)(qoff[i + 1] - o);
+  if (PASS == 0) {
+    uint32_t st = ST_OK;
+    CountSink<SR> sink{cands, 0, (uint32_t)PLAIN_KC, &st, PLAIN_SET_CAP, P.max_hits, P.resolve, 0ull};
+    uint32_t nc = mems_sweep<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, len, P, s0, s1, s2, s3, PLAIN_SET_CAP, sink, st,
+                                               touches);
+    uint32_t hits = 0, pos = 0;
+    if (nc != ~0u) {
+      if (P.mode == 0) nc = finalize_smems(cands, nc);
+      for (uint32_t k = 0; k < nc; k++) { hits += cands[k].nivs; pos += (uint32_t)cands[k].ivoff; }
+      atomicAdd(ivs_need, sink.ivs_all);
+    }
+    if (st) { hits = 0; pos = 0; }
+    out.hit_count[i] = hits; pos_count[i] = pos; out.status[i] = st;
+  } else {
+    // reads the count pass found too large for local memory keep their flags; a pool
+    // overflow of an earlier attempt is cleared (the host regrew the pools)
+    uint32_t st = out.status[i] & (ST_SET_OVF | ST_CAND_OVF);
+    uint64_t hs = 0; uint32_t hc = 0;
+    if (st == ST_OK) {
+      CandSink<SR> sink{cands, 0, (uint32_t)PLAIN_KC, &ivpool, &st, PLAIN_SET_CAP};
+      uint32_t nc = mems_sweep<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, len, P, s0, s1, s2, s3, PLAIN_SET_CAP, sink,
+                                                 st, touches);
+      if (nc != ~0u) {
+        if (P.mode == 0) nc = finalize_smems(cands, nc);
+        if (!write_hits(cands, nc, P, ivpool, hitpool, hs, hc)) st |= ST_POOL_OVF;
+      }
+      if (st) { hs = 0; hc = 0; }
+    }
+    out.status[i] = st;
+    out.hit_start[i] = hs; out.hit_count[i] = hc;
+    if (st & (ST_SET_OVF | ST_CAND_OVF)) out.ovf_list[atomicAdd(out.n_ovf, 1u)] = i;
+  }
+  if (COUNT_TOUCH && touches) atomicAdd(out.touches, (unsigned long long)touches);
+}
 
 // =====================================================================================
 // Long reads: the SMEM sweep of a read cut into segments.
@@ -756,7 +843,7 @@ __global__ void k_unit_fill(const uint32_t* __restrict__ long_ids, uint32_t n_lo
 
 // One persistent queue over the segments of the long reads followed by the whole short
 // reads of the batch (the longest jobs first; the short reads fill the tail).
-template <bool COUNT_TOUCH, int STRIDE, int MINB>
+template <bool COUNT_TOUCH, int STRIDE, int MINB, uint32_t FMT>
 __global__ void __launch_bounds__(128, MINB) k_mems_seg(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
                                                  const uint16_t* __restrict__ compat_rv, const uint8_t* __restrict__ q,
                                                  const uint64_t* __restrict__ qoff, MemsParams P, Pool ivpool,
@@ -796,7 +883,7 @@ __global__ void __launch_bounds__(128, MINB) k_mems_seg(DevFm Fw, DevFm Rv, cons
     uint32_t p = s;
     while (p < e) {
       if (unit) { uint32_t d = p - s; bits[d >> 5] |= 1u << (d & 31); }
-      p = smem_pivot<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
+      p = smem_pivot<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
       if (p == ~0u) break;
     }
     uint32_t nc = sink.nc;
@@ -837,7 +924,7 @@ __global__ void __launch_bounds__(128, MINB) k_mems_seg(DevFm Fw, DevFm Rv, cons
 // Fix-up pass, one thread per segment after the first: sweeps from the previous segment's
 // exit pivot until the chain meets this segment's chain (usually within a few pivots), so
 // the merge below only has to check that the entry it assumed is the true one.
-template <bool COUNT_TOUCH, int STRIDE, int MINB>
+template <bool COUNT_TOUCH, int STRIDE, int MINB, uint32_t FMT>
 __global__ void __launch_bounds__(128, MINB) k_mems_fix(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
                                                  const uint16_t* __restrict__ compat_rv, const uint8_t* __restrict__ q,
                                                  const uint64_t* __restrict__ qoff, MemsParams P, Pool ivpool,
@@ -868,7 +955,7 @@ __global__ void __launch_bounds__(128, MINB) k_mems_fix(DevFm Fw, DevFm Rv, cons
     CandSink<SR> sink{cands, 0, W.cand_cap, &ivpool, &st, W.set_cap};
     uint32_t p = entry;
     while (p < e && !((bits[(p - s) >> 5] >> ((p - s) & 31)) & 1u)) {
-      p = smem_pivot<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
+      p = smem_pivot<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
       if (p == ~0u) break;
     }
     if (COUNT_TOUCH && W.work_log) atomicAdd(W.work_log + 4 * (size_t)i, (uint32_t)(touches - t0));
@@ -888,7 +975,7 @@ __global__ void __launch_bounds__(128, MINB) k_mems_fix(DevFm Fw, DevFm Rv, cons
   if (COUNT_TOUCH && touches) atomicAdd(G.touches, (unsigned long long)touches);
 }
 
-template <bool COUNT_TOUCH, int STRIDE, int MINB>
+template <bool COUNT_TOUCH, int STRIDE, int MINB, uint32_t FMT>
 __global__ void __launch_bounds__(128, MINB) k_mems_merge(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
                                                    const uint16_t* __restrict__ compat_rv,
                                                    const uint8_t* __restrict__ q, const uint64_t* __restrict__ qoff,
@@ -946,7 +1033,7 @@ __global__ void __launch_bounds__(128, MINB) k_mems_merge(DevFm Fw, DevFm Rv, co
       uint32_t p = t;
       const uint32_t* bits = G.bits + u * G.seg_words;
       while (p < e && !((bits[(p - s) >> 5] >> ((p - s) & 31)) & 1u)) {
-        p = smem_pivot<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
+        p = smem_pivot<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
         if (p == ~0u) { fail = true; break; }
       }
       if (fail) break;

@@ -96,6 +96,25 @@ def _build(sequences: Sequence[DnaSequence], config: FmIndexConfig, tag: int, ki
     return data
 
 
+def _build_gpu(sequences: Sequence[DnaSequence], config: FmIndexConfig, tag: int, kind: int, device: int = 0) -> bytes:
+    """hfm_build_index_gpu: the same bytes as _build, constructed on the GPU."""
+    if not sequences:
+        raise FmIndexError.empty_sequence()
+    codes = [s.as_slice() for s in sequences]
+    flat, off = L.pack_queries(codes)
+    hdr = (C.c_char_p * len(sequences))(*[s.header().encode() for s in sequences])
+    opts = L.HfmBuildOpts(config.sa_sample_rate, config.lookup_depth, tag, config.occ_encoding, 1)
+    out = L.u8p()
+    n = C.c_size_t()
+    L.check(L.lib().hfm_build_index_gpu(L.ptr(flat, L.u8p), L.ptr(off, L.u64p), len(sequences), hdr, C.byref(opts),
+                                        kind, device, C.byref(out), C.byref(n)))
+    try:
+        data = C.string_at(out, n.value)
+    finally:
+        L.lib().hfm_free(out)
+    return data
+
+
 class _Handle:
     """Owns one device-resident index (hfm_index*)."""
 

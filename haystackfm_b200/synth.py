@@ -172,6 +172,31 @@ def _mutate(seq: np.ndarray, rate: float, rng) -> np.ndarray:
     return res
 
 
+def _mutate_many(cat: np.ndarray, seg: np.ndarray, rate: float, rng):
+    """_mutate over many sequences at once (`cat`: their concatenation, `seg`: their
+    lengths).  -> (concatenated results, result lengths)."""
+    n = len(cat)
+    ev = rng.random(n, dtype=np.float32)
+    kind = rng.integers(0, 3, size=n, dtype=np.uint8)
+    shift = rng.integers(1, 4, size=n, dtype=np.uint8)
+    hit = ev < rate
+    sub = hit & (kind == 0)
+    ins = hit & (kind == 1)
+    dele = hit & (kind == 2)
+    out = cat.copy()
+    out[sub] = ((out[sub] - 1 + shift[sub]) % 4) + 1
+    reps = np.ones(n, dtype=np.int8)
+    reps[dele] = 0
+    reps[ins] = 2
+    res = np.repeat(out, reps)
+    ends = np.cumsum(reps, dtype=np.int64)
+    pos = ends[ins] - 1                      # the second copy of each inserted base
+    res[pos] = rng.integers(1, 5, size=len(pos), dtype=np.uint8)
+    bounds = np.cumsum(seg)
+    rl = np.diff(np.concatenate([[0], ends[bounds - 1]]))
+    return res, rl
+
+
 def sample_mixed_reads(ref: Reference, n_reads=200_000, short_frac=0.8, short_len=150, long_median=3000,
                        long_sigma=0.6, min_len=100, max_len=10_000, short_sub=0.01, long_err=0.08,
                        n_rate=0.001, seed=5, avoid_masked=False):
@@ -218,14 +243,26 @@ def sample_mixed_reads(ref: Reference, n_reads=200_000, short_frac=0.8, short_le
     rows = np.where(sub, ((rows - 1 + shift) % 4) + 1, rows).astype(np.uint8)
     for k, i in enumerate(sh):
         out[i] = rows[k]
-    for i in np.nonzero(is_long)[0]:
-        s = ref.truth[cid[i]][starts[i]:starts[i] + src_len[i]]
-        if rc[i]:
-            s = (5 - s)[::-1]
-        out[i] = _mutate(np.ascontiguousarray(s), long_err, rng)[:lens[i]]
+    # long reads: source spans (reverse-complemented where drawn), then mixed errors, in
+    # vectorised chunks of reads
+    li = np.nonzero(is_long)[0]
+    chunk = 4_000
+    for a in range(0, len(li), chunk):
+        idx = li[a:a + chunk]
+        srcs = [ref.truth[cid[i]][starts[i]:starts[i] + src_len[i]] for i in idx]
+        srcs = [x[::-1] if rc[i] else x for x, i in zip(srcs, idx)]
+        cat = np.concatenate(srcs).astype(np.uint8)
+        seg = src_len[idx].astype(np.int64)
+        flip = np.repeat(rc[idx], seg)
+        cat = np.where(flip, 5 - cat, cat).astype(np.uint8)
+        res, rl = _mutate_many(cat, seg, long_err, rng)
+        roff = np.concatenate([[0], np.cumsum(rl)])
+        for k, i in enumerate(idx):
+            out[i] = res[roff[k]:roff[k] + min(int(rl[k]), int(lens[i]))]
     lens = np.array([len(s) for s in out], dtype=np.int64)
     flat = np.concatenate(out).astype(np.uint8) if out else np.zeros(0, np.uint8)
-    flat[rng.random(len(flat)) < n_rate] = N
+    if n_rate > 0:
+        flat[rng.random(len(flat)) < n_rate] = N
     off = np.zeros(n_reads + 1, dtype=np.uint64)
     np.cumsum(lens, out=off[1:])
     return flat, off, lens

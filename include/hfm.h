@@ -28,7 +28,7 @@ extern "C" {
 #define HFM_E_OOM (-2)      /* device or host allocation failed                             */
 #define HFM_E_FORMAT (-3)   /* bad bincode / alphabet tag / inconsistent index (DeserializeError) */
 #define HFM_E_ARG (-4)      /* invalid argument                                             */
-#define HFM_E_TIMEOUT (-5)  /* device watchdog expired                                      */
+#define HFM_E_TIMEOUT (-5)  /* the handle's deadline (hfm_set_timeout) passed while waiting    */
 #define HFM_E_OVERFLOW (-6) /* a per-read work set outgrew the largest fallback capacity     */
 #define HFM_E_WALK (-7)     /* an LF walk exceeded sample_rate steps (index inconsistent)   */
 
@@ -118,6 +118,16 @@ int hfm_build_index(const uint8_t* codes, const uint64_t* seq_off, uint32_t nseq
                     const char* const* headers, const hfm_build_opts* opts, int kind,
                     uint8_t** bytes_out, size_t* len_out);
 
+/* The same bytes as hfm_build_index, built on GPU `device` (replaces FmIndex::build /
+ * BidirFmIndex::build, src/fm_index/mod.rs:209-284, src/fm_index/bidir_index.rs:91-116,
+ * whose wgpu build is IUPAC-only with a 16-lane Occ table and no lookup table; this one
+ * keeps build_cpu_with's contract).  Suffixes are sorted by prefix doubling over a device
+ * radix sort; BWT, Occ records, sampled SA and lookup table are built on the device.
+ * Needs about 39 bytes of device memory per text position while sorting. */
+int hfm_build_index_gpu(const uint8_t* codes, const uint64_t* seq_off, uint32_t nseq,
+                        const char* const* headers, const hfm_build_opts* opts, int kind, int device,
+                        uint8_t** bytes_out, size_t* len_out);
+
 /* ---- index load / free (replaces FmIndex::from_bytes / BidirFmIndex::from_bytes,
  *      src/fm_index/serialize.rs:32-52, src/fm_index/bidir_index.rs:195-210, and the
  *      per-call uploads of src/gpu/locate.rs:69-111, src/gpu/mem_find.rs:56-102,
@@ -149,7 +159,12 @@ int hfm_mems_batch(hfm_index* idx, const uint8_t* q, const uint64_t* q_off, uint
 
 /* ---- queries, device buffers (reads already resident in HBM) -------------
  * Same semantics as above.  d_q / d_q_off are device pointers; results are written to
- * device memory owned by the handle and stay valid until the next call on it. */
+ * device memory owned by the handle and stay valid until the next call on it.
+ * Ordering: every call runs on the handle's own stream (created non-blocking, so it does
+ * not wait for the legacy default stream or for any stream of the caller).  Device inputs
+ * and caller-owned device outputs must be complete before the call is made (synchronize
+ * the stream that wrote them); the call returns after its device work has finished, so
+ * its outputs are ready for any stream when it returns. */
 typedef struct hfm_dev_hits {
   uint32_t nq; uint32_t _pad; uint64_t total;
   uint64_t* d_offsets; uint32_t* d_counts; uint32_t* d_pairs;
@@ -249,10 +264,18 @@ void* hfm_index_stream(hfm_index* idx);    /* the handle's cudaStream_t (for eve
 int hfm_last_stats(const hfm_index* idx, hfm_stats* out);
 int hfm_set_counters(hfm_index* idx, int enable);  /* per-read work counters on/off (default off) */
 
+/* Host-side deadline for the waits inside every call on the handle (no counterpart in the
+ * reference, whose wgpu calls block without a limit; it stands in for the device watchdog
+ * of FmIndexError::GpuError).  ms = 0 (default): wait without a limit.  When a wait passes
+ * the deadline the call returns HFM_E_TIMEOUT at once: its outputs are undefined and a
+ * device-to-host copy it issued may still land in its output later (hfm_count_batch's
+ * counts_out included) until the next call on the handle, which first drains the abandoned
+ * work; the handle stays usable. */
+int hfm_set_timeout(hfm_index* idx, uint32_t ms);
+
 /* Tunable parameters of the SMEM/MEM search and their autotuner (no counterpart in the
- * reference).  mems_variant: fast pass with 32-entry candidate lists in local memory at 5,
- * 6 or 8 resident blocks per SM (0, 1, 2) or 1024-entry lists in global memory at 8 blocks
- * (3, default).  seg_len: SMEM reads longer than 2*seg_len are swept in seg_len-position
+ * reference).  mems_variant: fast pass with 32-entry candidate lists in local memory (2)
+ * or 1024-entry lists in global memory (3, default), 8 resident blocks per SM.  seg_len: SMEM reads longer than 2*seg_len are swept in seg_len-position
  * segments (multiple of 32 in 64..4096, default 512).  Results never depend on them.
  * hfm_autotune_mems times the search of a sample batch under each candidate setting
  * (variant 3 with seg_len 512, 256, 1024; variant 2), best of `reps` runs after a warm-up

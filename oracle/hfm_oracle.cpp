@@ -707,6 +707,127 @@ static std::vector<uint32_t> naive_sa(const std::vector<uint8_t>& t) {
   return sa;
 }
 
+// Parallel LSD radix sort of (key, value) pairs on the low `bits` bits of the keys; passes
+// whose digit is the same for every key are skipped.
+static void radix_sort_pairs(std::vector<uint64_t>& key, std::vector<uint32_t>& val, int bits, int threads) {
+  const uint64_t n = key.size();
+  std::vector<uint64_t> k2(n);
+  std::vector<uint32_t> v2(n);
+  threads = std::max(1, std::min<int>(threads, (int)std::max<uint64_t>(1, n >> 16)));
+  const uint64_t per = (n + threads - 1) / threads;
+  std::vector<uint64_t> hist((size_t)threads * 256);
+  for (int shift = 0; shift < bits; shift += 8) {
+    std::fill(hist.begin(), hist.end(), 0);
+    std::vector<std::thread> th;
+    for (int t = 0; t < threads; t++)
+      th.emplace_back([&, t] {
+        uint64_t a = t * per, b = std::min(n, a + per);
+        uint64_t* h = &hist[(size_t)t * 256];
+        for (uint64_t i = a; i < b; i++) h[(key[i] >> shift) & 255]++;
+      });
+    for (auto& x : th) x.join();
+    th.clear();
+    int nonzero = 0;
+    for (int d = 0; d < 256; d++) {
+      uint64_t s = 0;
+      for (int t = 0; t < threads; t++) s += hist[(size_t)t * 256 + d];
+      nonzero += s != 0;
+    }
+    if (nonzero <= 1) continue;                  // every key has this digit
+    uint64_t run = 0;                            // digit-major, thread-minor offsets: stable
+    for (int d = 0; d < 256; d++)
+      for (int t = 0; t < threads; t++) { uint64_t c = hist[(size_t)t * 256 + d]; hist[(size_t)t * 256 + d] = run; run += c; }
+    for (int t = 0; t < threads; t++)
+      th.emplace_back([&, t] {
+        uint64_t a = t * per, b = std::min(n, a + per);
+        uint64_t* h = &hist[(size_t)t * 256];
+        for (uint64_t i = a; i < b; i++) {
+          uint64_t o = h[(key[i] >> shift) & 255]++;
+          k2[o] = key[i]; v2[o] = val[i];
+        }
+      });
+    for (auto& x : th) x.join();
+    key.swap(k2); val.swap(v2);
+  }
+}
+
+// Suffix array by prefix doubling (Manber & Myers 1993, refining only the groups that are
+// still tied, as Larsson & Sadakane 2007 do).  It is an algorithm independent of the
+// product's SA-IS builder, so an index built here checks that builder at scale.  The
+// order is true lexicographic order of the code slices with a proper prefix first — the
+// order of build_suffix_array_naive (src/suffix_array/cpu.rs:20-25), which `naive_sa`
+// above computes by comparison; the two are compared in the oracle's own tests.
+static std::vector<uint32_t> doubling_sa(const std::vector<uint8_t>& t, int threads) {
+  const uint64_t n = t.size();
+  std::vector<uint32_t> sa(n);
+  if (n == 0) return sa;
+  threads = std::max(1, threads);
+  constexpr int K = 12;                          // 12 symbols of 5 bits: code + 1, 0 past the end
+  std::vector<uint64_t> key(n);
+  auto par = [&](uint64_t m, auto f) {
+    int nt = (int)std::min<uint64_t>((uint64_t)threads, std::max<uint64_t>(1, m >> 14));
+    uint64_t per = (m + nt - 1) / nt;
+    std::vector<std::thread> th;
+    for (int q = 0; q < nt; q++) th.emplace_back([&, q] { f(q * per, std::min(m, q * per + per)); });
+    for (auto& x : th) x.join();
+  };
+  par(n, [&](uint64_t a, uint64_t b) {
+    for (uint64_t i = a; i < b; i++) {
+      uint64_t k = 0;
+      for (int j = 0; j < K; j++) k = (k << 5) | (i + j < n ? (uint64_t)t[i + j] + 1 : 0);
+      key[i] = k; sa[i] = (uint32_t)i;
+    }
+  });
+  radix_sort_pairs(key, sa, 5 * K, threads);
+  // rank = 1 + index of the last member of the suffix's group (0 is "past the end")
+  std::vector<uint32_t> rank(n);
+  std::vector<std::pair<uint32_t, uint32_t>> groups;   // [a, b) still tied
+  {
+    uint64_t a = 0;
+    for (uint64_t j = 1; j <= n; j++)
+      if (j == n || key[j] != key[a]) {
+        for (uint64_t q = a; q < j; q++) rank[sa[q]] = (uint32_t)j;
+        if (j - a > 1) groups.push_back({(uint32_t)a, (uint32_t)j});
+        a = j;
+      }
+  }
+  std::vector<uint64_t>().swap(key);
+  std::vector<uint32_t> next_rank;
+  for (uint64_t h = K; !groups.empty(); h *= 2) {
+    next_rank = rank;                            // reads use this round's ranks only
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> out(threads);
+    std::atomic<size_t> gi{0};
+    std::vector<std::thread> th;
+    for (int q = 0; q < threads; q++)
+      th.emplace_back([&, q] {
+        std::vector<std::pair<uint32_t, uint32_t>> tmp;
+        for (size_t g; (g = gi.fetch_add(1)) < groups.size();) {
+          uint32_t a = groups[g].first, b = groups[g].second;
+          tmp.clear();
+          for (uint32_t j = a; j < b; j++) {
+            uint64_t i = sa[j];
+            tmp.push_back({i + h < n ? rank[i + h] : 0u, (uint32_t)i});
+          }
+          std::sort(tmp.begin(), tmp.end());
+          uint32_t s = 0;
+          for (uint32_t j = 1; j <= b - a; j++)
+            if (j == b - a || tmp[j].first != tmp[s].first) {
+              for (uint32_t u = s; u < j; u++) { sa[a + u] = tmp[u].second; next_rank[tmp[u].second] = a + j; }
+              if (j - s > 1) out[q].push_back({a + s, a + j});
+              s = j;
+            }
+        }
+      });
+    for (auto& x : th) x.join();
+    rank.swap(next_rank);
+    groups.clear();
+    for (auto& o : out) groups.insert(groups.end(), o.begin(), o.end());
+  }
+  return sa;
+}
+
+static int g_build_threads = 1;   // threads of the oracle's index construction
+
 static FmIndex build_fm(const std::vector<uint8_t>& text, const std::vector<uint32_t>& bounds,
                         const std::vector<std::string>& headers, uint32_t rate, uint32_t lookup_depth,
                         uint8_t tag, uint32_t encoding) {
@@ -717,7 +838,7 @@ static FmIndex build_fm(const std::vector<uint8_t>& text, const std::vector<uint
   f.seq_boundaries = bounds;
   f.headers = headers;
   f.c = CArray::from_text(text);
-  std::vector<uint32_t> sa = naive_sa(text);
+  std::vector<uint32_t> sa = doubling_sa(text, g_build_threads);
   uint64_t n = text.size();
   std::vector<uint8_t> bwt(n);
   for (uint64_t i = 0; i < n; i++) bwt[i] = text[sa[i] == 0 ? n - 1 : sa[i] - 1];
@@ -1074,5 +1195,16 @@ int orc_suffix_array(const uint8_t* t, uint64_t n, uint32_t* out) {
   std::memcpy(out, sa.data(), n * 4);
   return 0;
 }
+
+// The prefix-doubling sorter that orc_build uses (checked against orc_suffix_array).
+int orc_suffix_array_doubling(const uint8_t* t, uint64_t n, uint32_t* out, int threads) {
+  std::vector<uint8_t> v(t, t + n);
+  std::vector<uint32_t> sa = doubling_sa(v, threads);
+  if (n) std::memcpy(out, sa.data(), n * 4);
+  return 0;
+}
+
+// Host threads of orc_build's suffix sort (default 1).
+void orc_set_build_threads(int threads) { g_build_threads = std::max(1, threads); }
 
 }  // extern "C"

@@ -60,6 +60,8 @@ def lib():
         L.orc_smem_segment_check.argtypes = [C.c_void_p, u8p, u64p, C.c_uint32, C.c_uint32, C.c_uint32,
                                              u32p, u32p]
         L.orc_suffix_array.argtypes = [u8p, C.c_uint64, u32p]
+        L.orc_suffix_array_doubling.argtypes = [u8p, C.c_uint64, u32p, C.c_int]
+        L.orc_set_build_threads.argtypes = [C.c_int]
         _lib = L
     return _lib
 
@@ -93,7 +95,7 @@ def pack_queries(queries):
 
 
 def build_index_bytes(seqs, *, rate=32, lookup_depth=0, tag=0, encoding=0, kind=0, headers=None) -> bytes:
-    """Oracle construction (naive suffix sort): FmIndex (kind 0) or BidirFmIndex (kind 1) bincode."""
+    """Oracle construction (prefix-doubling suffix sort): FmIndex (kind 0) or BidirFmIndex (kind 1) bincode."""
     flat, off = pack_queries(seqs)
     hdr = None
     if headers is not None:
@@ -110,10 +112,24 @@ def build_index_bytes(seqs, *, rate=32, lookup_depth=0, tag=0, encoding=0, kind=
 
 
 def suffix_array(codes) -> np.ndarray:
+    """Comparison sort of the suffixes (build_suffix_array_naive)."""
     t = np.ascontiguousarray(codes, dtype=np.uint8)
     out = np.zeros(len(t), dtype=np.uint32)
     lib().orc_suffix_array(_p(t, u8p), len(t), _p(out, u32p))
     return out
+
+
+def suffix_array_doubling(codes, threads: int = 1) -> np.ndarray:
+    """The prefix-doubling sorter that the oracle's index construction uses."""
+    t = np.ascontiguousarray(codes, dtype=np.uint8)
+    out = np.zeros(len(t), dtype=np.uint32)
+    lib().orc_suffix_array_doubling(_p(t, u8p), len(t), _p(out, u32p), int(threads))
+    return out
+
+
+def set_build_threads(threads: int) -> None:
+    """Host threads of the oracle's suffix sort during index construction."""
+    lib().orc_set_build_threads(int(threads))
 
 
 class OracleIndex:

@@ -121,3 +121,28 @@ def test_null_arguments_rejected_without_a_gpu():
     assert lib.hfm_last_error()                               # a message was set
     lib.hfm_mlp_free(None)                                    # no-ops
     assert lib.hfm_mlp_stream(None) in (None, 0)
+
+
+def test_oracle_doubling_sort_equals_comparison_sort(oracle):
+    """The oracle builds its indices with a prefix-doubling suffix sort (an algorithm
+    independent of the product's SA-IS); it must give the comparison sort's order on texts
+    with interior sentinels, long runs and periodic stretches."""
+    rng = np.random.default_rng(13)
+    for trial in range(120):
+        n = int(rng.integers(1, 600))
+        kind = trial % 4
+        if kind == 0:
+            t = rng.integers(0, 16, n).astype(np.uint8)
+        elif kind == 1:
+            t = rng.integers(0, 3, n).astype(np.uint8)
+        elif kind == 2:
+            t = np.full(n, int(rng.integers(0, 16)), np.uint8)
+        else:
+            t = np.tile(rng.integers(0, 5, int(rng.integers(1, 9))).astype(np.uint8), n)[:n]
+        want = oracle.suffix_array(t)
+        for threads in (1, 3):
+            assert np.array_equal(oracle.suffix_array_doubling(t, threads), want), (trial, threads)
+
+
+def test_null_handle_timeout_rejected():
+    assert L.lib().hfm_set_timeout(None, 5) == HFM_E_ARG

@@ -1,0 +1,56 @@
+"""GPU index construction (hfm_build_index_gpu) against the CPU builder: the bincode bytes
+must be identical — suffix order, BWT, compacted Occ records, sampled SA with forced
+sequence starts, lookup table — for both alphabets, both Occ encodings and both index
+kinds, on texts with many sequences, long runs and periodic stretches."""
+from __future__ import annotations
+
+import random
+
+import numpy as np
+import pytest
+
+from haystackfm_b200 import alphabet as al
+from haystackfm_b200 import synth
+from haystackfm_b200.fm_index import FmIndexConfig, KIND_BIDIR, KIND_FM, _build, _build_gpu
+
+pytestmark = pytest.mark.gpu
+
+
+def _both(contigs, rate, lookup, tag, enc, kind):
+    seqs = [al.DnaSequence(np.asarray(c, dtype=np.uint8)) for c in contigs]
+    cfg = FmIndexConfig(sa_sample_rate=rate, lookup_depth=lookup, occ_encoding=enc, build_threads=2)
+    return _build(seqs, cfg, tag, kind), _build_gpu(seqs, cfg, tag, kind)
+
+
+def test_gpu_builder_bytes_equal_cpu_builder_small():
+    rng = random.Random(7)
+    for trial in range(40):
+        alphabet = rng.choice([[1, 2, 3, 4], [1, 2, 3, 4, 5], list(range(1, 16)), [1], [1, 2]])
+        tag = 1 if max(alphabet) <= 4 and rng.random() < 0.5 else 0
+        contigs = []
+        for _ in range(rng.randint(1, 6)):
+            n = rng.randint(1, 700)
+            kind = rng.random()
+            if kind < 0.2:
+                c = [rng.choice(alphabet)] * n                            # a run
+            elif kind < 0.4:
+                unit = [rng.choice(alphabet) for _ in range(rng.randint(1, 9))]
+                c = (unit * (n // len(unit) + 1))[:n]                     # periodic
+            else:
+                c = [rng.choice(alphabet) for _ in range(n)]
+            contigs.append(c)
+        rate = rng.choice([1, 2, 7, 32])
+        lookup = rng.choice([0, 0, 2, 5])
+        enc = rng.choice([0, 1])
+        kind = rng.choice([KIND_FM, KIND_BIDIR])
+        cpu, gpu = _both(contigs, rate, lookup, tag, enc, kind)
+        assert gpu == cpu, (trial, rate, lookup, tag, enc, kind)
+
+
+def test_gpu_builder_bytes_equal_cpu_builder_genomes():
+    ref = synth.iupac_reference(total=3_000_000, n_contigs=30, seed=61)
+    cpu, gpu = _both(ref.contigs, 32, 10, 0, 0, KIND_BIDIR)
+    assert gpu == cpu
+    rep = synth.repeat_reference(total=3_000_000, n_contigs=6, seed=62)
+    cpu, gpu = _both(rep.contigs, 32, 10, 1, 0, KIND_BIDIR)
+    assert gpu == cpu

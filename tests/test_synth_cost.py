@@ -64,3 +64,24 @@ def test_work_targets_and_errors():
     assert np.allclose(e.mae, 0) and np.allclose(e.r2, 1) and abs(e.spearman_touches - 1) < 1e-9
     e2 = prediction_error(-y, y)
     assert e2.spearman_touches < 0
+
+
+def test_device_generators_shapes_and_seeding():
+    """The genome-scale generators (run here on the CPU device): ACGT-only repeat genome
+    with shared 16-mers, reads with the stated error model, seeded."""
+    from haystackfm_b200 import synth_gpu as sg
+    g, b = sg.repeat_genome(total=3_000_000, n_contigs=5, seed=3, device="cpu")
+    assert g.shape[0] == 3_000_000 and int(b[-1]) == 3_000_000 and len(b) == 5
+    assert int(g.min()) >= 1 and int(g.max()) <= 4
+    uniform = np.random.default_rng(3).integers(1, 5, size=3_000_000, dtype=np.uint8)
+    assert _dup_fraction(g.numpy()) > 10 * max(_dup_fraction(uniform), 1e-4)
+    g2, _ = sg.repeat_genome(total=3_000_000, n_contigs=5, seed=3, device="cpu")
+    assert torch.equal(g, g2)
+    r = sg.sample_reads(g, b, 4000, seed=4)
+    assert r.shape == (4000, 150) and 0.0003 < float((r == 5).float().mean()) < 0.003
+    flat, off = sg.sample_mixed_reads(g, b, 3000, seed=5)
+    lens = torch.diff(off).numpy()
+    assert int(off[-1]) == flat.shape[0] and 0.75 < (lens == 150).mean() < 0.85
+    assert lens.max() <= 10_000 and 2000 < np.median(lens[lens != 150]) < 4500
+    f2, o2 = sg.sample_mixed_reads(g, b, 3000, seed=5)
+    assert torch.equal(flat, f2) and torch.equal(off, o2)
