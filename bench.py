@@ -62,8 +62,14 @@ def parse():
     ap.add_argument("--train-reads", type=int, default=1_000_000,
                     help="reads (a separate seeded sample) whose logged work trains the cost model")
     ap.add_argument("--train-epochs", type=int, default=4)
-    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-length workload")
-    ap.add_argument("--mixed-reads", type=int, default=200_000)
+    ap.add_argument("--no-genome", action="store_true", help="skip the 3.1 Gbp genome workloads")
+    ap.add_argument("--no-plain-launch", action="store_true", help="skip timing the plain launch baseline")
+    ap.add_argument("--genome-len", type=int, default=3_100_000_000)
+    ap.add_argument("--genome-reads", type=int, default=2_000_000, help="mixed-length reads (uneven, training)")
+    ap.add_argument("--eval-reads", type=int, default=10_000_000, help="held-out 150 bp reads")
+    ap.add_argument("--eval-mixed", type=int, default=1_000_000, help="held-out mixed-length reads")
+    ap.add_argument("--genome-steps", type=int, default=2)
+    ap.add_argument("--genome-parity", type=int, default=2048, help="reads per set checked against the oracle")
     ap.add_argument("--no-serving", action="store_true", help="skip the batch-latency measurement")
     ap.add_argument("--serving-batches", type=int, default=300)
     ap.add_argument("--profile-smem", action="store_true",
@@ -339,85 +345,155 @@ def serving_latency(h, lib, L, kp, rp, bounds, n, n_batches, seed=17):
             "path": "hfm_locate_batch + hfm_mems_batch, host buffers, one handle, back to back"}
 
 
-def mixed_workload(args, device, torch):
-    """Mixed-length reads (80% 150 bp, 20% lognormal median 3 kbp up to 10 kbp, 8% indel
-    errors) on an ACGT-only 100 Mbp genome with repeat families and tandem repeats
-    (ExactDna bidirectional index, rate 32, lookup 10): locate of each read's first 32-mer +
-    find_smems (min_len 19, max_hits 1024), plain order vs the learned schedule."""
-    from haystackfm_b200 import alphabet as al, synth
+def genome_workloads(args, device, torch):
+    """configs[2] and configs[3] on a 3.1 Gbp repeat-rich ACGT genome (ExactDna
+    bidirectional index, sa_sample_rate 32, lookup_depth 10, built on the GPU):
+
+    * uneven: 2M mixed-length reads, find_smems (min_len 19, max_hits 1024, positions
+      mapped): the persistent work-queue path (autotuned) against the plain
+      one-thread-per-read launch with its count pass;
+    * learned: the read-cost model trained on the work the exact kernel logs for those
+      2M reads, evaluated on 10M held-out 150 bp reads and 1M held-out mixed-length reads:
+      prediction error, and the learned path (outputs pre-sized from the predicted totals,
+      binned order when it is faster) against the plain launch, outputs compared byte for
+      byte;
+    * parity: outputs for a read subsample against the CPU oracle on the same index bytes."""
+    from haystackfm_b200 import alphabet as al
+    from haystackfm_b200 import synth_gpu as sg
     from haystackfm_b200 import _lib as L
     from haystackfm_b200.cost_model import LearnedSmem, prediction_error, work_targets
-    from haystackfm_b200.fm_index import BidirFmIndex, FmIndexConfig, KIND_BIDIR, _build
+    from haystackfm_b200.fm_index import BidirFmIndex, FmIndexConfig, KIND_BIDIR, _build_gpu
+    from haystackfm_b200.fm_index import device_to_host as d2h
+    dev = torch.device("cuda", device)
+    out = {"genome": f"{args.genome_len / 1e9:.2f} Gbp ACGT, 24 contigs, 40% interspersed repeats (20 families, "
+                     f"300 bp / 6 kbp consensus, 10-20% divergent copies), 5% tandem repeats (period 2-60)",
+           "alphabet": "ExactDna", "sa_sample_rate": 32, "lookup_depth": 10, "min_len": 19, "max_hits_per_mem": 1024,
+           "data": "synthetic, generated on the GPU (haystackfm_b200/synth_gpu.py, seeds 11/21/22/23)"}
     t0 = time.time()
-    ref = synth.repeat_reference(total=args.ref_len, seed=11)
-    key = hashlib.sha1(f"repeat-v1-{args.ref_len}-11-exact-rate32-lut10".encode()).hexdigest()[:16]
-    path = os.path.join(tempfile.gettempdir(), "hfm_bench_cache", key + ".bin")
-    if os.path.exists(path):
-        data = open(path, "rb").read()
-    else:
-        data = _build([al.DnaSequence(c) for c in ref.contigs],
-                      FmIndexConfig(sa_sample_rate=32, lookup_depth=10, build_threads=2), 1, KIND_BIDIR)
-        tmp = path + f".{os.getpid()}"
-        with open(tmp, "wb") as f:
-            f.write(data)
-        os.replace(tmp, path)
+    genome, gb = sg.repeat_genome(total=args.genome_len, n_contigs=24, seed=11, device=dev)
+    r3_q, r3_o = sg.sample_mixed_reads(genome, gb, args.genome_reads, seed=21)
+    e150 = sg.sample_reads(genome, gb, args.eval_reads, n_rate=0.0, seed=22)
+    em_q, em_o = sg.sample_mixed_reads(genome, gb, args.eval_mixed, seed=23)
+    host = genome.cpu().numpy()
+    del genome
+    torch.cuda.synchronize()
+    out["synth_s"] = round(time.time() - t0, 1)
+    begins = np.concatenate([[0], gb[:-1]])
+    seqs = [al.DnaSequence(host[a:b]) for a, b in zip(begins, gb)]
+    torch.cuda.empty_cache()
+    t0 = time.time()
+    data = _build_gpu(seqs, FmIndexConfig(sa_sample_rate=32, lookup_depth=10), 1, KIND_BIDIR, device=device)
+    out["index_build_s"] = round(time.time() - t0, 1)
+    out["index_bytes"] = len(data)
+    out["index_sha256"] = hashlib.sha256(data).hexdigest()
+    del seqs, host
+    t0 = time.time()
     idx = BidirFmIndex.from_bytes(data, device=device)
+    out["index_load_s"] = round(time.time() - t0, 1)
     h = idx.handle
     lib = L.lib()
     bounds = np.ascontiguousarray(idx.seq_boundaries(), dtype=np.uint32)
     nb = len(bounds)
-    m = args.mixed_reads
-    flat, off, lens = synth.sample_mixed_reads(ref, n_reads=m, seed=5, n_rate=0.0)
-    flat_t, off_t, _ = synth.sample_mixed_reads(ref, n_reads=m, seed=6, n_rate=0.0)
-    dev = torch.device("cuda", device)
-    q = torch.from_numpy(flat).to(dev)
-    o = torch.from_numpy(off.view(np.int64)).to(dev)
-    k32 = torch.from_numpy(np.ascontiguousarray(np.stack([flat[int(a):int(a) + 32] for a in off[:-1]]))
-                           .reshape(-1)).to(dev)
-    o32 = torch.arange(0, (m + 1) * 32, 32, dtype=torch.int64, device=dev)
-    setup_s = time.time() - t0
-    ls = LearnedSmem(h, device, seed=1)
-    qt = torch.from_numpy(flat_t).to(dev)
-    ot = torch.from_numpy(off_t.view(np.int64)).to(dev)
-    tuning = h.autotune_mems(qt, ot, m, 19, 0, bounds, 1024, reps=1)     # on the training reads
-    losses, _, _ = ls.fit(qt, ot, m, 19, 0, bounds, 1024, epochs=8, batch=4096, lr=1e-3)
-    del qt, ot
-    ev_log = ls.log_work(q, o, m, 19, 0, bounds, 1024)
-    _, _, y = ls.plan(q, o, m)
-    err = prediction_error(y, work_targets(ev_log)).as_dict()
-    del ev_log
-
-    def step(learned):
-        dh = L.HfmDevHits()
-        L.check(lib.hfm_locate_batch_device(h.h, k32.data_ptr(), o32.data_ptr(), m, 1024, C.byref(dh)))
-        if learned:
-            ls.run(q, o, m, 19, 0, L.ptr(bounds, L.u32p), nb, 1024)
-        else:
-            dm = L.HfmDevMems()
-            L.check(lib.hfm_mems_batch_device(h.h, q.data_ptr(), o.data_ptr(), m, 19, 0, L.ptr(bounds, L.u32p), nb,
-                                              1024, C.byref(dm)))
-
+    bp = L.ptr(bounds, L.u32p)
     stream = torch.cuda.ExternalStream(h.stream(), device=dev)
-    res = {}
-    for name, learned in (("plain", False), ("learned", True)):
-        for _ in range(max(args.warmup, 3)):
-            step(learned)
+
+    def timed(fn, steps, warmup=1):
+        for _ in range(warmup):
+            fn()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
-            step(learned)
+        for _ in range(steps):
+            fn()
         e1.record(stream)
         torch.cuda.synchronize()
-        res[name] = e0.elapsed_time(e1) / args.steps
-    return {"workload": "mixed_length_repeats_locate_smem", "reads": m, "read_mbp": round(len(flat) / 1e6, 1),
-            "genome": f"{args.ref_len // 1_000_000} Mbp ACGT, 40% interspersed repeats, 5% tandem repeats",
-            "alphabet": "ExactDna", "setup_s": round(setup_s, 1), "autotuned": tuning,
-            "plain_ms_per_step": res["plain"], "plain_reads_per_s": m / (res["plain"] / 1000),
-            "learned_ms_per_step": res["learned"], "learned_reads_per_s": m / (res["learned"] / 1000),
-            "learned_enabled": bool(ls.enabled), "calibration": ls.calibration,
-            "holdout_error": ls.holdout_error.as_dict() if ls.holdout_error else None, "eval_error": err,
-            "train_mse": [round(float(v), 4) for v in losses]}
+        return e0.elapsed_time(e1) / steps
+
+    def mems(q, o, n):
+        dm = L.HfmDevMems()
+        L.check(lib.hfm_mems_batch_device(h.h, q.data_ptr(), o.data_ptr(), n, 19, 0, bp, nb, 1024, C.byref(dm)))
+        return dm
+
+    def with_tuning(variant, fn):
+        saved = h.tuning()
+        h.set_tuning(variant, saved["seg_len"])
+        try:
+            return fn()
+        finally:
+            h.set_tuning(saved["mems_variant"], saved["seg_len"])
+
+    n3 = args.genome_reads
+    steps = args.genome_steps
+    tuning = h.autotune_mems(r3_q, r3_o, n3, 19, 0, bounds, 1024, reps=1)
+    ms_persist = timed(lambda: mems(r3_q, r3_o, n3), steps)
+    ms_plain = with_tuning(4, lambda: timed(lambda: mems(r3_q, r3_o, n3), steps))
+    out["uneven"] = {"reads": n3, "read_bases": int(r3_o[-1].item()),
+                     "mix": "80% 150 bp (1% substitutions), 20% lognormal median 3 kbp up to 10 kbp (8% subs/indels)",
+                     "persistent_ms": round(ms_persist, 2), "persistent_reads_per_s": n3 / (ms_persist / 1e3),
+                     "plain_launch_ms": round(ms_plain, 2), "plain_launch_reads_per_s": n3 / (ms_plain / 1e3),
+                     "speedup_vs_plain_launch": round(ms_plain / ms_persist, 3), "autotuned": tuning}
+    # learned: train on the logged work of the 2M reads, evaluate on held-out reads
+    ls = LearnedSmem(h, device, seed=1)
+    t0 = time.time()
+    losses, _, _ = ls.fit(r3_q, r3_o, n3, 19, 0, bounds, 1024, epochs=args.train_epochs, batch=8192, lr=1e-3)
+    learned = {"train_reads": n3, "epochs": args.train_epochs, "fit_s": round(time.time() - t0, 1),
+               "train_mse": [round(float(v), 4) for v in losses],
+               "holdout_error": ls.holdout_error.as_dict() if ls.holdout_error else None,
+               "order_enabled": bool(ls.enabled), "calibration": ls.calibration, "presize": True}
+    o150 = torch.arange(0, (args.eval_reads + 1) * 150, 150, dtype=torch.int64, device=dev)
+    q150 = e150.reshape(-1)
+    for name, (q, o, n) in (("eval_150bp", (q150, o150, args.eval_reads)),
+                            ("eval_mixed", (em_q, em_o, args.eval_mixed))):
+        log = ls.log_work(q, o, n, 19, 0, bounds, 1024)
+        _, _, y = ls.plan(q, o, n)
+        err = prediction_error(y, work_targets(log)).as_dict()
+        del log
+        ms_l = timed(lambda: ls.run(q, o, n, 19, 0, bp, nb, 1024), steps)
+        dm = ls.run(q, o, n, 19, 0, bp, nb, 1024)
+        got = device_mems_tensors(torch, dev, dm, n, clone=True)
+        ms_pl = with_tuning(4, lambda: timed(lambda: mems(q, o, n), steps))
+        dm = with_tuning(4, lambda: mems(q, o, n))
+        ref = device_mems_tensors(torch, dev, dm, n, clone=False)
+        eq = all(a.shape == b.shape and bool(torch.equal(a, b)) for a, b in zip(got, ref))
+        ms_p = timed(lambda: mems(q, o, n), steps)
+        learned[name] = {"reads": n, "prediction_error": err, "learned_ms": round(ms_l, 2),
+                         "learned_reads_per_s": n / (ms_l / 1e3), "plain_launch_ms": round(ms_pl, 2),
+                         "persistent_unlearned_ms": round(ms_p, 2),
+                         "speedup_vs_plain_launch": round(ms_pl / ms_l, 3),
+                         "speedup_vs_persistent_unlearned": round(ms_p / ms_l, 3),
+                         "outputs_equal_to_plain_launch": eq, "mem_hits": int(dm.n_hits),
+                         "mem_positions": int(dm.n_positions)}
+        del got, ref
+    out["learned"] = learned
+    # parity subsample against the oracle (CPU) on the same index bytes
+    if not args.no_cpu_baseline and args.genome_parity > 0:
+        from oracle import oracle as orc
+        orc.build()
+        t0 = time.time()
+        o = orc.OracleIndex(data, 1)
+        threads = os.cpu_count() or 1
+        k = args.genome_parity
+        par = {}
+        for name, (q, off) in (("uneven", (r3_q, r3_o)), ("eval_150bp", (q150, o150))):
+            offs = off[:k + 1].cpu().numpy().astype(np.uint64)
+            flat = q[:int(offs[-1])].cpu().numpy()
+            dm = mems(q, off, int(len(off) - 1))
+            hoff = d2h(dm.d_hit_offsets, k + 1, "<i8", dev).view(np.uint64)
+            hits = d2h(dm.d_hits, 8 * int(hoff[-1]), "<i4", dev).view(np.uint32).reshape(-1, 8)
+            npos = 0
+            if len(hits):
+                npos = (int(hits[-1][6]) | (int(hits[-1][7]) << 32)) + int(hits[-1][5])
+            pos = d2h(dm.d_positions, 2 * npos, "<i4", dev).view(np.uint32).reshape(-1, 2)
+            want = o.mems_packed(flat, offs, 19, 0, bounds, 1024, threads)
+            bad = [f for f, a, b in zip(("hit_offsets", "hits", "positions"), (hoff, hits, pos), want)
+                   if a.shape != b.shape or not np.array_equal(a, b)]
+            par[name] = {"reads_checked": k, "equal": not bad, "mismatched": bad, "mem_hits": int(len(want[1]))}
+        par["oracle_s"] = round(time.time() - t0, 1)
+        par["what"] = "timed path's outputs (MemHit CSR, positions) for the first reads of each set vs oracle/hfm_oracle.cpp"
+        out["parity"] = par
+        del o
+    del ls, idx, h
+    return out
 
 
 def main():
@@ -556,6 +632,33 @@ def main():
             pms = float(t.item())
         plain_info = {"value": world * n * args.steps / (pms / 1000.0), "ms_per_step": pms / args.steps}
         learned_info["speedup_vs_plain"] = round(plain_info["ms_per_step"] / (ms / args.steps), 4)
+    # the plain one-thread-per-read launch with its count pass (the reference GPU path's
+    # structure), same loop: the baseline of the persistent path
+    plain_launch = None
+    if not args.no_plain_launch:
+        saved = h.tuning()
+        h.set_tuning(4, saved["seg_len"])
+        for _ in range(max(1, args.warmup // 2)):
+            step(plain=True)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step(plain=True)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        lms = ev0.elapsed_time(ev1)
+        h.set_tuning(saved["mems_variant"], saved["seg_len"])
+        if dist:
+            t = torch.tensor([lms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            lms = float(t.item())
+        plain_launch = {"value": world * n * args.steps / (lms / 1000.0), "ms_per_step": lms / args.steps,
+                        "value_speedup": round(lms / ms, 4),
+                        "what": "locate + find_smems with the SMEM search as one thread per read over a grid of the "
+                                "batch, local-memory sets, count pass + host-read totals + write pass"}
     # learned order vs plain order on the whole batch: every output array byte for byte
     learned_parity = None
     if learned is not None:
@@ -608,8 +711,19 @@ def main():
         tj = json.load(open(tpath))
         if dom in tj:
             traffic = tj[dom]["dram_bytes_per_unit"] * units
+    # the random-access ceiling: independent 32 B / 64 B loads over 8 GB on every SM (the
+    # access pattern of Occ records, which a streaming copy does not have)
+    gather = {}
+    for span in (32, 64):
+        gbs, gms = C.c_float(), C.c_float()
+        L.check(lib.hfm_probe_gather(local, 8 << 30, span, C.byref(gbs), C.byref(gms)))
+        gather[f"random_{span}B_gbs"] = round(gbs.value, 1)
+    rec_span = 32 if h.info().num_lanes <= 5 else 64
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                "random_gather_ceiling": gather, "record_bytes": rec_span,
+                # touches/s of the kernel (32 algorithmic bytes each) over record fetches/s of the probe
+                "frac_of_random_gather": (achieved / 32) / (gather[f"random_{rec_span}B_gbs"] / rec_span),
                 "kernel_ms": kms, "alg_bytes": kbytes, "units": units, "unit_name": unit_name,
                 "kernels_ms": {k: v[0] for k, v in kern.items()},
                 "kernels_gbs": {k: (v[1] / (v[0] / 1000) / 1e9 if v[0] > 0 else None) for k, v in kern.items()}}
@@ -678,10 +792,6 @@ def main():
     serving = None
     if not args.no_serving and rank == 0 and world == 1:      # single-GPU measurements
         serving = serving_latency(h, lib, L, kp, rp, bounds, n, args.serving_batches)
-    mixed = None
-    if not args.no_mixed and rank == 0 and world == 1:
-        del handles
-        mixed = mixed_workload(args, local, torch)
 
     # CPU baseline (the same CPU_SAMPLE reads the reference arm times) and parity: the timed
     # calls' outputs for the first PARITY_READS reads, byte for byte against the oracle
@@ -713,17 +823,24 @@ def main():
         if parity is None:
             parity = {}
         parity["learned_vs_plain"] = learned_parity
+    run_path = ("learned-binned" if learned is not None and learned.enabled else
+                "plain order (learned order not faster on held-out reads)"
+                if learned is not None and learned.calibration is not None else
+                "plain order (cost model not predictive on held-out reads)" if learned is not None else "plain")
+    genome = None
+    if not args.no_genome and rank == 0 and world == 1:
+        del handles, idx, h, learned
+        import gc
+        gc.collect()
+        torch.cuda.empty_cache()
+        genome = genome_workloads(args, local, torch)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "reads/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded generators, haystackfm_b200/synth.py)",
             "config": bench_config(args, world),
-            "run": {"path": ("learned-binned" if learned is not None and learned.enabled else
-                             "plain order (learned order not faster on held-out reads)"
-                             if learned is not None and learned.calibration is not None else
-                             "plain order (cost model not predictive on held-out reads)" if learned is not None
-                             else "plain"),
+            "run": {"path": run_path,
                     "index_build_s": round(build_s, 1), "index_cached": not built,
                     "index_sha256": hashlib.sha256(data).hexdigest(),
                     "locate_positions": int(loc_total), "mem_hits": int(n_hits), "mem_positions": int(n_pos),
@@ -731,7 +848,8 @@ def main():
                     "autotuned": tuning_main},
             "parity": parity,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "plain": plain_info, "learned": learned_info, "serving": serving, "mixed": mixed,
+            "plain": plain_info, "plain_launch": plain_launch, "learned": learned_info, "serving": serving,
+            "genome": genome,
             "clocks": clk,
         }
         print(json.dumps(line), flush=True)

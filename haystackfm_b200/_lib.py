@@ -129,6 +129,8 @@ SIGNATURES = {
     "hfm_last_stats": (C.c_int, [C.c_void_p, C.POINTER(HfmStats)]),
     "hfm_set_counters": (C.c_int, [C.c_void_p, C.c_int]),
     "hfm_set_timeout": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "hfm_mems_reserve": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64]),
+    "hfm_probe_gather": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
 }
 
 _lib = None

@@ -35,6 +35,12 @@ def torch_ones_like(t):
     return _torch().ones_like(t)
 
 
+def torch_expm1_sum(y) -> np.ndarray:
+    """Sum over reads of expm1 of the log1p predictions -> float64[3] (host)."""
+    torch = _torch()
+    return torch.expm1(y.double().clamp(max=40.0)).clamp_min(0).sum(dim=0).cpu().numpy()
+
+
 def work_targets(log) -> "torch.Tensor":
     """Work log rows (u32 touches, MemHits, positions, flags) -> float32 log1p targets [n, 3]."""
     torch = _torch()
@@ -170,6 +176,9 @@ class LearnedSmem:
         self.calibration: Optional[dict] = None
         self._order = None
         self._y = None
+        self.presize = True            # reserve pools and outputs from the predicted totals
+        self.total_scale = np.ones(3)  # actual / predicted totals on the training reads
+        self.margin = 1.15
 
     def log_work(self, q_d, off_d, nq, min_len, mode, bounds, max_hits):
         torch = _torch()
@@ -208,6 +217,10 @@ class LearnedSmem:
         w3 *= sd_h[:, None]
         p[NPARAM - 3:] = p[NPARAM - 3:] * sd_h + mu_h
         self.model.set_params(p)
+        # totals: the model's summed predictions against the logged totals (pre-sizing)
+        pred_tot = torch_expm1_sum(self.model.forward(x))
+        true_tot = log[:, :3].to(_torch().int64).clamp_min(0).sum(dim=0).double().cpu().numpy()
+        self.total_scale = np.where(pred_tot > 0, true_tot / np.maximum(pred_tot, 1e-9), 1.0)
         if ntr < nq:
             self.holdout_error = prediction_error(self.model.forward(x[ntr:].contiguous()), t[ntr:])
             self.enabled = self.holdout_error.spearman_touches >= self.min_spearman
@@ -260,9 +273,20 @@ class LearnedSmem:
         order, nw = self.model.schedule(y, self.warp_min_hits, order=self._order)
         return order, nw, y
 
+    def reserve_from(self, y, nq):
+        """Pre-size the handle's pools and result arrays from the predicted totals (in place
+        of a count pass); candidate intervals are reserved at 3 per predicted MemHit."""
+        tot = torch_expm1_sum(y) * self.total_scale * self.margin
+        hits = int(tot[1]) + nq
+        L.check(L.lib().hfm_mems_reserve(self.handle.h, nq, 3 * hits + 4 * nq, hits, int(tot[2]) + nq))
+
     def run(self, q_d, off_d, nq, min_len, mode, bounds_ptr, n_bounds, max_hits) -> L.HfmDevMems:
+        order, nw = None, 0
+        if self.enabled or self.presize:
+            order, nw, y = self.plan(q_d, off_d, nq)
+            if self.presize and nq:
+                self.reserve_from(y, nq)
         if self.enabled:
-            order, nw, _ = self.plan(q_d, off_d, nq)
             sc = L.HfmSched(order.data_ptr() if nq else None, nw, 0, None)
         else:
             sc = L.HfmSched(None, 0, 0, None)

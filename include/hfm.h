@@ -219,6 +219,16 @@ int hfm_mems_batch_device_sched(hfm_index* idx, const uint8_t* d_q, const uint64
                                 uint32_t min_len, uint32_t mode, const uint32_t* ref_bounds, uint32_t n_bounds,
                                 uint32_t max_hits, const hfm_sched* sched, hfm_dev_mems* out);
 
+/* Pre-sizes a handle's SMEM/MEM work pools and result arrays for a batch of nq reads
+ * expected to produce `intervals` candidate intervals, `hits` MemHits and `positions`
+ * resolved positions (no counterpart in the reference, which counts every batch on the
+ * device, downloads the counts and allocates before a second pass; src/gpu/mem_find.rs:
+ * 213-244, src/fm_index/bidir_index.rs:442-514).  The learned read-cost model calls it
+ * with its predicted totals, so the search runs once with no count pass and no buffer
+ * growth; a batch that outgrows the reservation is rerun with grown pools (same results).
+ * Buffers only grow. */
+int hfm_mems_reserve(hfm_index* idx, uint32_t nq, uint64_t intervals, uint64_t hits, uint64_t positions);
+
 /* ---- learned read-cost model (no counterpart in the reference) -------------
  * A 258 -> 128 -> 128 -> 3 ReLU MLP (BF16 weights and activations, FP32 accumulation)
  * predicting, per read, log1p of the exact SMEM kernel's work log (hfm_sched.d_work_log):
@@ -257,6 +267,13 @@ int hfm_mlp_train(hfm_mlp* m, const uint16_t* d_x, const float* d_t, uint32_t n,
 int hfm_mlp_schedule(hfm_mlp* m, const float* d_y, uint32_t nq, float warp_min_hits, uint32_t* d_order,
                      uint32_t* n_warp);
 
+/* Random-access ceiling of GPU `device` (no counterpart in the reference): independent
+ * loads of `span` (32 or 64) bytes at uniformly random span-aligned offsets of a
+ * buffer_bytes device buffer (>= 64 MiB; it is allocated and freed by the call), 256 bytes
+ * in flight per thread on 8 x 256 threads per SM.  *gbs_out = bytes loaded / second
+ * (CUDA events), *ms_out (may be NULL) = one launch. */
+int hfm_probe_gather(int device, uint64_t buffer_bytes, uint32_t span, float* gbs_out, float* ms_out);
+
 /* ---- misc ----------------------------------------------------------------- */
 void hfm_free(void* p);                    /* frees hfm_hits*, hfm_mem_out*, build bytes */
 const char* hfm_last_error(void);          /* thread-local message of the last failure   */
@@ -274,8 +291,12 @@ int hfm_set_counters(hfm_index* idx, int enable);  /* per-read work counters on/
 int hfm_set_timeout(hfm_index* idx, uint32_t ms);
 
 /* Tunable parameters of the SMEM/MEM search and their autotuner (no counterpart in the
- * reference).  mems_variant: fast pass with 32-entry candidate lists in local memory (2)
- * or 1024-entry lists in global memory (3, default), 8 resident blocks per SM.  seg_len: SMEM reads longer than 2*seg_len are swept in seg_len-position
+ * reference).  mems_variant: persistent fast pass with 32-entry candidate lists in local
+ * memory (2) or 1024-entry lists in global memory (3, default), 8 resident blocks per SM;
+ * 4: the plain launch — one thread per read over a grid the size of the batch, sets and
+ * candidates in local memory, a count pass whose totals are read back to size the outputs
+ * before the write pass (the reference GPU search's structure, shaders/mem_find.wgsl,
+ * src/gpu/mem_find.rs:213-244), kept as the baseline.  seg_len: SMEM reads longer than 2*seg_len are swept in seg_len-position
  * segments (multiple of 32 in 64..4096, default 512).  Results never depend on them.
  * hfm_autotune_mems times the search of a sample batch under each candidate setting
  * (variant 3 with seg_len 512, 256, 1024; variant 2), best of `reps` runs after a warm-up

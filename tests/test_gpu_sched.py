@@ -132,3 +132,25 @@ def test_autotune_keeps_results(oracle):
         h.set_tuning(4, 512)
     with pytest.raises(FmIndexError):
         h.set_tuning(3, 100)
+
+
+def test_plain_launch_bit_exact(mixed_case, oracle):
+    """The plain launch (mems_variant 4: one thread per read, local sets, count pass +
+    write pass) gives the oracle's bytes — long reads, set overflows into the warp kernel
+    and pool sizing by the count pass included — in SMEM and MEM mode, with and without
+    positions."""
+    idx, flat, off, lens, bounds, want = mixed_case
+    h = idx.handle
+    saved = h.tuning()
+    h.set_tuning(4, saved["seg_len"])
+    try:
+        _same(h.mems_packed(flat, off, 19, 0, bounds, 64), want)
+        _same(h.mems_packed(flat, off, 19, 0, bounds, 64), want)          # warm pools
+        o = oracle.OracleIndex(idx.to_bytes(), KIND_BIDIR)
+        short = np.nonzero(lens <= 400)[0][:60]
+        sub_flat = np.concatenate([flat[int(off[i]):int(off[i + 1])] for i in short])
+        sub_off = np.concatenate([[0], np.cumsum(lens[short])]).astype(np.uint64)
+        _same(h.mems_packed(sub_flat, sub_off, 15, 1, bounds, 8), o.mems_packed(sub_flat, sub_off, 15, 1, bounds, 8))
+        _same(h.mems_packed(sub_flat, sub_off, 19, 0, [], 8), o.mems_packed(sub_flat, sub_off, 19, 0, [], 8))
+    finally:
+        h.set_tuning(saved["mems_variant"], saved["seg_len"])
