@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--train-epochs", type=int, default=4)
     ap.add_argument("--no-genome", action="store_true", help="skip the 3.1 Gbp genome workloads")
     ap.add_argument("--no-plain-launch", action="store_true", help="skip timing the plain launch baseline")
+    ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph chain measurement")
     ap.add_argument("--genome-len", type=int, default=3_100_000_000)
     ap.add_argument("--genome-reads", type=int, default=2_000_000, help="mixed-length reads (uneven, training)")
     ap.add_argument("--eval-reads", type=int, default=10_000_000, help="held-out 150 bp reads")
@@ -71,7 +72,8 @@ def parse():
     ap.add_argument("--genome-steps", type=int, default=2)
     ap.add_argument("--genome-parity", type=int, default=2048, help="reads per set checked against the oracle")
     ap.add_argument("--no-serving", action="store_true", help="skip the batch-latency measurement")
-    ap.add_argument("--serving-batches", type=int, default=300)
+    ap.add_argument("--serving-batches", type=int, default=1000)
+    ap.add_argument("--serving-workers", type=int, default=3)
     ap.add_argument("--profile-smem", action="store_true",
                     help="one SMEM search launch (no position resolve) for ncu, then its work counters")
     return ap.parse_args()
@@ -345,6 +347,103 @@ def serving_latency(h, lib, L, kp, rp, bounds, n, n_batches, seed=17):
             "path": "hfm_locate_batch + hfm_mems_batch, host buffers, one handle, back to back"}
 
 
+def serving_loop(h, lib, L, torch, dev, q, off, pool, bounds, n_batches, model, workers, rate=2000.0, seed=17):
+    """batches arrive as a Poisson stream (mean `rate` per second) with sizes
+    log-uniform in 1..100,000 reads, taken from a pool of mixed-length reads (80% 150 bp, 20%
+    long) held in HBM.  A batch is admitted once the predicted output bytes of the batches in
+    flight plus its own fit the HBM budget (the free device memory at the start, less a
+    margin); admitted batches run on `workers` handles that share the index (their own
+    streams and buffers), each as locate of every read's first 32-mer (cap 1024) then
+    find_smems (min_len 19, max_hits 1024).  Latency = completion - arrival, on the host
+    clock."""
+    import queue
+    import threading
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_batches))
+    sizes = np.minimum(np.exp(rng.uniform(0, np.log(100_000), n_batches)).astype(np.int64), pool)
+    sizes = np.maximum(sizes, 1)
+    starts = rng.integers(0, pool - sizes + 1)
+    nb = len(bounds)
+    bp = L.ptr(bounds, L.u32p)
+    # first 32 codes of every read of the pool, and their offsets
+    lens = (off[1:] - off[:-1])
+    idx32 = off[:-1, None] + torch.arange(32, device=dev)[None, :]
+    k32 = q[idx32.clamp(max=q.shape[0] - 1)].reshape(-1).contiguous()
+    o32 = torch.arange(0, (pool + 1) * 32, 32, dtype=torch.int64, device=dev)
+    assert int(lens.min()) >= 32
+    # predicted output bytes per read (positions x 8 + MemHits x 32), from the cost model
+    y = model.model.predict(q, off, pool)
+    per = (torch.expm1(y[:, 2].double().clamp(max=40)) * 8 + torch.expm1(y[:, 1].double().clamp(max=40)) * 32 + 64)
+    cum = torch.cat([torch.zeros(1, dtype=torch.float64, device=dev), torch.cumsum(per, 0)]).cpu().numpy()
+    free_b, _ = torch.cuda.mem_get_info(dev)
+    budget = max(1.0, 0.5 * free_b)
+    handles = [h.share() for _ in range(workers)]
+    cond = threading.Condition()
+    state = {"inflight": 0.0, "max_inflight": 0.0, "waited": 0}
+    lat = np.zeros(n_batches)
+    done_t = np.zeros(n_batches)
+    work = queue.Queue()
+    errors = []
+
+    def worker(hh):
+        try:
+            while True:
+                item = work.get()
+                if item is None:
+                    return
+                i, a, m, est = item
+                with cond:
+                    if state["inflight"] + est > budget and state["inflight"] > 0:
+                        state["waited"] += 1
+                    while state["inflight"] + est > budget and state["inflight"] > 0:
+                        cond.wait()
+                    state["inflight"] += est
+                    state["max_inflight"] = max(state["max_inflight"], state["inflight"])
+                dh = L.HfmDevHits()
+                L.check(lib.hfm_locate_batch_device(hh.h, k32.data_ptr(), o32[a:].data_ptr(), m, 1024, C.byref(dh)))
+                dm = L.HfmDevMems()
+                L.check(lib.hfm_mems_batch_device(hh.h, q.data_ptr(), off[a:].data_ptr(), m, 19, 0, bp, nb, 1024,
+                                                  C.byref(dm)))
+                t = time.perf_counter()
+                done_t[i] = t
+                lat[i] = t - (t0 + arrivals[i])
+                with cond:
+                    state["inflight"] -= est
+                    cond.notify_all()
+        except Exception as e:              # reported after the loop
+            errors.append(repr(e))
+            with cond:
+                cond.notify_all()
+
+    torch.cuda.synchronize()
+    ths = [threading.Thread(target=worker, args=(hh,)) for hh in handles]
+    for t_ in ths:
+        t_.start()
+    t0 = time.perf_counter()
+    for i in range(n_batches):
+        now = time.perf_counter() - t0
+        if arrivals[i] > now:
+            time.sleep(arrivals[i] - now)
+        a, m = int(starts[i]), int(sizes[i])
+        work.put((i, a, m, float(cum[a + m] - cum[a])))
+    for _ in ths:
+        work.put(None)
+    for t_ in ths:
+        t_.join()
+    del handles
+    if errors:
+        raise RuntimeError("serving worker failed: " + errors[0])
+    span = float(done_t.max() - t0)
+    return {"batches": int(n_batches), "arrivals": f"Poisson, mean {rate:.0f} batches/s",
+            "batch_reads": "log-uniform 1..100000", "mean_batch": float(sizes.mean()),
+            "offered_reads_per_s": float(sizes.sum() / arrivals[-1]),
+            "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "max_ms": float(lat.max() * 1e3), "reads_per_s": float(sizes.sum() / span), "workers": workers,
+            "hbm_budget_gb": round(budget / 1e9, 1), "max_inflight_predicted_gb": round(state["max_inflight"] / 1e9, 2),
+            "batches_held_by_admission": int(state["waited"]),
+            "path": "hfm_locate_batch_device + hfm_mems_batch_device on handles sharing one device-resident index"}
+
+
 def genome_workloads(args, device, torch):
     """configs[2] and configs[3] on a 3.1 Gbp repeat-rich ACGT genome (ExactDna
     bidirectional index, sa_sample_rate 32, lookup_depth 10, built on the GPU):
@@ -427,7 +526,40 @@ def genome_workloads(args, device, torch):
     tuning = h.autotune_mems(r3_q, r3_o, n3, 19, 0, bounds, 1024, reps=1)
     ms_persist = timed(lambda: mems(r3_q, r3_o, n3), steps)
     ms_plain = with_tuning(4, lambda: timed(lambda: mems(r3_q, r3_o, n3), steps))
+    # the same search as one CUDA-graph replay of the fixed-capacity chain
+    dm0 = mems(r3_q, r3_o, n3)
+    npos3 = int(dm0.n_positions)
+    g = C.c_void_p()
+    nbases3 = int(r3_o[-1].item())
+    L.check(lib.hfm_mems_graph_create(h.h, r3_q.data_ptr(), r3_o.data_ptr(), n3, nbases3, 19, 0, bp, nb, 1024,
+                                      int(npos3 * 1.25) + 4096, C.byref(g)))
+    rep = C.c_uint32()
+    dmg = L.HfmDevMems()
+
+    def glaunch():
+        L.check(lib.hfm_mems_graph_launch(g, C.byref(dmg), C.byref(rep)))
+
+    def host_ms(fn, k, warm=1):
+        for _ in range(warm):
+            fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(k):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3 / k
+    ms_graph = host_ms(glaunch, steps)
+    g_replayed = int(rep.value)
+    snap = device_mems_tensors(torch, dev, dmg, n3, clone=True)
+    now = device_mems_tensors(torch, dev, mems(r3_q, r3_o, n3), n3, clone=False)
+    g_eq = all(a.shape == b.shape and bool(torch.equal(a, b)) for a, b in zip(snap, now))
+    del snap, now
+    lib.hfm_mems_graph_free(g)
+    ms_adapt_host = host_ms(lambda: mems(r3_q, r3_o, n3), steps)
     out["uneven"] = {"reads": n3, "read_bases": int(r3_o[-1].item()),
+                     "graph_ms_host": round(ms_graph, 2), "adaptive_ms_host": round(ms_adapt_host, 2),
+                     "graph_last_launch_replayed": g_replayed, "graph_outputs_equal": g_eq,
+                     "graph_speedup_vs_plain_launch": round(ms_plain / ms_graph, 3),
                      "mix": "80% 150 bp (1% substitutions), 20% lognormal median 3 kbp up to 10 kbp (8% subs/indels)",
                      "persistent_ms": round(ms_persist, 2), "persistent_reads_per_s": n3 / (ms_persist / 1e3),
                      "plain_launch_ms": round(ms_plain, 2), "plain_launch_reads_per_s": n3 / (ms_plain / 1e3),
@@ -465,6 +597,10 @@ def genome_workloads(args, device, torch):
                          "mem_positions": int(dm.n_positions)}
         del got, ref
     out["learned"] = learned
+    # serving loop on the same device-resident index
+    if not args.no_serving and args.serving_batches > 0:
+        out["serving"] = serving_loop(h, lib, L, torch, dev, em_q, em_o, args.eval_mixed, bounds, args.serving_batches,
+                                      ls, args.serving_workers)
     # parity subsample against the oracle (CPU) on the same index bytes
     if not args.no_cpu_baseline and args.genome_parity > 0:
         from oracle import oracle as orc
@@ -672,6 +808,48 @@ def main():
         learned_parity = {"reads_checked": n, "equal": eq, "mem_hits": int(dm_l.n_hits),
                           "mem_positions": int(dm_l.n_positions)}
         del snap, now
+    # the CUDA-graph-captured SMEM chain against the adaptive chain on the same batch
+    # (host clock around each call: both include their waits for the device)
+    graph_info = None
+    if not args.no_graph:
+        g = C.c_void_p()
+        L.check(lib.hfm_mems_graph_create(h.h, reads_d.data_ptr(), off_d.data_ptr(), n, n * 150, 19, 0,
+                                          L.ptr(bounds, L.u32p), nb, 1024, int(n_pos * 1.25) + 4096, C.byref(g)))
+        rep = C.c_uint32()
+        dmg = L.HfmDevMems()
+
+        def host_ms(fn, k):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(k):
+                fn()
+            torch.cuda.synchronize()
+            return (time.perf_counter() - t0) * 1e3 / k
+
+        def glaunch():
+            L.check(lib.hfm_mems_graph_launch(g, C.byref(dmg), C.byref(rep)))
+
+        def adapt():
+            dm = L.HfmDevMems()
+            L.check(lib.hfm_mems_batch_device(h.h, reads_d.data_ptr(), off_d.data_ptr(), n, 19, 0,
+                                              L.ptr(bounds, L.u32p), nb, 1024, C.byref(dm)))
+        for _ in range(2):
+            glaunch()
+        g_ms = host_ms(glaunch, args.steps)
+        replayed = int(rep.value)
+        a_ms = host_ms(adapt, args.steps)
+        snap = device_mems_tensors(torch, dev, dmg, n, clone=True)
+        dm_a = L.HfmDevMems()
+        L.check(lib.hfm_mems_batch_device(h.h, reads_d.data_ptr(), off_d.data_ptr(), n, 19, 0, L.ptr(bounds, L.u32p),
+                                          nb, 1024, C.byref(dm_a)))
+        now = device_mems_tensors(torch, dev, dm_a, n, clone=False)
+        geq = all(a.shape == b.shape and bool(torch.equal(a, b)) for a, b in zip(snap, now))
+        del snap, now
+        lib.hfm_mems_graph_free(g)
+        graph_info = {"graph_ms": round(g_ms, 3), "adaptive_ms": round(a_ms, 3), "speedup": round(a_ms / g_ms, 4),
+                      "last_launch_replayed": replayed, "outputs_equal": geq,
+                      "what": "find_smems of the batch: one CUDA graph replay of the fixed-capacity chain "
+                              "(hfm_mems_graph_launch) vs hfm_mems_batch_device; host clock per call"}
     # kernel times (CUDA events around each launch, recorded by the library on its stream)
     k_mems_ms = statistics.mean(s2.ms_search_kernel for _, s2, *_ in per)
     k_res_mem_ms = statistics.mean(s2.ms_resolve_kernel for _, s2, *_ in per)
@@ -791,7 +969,7 @@ def main():
 
     serving = None
     if not args.no_serving and rank == 0 and world == 1:      # single-GPU measurements
-        serving = serving_latency(h, lib, L, kp, rp, bounds, n, args.serving_batches)
+        serving = serving_latency(h, lib, L, kp, rp, bounds, n, 300)
 
     # CPU baseline (the same CPU_SAMPLE reads the reference arm times) and parity: the timed
     # calls' outputs for the first PARITY_READS reads, byte for byte against the oracle
@@ -848,7 +1026,8 @@ def main():
                     "autotuned": tuning_main},
             "parity": parity,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "plain": plain_info, "plain_launch": plain_launch, "learned": learned_info, "serving": serving,
+            "plain": plain_info, "plain_launch": plain_launch, "graph": graph_info, "learned": learned_info,
+            "serving": serving,
             "genome": genome,
             "clocks": clk,
         }

@@ -90,6 +90,7 @@ SIGNATURES = {
                                       C.c_int, C.c_int, C.POINTER(u8p), C.POINTER(C.c_size_t)]),
     "hfm_index_load": (C.c_int, [u8p, C.c_size_t, C.c_int, C.POINTER(HfmOpts), C.POINTER(C.c_void_p)]),
     "hfm_index_free": (None, [C.c_void_p]),
+    "hfm_index_share": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "hfm_index_info_get": (C.c_int, [C.c_void_p, C.POINTER(HfmIndexInfo)]),
     "hfm_count_batch": (C.c_int, [C.c_void_p, u8p, u64p, C.c_uint32, u32p]),
     "hfm_locate_batch": (C.c_int, [C.c_void_p, u8p, u64p, C.c_uint32, C.c_uint32, C.POINTER(C.POINTER(HfmHits))]),
@@ -129,6 +130,11 @@ SIGNATURES = {
     "hfm_last_stats": (C.c_int, [C.c_void_p, C.POINTER(HfmStats)]),
     "hfm_set_counters": (C.c_int, [C.c_void_p, C.c_int]),
     "hfm_set_timeout": (C.c_int, [C.c_void_p, C.c_uint32]),
+    "hfm_mems_graph_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint32,
+                                        C.c_uint32, u32p, C.c_uint32, C.c_uint32, C.c_uint64,
+                                        C.POINTER(C.c_void_p)]),
+    "hfm_mems_graph_launch": (C.c_int, [C.c_void_p, C.POINTER(HfmDevMems), C.POINTER(C.c_uint32)]),
+    "hfm_mems_graph_free": (None, [C.c_void_p]),
     "hfm_mems_reserve": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64]),
     "hfm_probe_gather": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
 }

@@ -133,6 +133,7 @@ struct hfm_index {
   Counters* h_ctr = nullptr;        // pinned
   uint32_t timeout_ms = 0;          // host-side deadline of every wait on the stream (0: none)
   std::vector<void*> orphans;       // result blocks of calls that timed out (freed once the stream drains)
+  bool shared_index = false;        // fwd / rev device buffers belong to another handle
   cudaEvent_t ev_wait = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaEvent_t evk[4] = {nullptr, nullptr, nullptr, nullptr};   // main search kernel, resolve kernel
@@ -902,6 +903,252 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   return HFM_OK;
 }
 
+// ---------------------------------------------------------------------------
+// The SMEM/MEM pass chain with fixed capacities, for CUDA-graph capture.
+//
+// mems_device decides on the host between passes (the overflow tiers it runs, how many
+// long-read segments there are, how large the outputs are) and so reads counters back
+// after every pass.  This chain makes every such decision on the device: each pass runs
+// over capacities fixed beforehand (the handle's reserved pools, `pos_cap` positions) and
+// reads its counts from device memory, so the whole chain is one stream of asynchronous
+// work that a CUDA graph can capture and replay.  Whatever outgrows a capacity is only
+// flagged (pool counters, still_ovf, the totals' overflow bit): the host checks the flags
+// after the replay and reruns the batch on mems_device, which gives the same results.
+//
+// fixed_chain(launch = false) makes every allocation the chain needs; fixed_chain(launch =
+// true) issues the same sequence of kernels and copies, allocating nothing.
+// ---------------------------------------------------------------------------
+struct GraphTotals { uint64_t nh, npos, upos; uint32_t ovf, _pad; };
+
+// Totals of the chain: MemHits, and the position counts the resolve passes cover, both 0
+// (with ovf set) when a count exceeds the position capacity.
+__global__ void k_graph_totals(const uint64_t* __restrict__ hit_base, uint32_t nq, const uint64_t* __restrict__ pos_total,
+                               const uint64_t* __restrict__ u_total, uint64_t pos_cap, GraphTotals* __restrict__ t) {
+  if (blockIdx.x || threadIdx.x) return;
+  const uint64_t np = *pos_total, nu = u_total ? *u_total : 0;
+  const bool over = np > pos_cap || nu > pos_cap;
+  t->nh = hit_base[nq];
+  t->npos = over ? 0 : np;
+  t->upos = over ? 0 : nu;
+  t->ovf = over ? 1u : 0u;
+}
+
+struct FixedChain {
+  const uint8_t* d_q; const uint64_t* d_qoff; uint32_t nq;
+  uint64_t max_bases;          // reads of at most this many codes in total
+  MemsParams P; uint32_t nb;   // ref bounds already in x->ref_bounds
+  bool dedup;
+  uint64_t pos_cap;
+  GraphTotals* d_tot; GraphTotals* h_tot;     // device / pinned host
+  uint64_t threads;            // resident threads of the persistent kernels
+};
+
+static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
+  const uint32_t nq = c.nq;
+  const FmDev& Fw = x->fwd; const FmDev& Rv = x->rev;
+  const uint32_t fmt = Fw.fmt;
+  uint32_t dummy = 0;
+  auto SCAN = [&](auto* in, uint32_t stride, uint64_t n, uint64_t* out) -> int {
+    if (!launch) {
+      uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+      return x->scan_tmp.ensure((tiles + 1) * 8);
+    }
+    return scan(x, in, stride, n, out, dummy);
+  };
+  const uint64_t hcap = x->hit_cap, pcap = c.pos_cap;
+  if (hcap >= 0xFFFFFFFFull) return set_error(HFM_E_ARG, "MemHit capacity above 2^32");
+  // work buffers
+  RET(x->hit_start.ensure((size_t)nq * 8 + 8)); RET(x->hit_count.ensure((size_t)nq * 4 + 4));
+  RET(x->status.ensure((size_t)nq * 4 + 4)); RET(x->ovf.ensure((size_t)nq * 4 + 4));
+  RET(x->ovf2.ensure((size_t)nq * 4 + 4)); RET(x->ovf3.ensure((size_t)nq * 4 + 4));
+  RET(x->mivpool.ensure(x->miv_cap * 16)); RET(x->hitpool.ensure(hcap * 32));
+  if (!launch) {                     // occupancy queried outside the capture
+    int bpsm = 0;
+    WITH_FMT(fmt, { CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_mems<false, 32, 0, 8, FM>, 128, 0)); });
+    c.threads = (uint64_t)std::max(1, bpsm) * x->num_sms * 128;
+  }
+  const uint64_t threads = c.threads;
+  RET(x->memwork.ensure(threads * 4 * MEM_SET_CAP * 16));
+  RET(x->cwork.ensure((size_t)threads * FAST_CAND_CAP * sizeof(Cand)));
+  const bool seg = c.P.mode == 0 && c.P.min_len > 0;
+  const uint64_t ucap = c.max_bases / x->seg_len + nq + 1;    // segments of the long reads
+  if (seg) {
+    RET(x->lflag.ensure((size_t)nq * 4 + 4)); RET(x->lpos.ensure(((size_t)nq + 1) * 8));
+    RET(x->sids.ensure((size_t)nq * 4 + 4)); RET(x->lids.ensure((size_t)nq * 4 + 4));
+    RET(x->ucount.ensure((size_t)nq * 4 + 4)); RET(x->ubase.ensure(((size_t)nq + 1) * 8));
+    RET(x->uread.ensure(ucap * 4)); RET(x->uk.ensure(ucap * 4));
+    RET(x->ubits.ensure(ucap * (x->seg_len / 32) * 4)); RET(x->uexit.ensure(ucap * 4));
+    RET(x->ust.ensure(ucap * 4)); RET(x->ucoff.ensure(ucap * 8)); RET(x->ucnt.ensure(ucap * 4));
+    RET(x->fxe.ensure(ucap * 4)); RET(x->fxc.ensure(ucap * 4)); RET(x->fxx.ensure(ucap * 4));
+    RET(x->fxo.ensure(ucap * 8)); RET(x->fxn.ensure(ucap * 4));
+    x->seg_cap = std::max<uint64_t>(x->seg_cap, ucap * 24 + 65536);
+    RET(x->segpool.ensure(x->seg_cap * sizeof(Cand)));
+  }
+  const uint32_t wgrid = (uint32_t)x->num_sms * 4;                  // warp tier: 16 warps per SM
+  RET(x->work.ensure((size_t)wgrid * 4 * MEM_WARP_SET_CAP * 4 * 16));
+  RET(x->hit_base.ensure(((size_t)nq + 1) * 8));
+  RET(x->hits.ensure((hcap + 1) * 32));
+  RET(x->npos_scan.ensure((hcap + 1) * 8));
+  RET(x->out_pairs.ensure(pcap * 8 + 8));
+  const uint64_t rblocks = (pcap + RES_T - 1) / RES_T, eblocks = (pcap + EXP_BLK - 1) / EXP_BLK;
+  RET(x->blockmap.ensure(rblocks * 4 + 4));
+  uint64_t hsize = 1024;
+  while (hsize < 2 * hcap) hsize <<= 1;
+  if (c.dedup) {
+    RET(x->hkeys.ensure(hsize * 8)); RET(x->hslot.ensure(hcap * 4 + 4));
+    RET(x->hflags.ensure(hsize * 4)); RET(x->huid.ensure((hsize + 1) * 8));
+    RET(x->urow.ensure(hcap * 4 + 4)); RET(x->ulen.ensure(hcap * 4 + 4)); RET(x->uoff.ensure((hcap + 1) * 8));
+    RET(x->uout.ensure(pcap * 8 + 8));
+    RET(x->blockmap2.ensure(eblocks * 4 + 4));
+  }
+  const MemsParams& P = c.P;
+  Counters* dc = dctr(x);
+  Pool ivp{x->mivpool.p, &dc->iv_used, x->miv_cap}, hp{x->hitpool.p, &dc->hit_used, hcap};
+  MemsOut o{x->hit_start.as<uint64_t>(), x->hit_count.as<uint32_t>(), x->status.as<uint32_t>(),
+            x->ovf.as<uint32_t>(), &dc->n_ovf, &dc->touches};
+  const uint16_t* cfw = Fw.compat.as<uint16_t>();
+  const uint16_t* crv = Rv.compat.as<uint16_t>();
+  if (launch) CK(cudaMemsetAsync(x->ctr.p, 0, sizeof(Counters), x->stream));
+  // search: long reads cut into segments, every read through the segment queue
+  if (seg) {
+    if (launch) {
+      k_long_flags<<<(nq + 255) / 256, 256, 0, x->stream>>>(nullptr, nq, c.d_qoff, 2 * x->seg_len, x->lflag.as<uint32_t>());
+      CK(cudaGetLastError());
+    }
+    RET(SCAN(x->lflag.as<uint32_t>(), 1, nq, x->lpos.as<uint64_t>()));
+    if (launch) {
+      CK(cudaMemsetAsync(x->ucount.p, 0, (size_t)nq * 4, x->stream));
+      k_split_ids<<<(nq + 255) / 256, 256, 0, x->stream>>>(nullptr, nq, x->lflag.as<uint32_t>(), x->lpos.as<uint64_t>(),
+                                                           x->sids.as<uint32_t>(), x->lids.as<uint32_t>(),
+                                                           x->ucount.as<uint32_t>(), c.d_qoff, x->seg_len);
+      CK(cudaGetLastError());
+    }
+    RET(SCAN(x->ucount.as<uint32_t>(), 1, nq, x->ubase.as<uint64_t>()));   // ubase[nq] = segments
+    const uint64_t* n_long_dev = x->lpos.as<uint64_t>() + nq;
+    const uint64_t* n_units_dev = x->ubase.as<uint64_t>() + nq;
+    if (launch) {
+      k_unit_fill<<<(nq + 255) / 256, 256, 0, x->stream>>>(x->lids.as<uint32_t>(), nq, x->ubase.as<uint64_t>(),
+                                                           x->uread.as<uint32_t>(), x->uk.as<uint32_t>(), n_long_dev);
+      CK(cudaGetLastError());
+      SegWork G{x->seg_len, x->seg_len / 32, x->uread.as<uint32_t>(), x->uk.as<uint32_t>(), 0u, x->ubits.as<uint32_t>(),
+                x->uexit.as<uint32_t>(), x->ust.as<uint32_t>(), x->ucoff.as<uint64_t>(), x->ucnt.as<uint32_t>(),
+                x->segpool.as<Cand>(), &dc->seg_used, x->seg_cap, x->sids.as<uint32_t>(), 0u, x->lids.as<uint32_t>(),
+                x->ubase.as<uint64_t>(), 0u, &dc->merge_queue, &dc->touches, x->fxe.as<uint32_t>(),
+                x->fxc.as<uint32_t>(), x->fxx.as<uint32_t>(), x->fxo.as<uint64_t>(), x->fxn.as<uint32_t>(),
+                n_units_dev, n_long_dev, nq};
+      MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), FAST_CAND_CAP, &dc->seg_queue, nullptr,
+                 0u, &dc->still_ovf, 0u, nullptr, nullptr};
+      MemsWork Wf = W;
+      Wf.queue = &dc->fix_queue;
+      const unsigned g = (unsigned)(threads / 128);
+      WITH_FMT(fmt, {
+        k_mems_seg<false, 32, 8, FM><<<g, 128, 0, x->stream>>>(Fw.d, Rv.d, cfw, crv, c.d_q, c.d_qoff, P, ivp, hp, o, W, G);
+        k_mems_fix<false, 32, 8, FM><<<g, 128, 0, x->stream>>>(Fw.d, Rv.d, cfw, crv, c.d_q, c.d_qoff, P, ivp, Wf, G);
+        k_mems_merge<false, 32, 8, FM><<<g, 128, 0, x->stream>>>(Fw.d, Rv.d, cfw, crv, c.d_q, c.d_qoff, P, ivp, hp, o, W,
+                                                                 G);
+      });
+      CK(cudaGetLastError());
+    }
+  } else if (launch) {
+    MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), FAST_CAND_CAP, &dc->queue, nullptr, nq,
+               &dc->still_ovf, 0u, nullptr, nullptr};
+    WITH_FMT(fmt, {
+      k_mems<false, 32, 0, 8, FM><<<(unsigned)(threads / 128), 128, 0, x->stream>>>(Fw.d, Rv.d, cfw, crv, c.d_q,
+                                                                                    c.d_qoff, P, ivp, hp, o, W);
+    });
+    CK(cudaGetLastError());
+  }
+  // overflow tiers, over the device lists: a per-thread rerun with a 1024-entry candidate
+  // list, then one warp per read with sets of MEM_WARP_SET_CAP intervals
+  if (launch) {
+    k_split_ovf<<<(nq + 255) / 256, 256, 0, x->stream>>>(x->ovf.as<uint32_t>(), nq, 0u, x->status.as<uint32_t>(),
+                                                         x->ovf3.as<uint32_t>(), &dc->n_mid, x->ovf2.as<uint32_t>(),
+                                                         &dc->n_wrp, &dc->n_ovf);
+    CK(cudaGetLastError());
+    const uint64_t tm = std::max<uint64_t>(128, std::min<uint64_t>((uint64_t)x->num_sms * MID_THREADS_PER_SM, threads));
+    MemsWork Wm{x->memwork.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), MID_CAND_CAP, &dc->queue3, x->ovf3.as<uint32_t>(),
+                0u, &dc->still_ovf, 0u, nullptr, &dc->n_mid};
+    MemsOut o2 = o;
+    o2.ovf_list = x->ovf2.as<uint32_t>();
+    o2.n_ovf = &dc->n_wrp;
+    WITH_FMT(fmt, {
+      k_mems<false, 32, 0, 8, FM><<<(unsigned)(tm / 128), 128, 0, x->stream>>>(Fw.d, Rv.d, cfw, crv, c.d_q, c.d_qoff, P,
+                                                                                ivp, hp, o2, Wm);
+    });
+    MemsWork Ww{x->work.as<BIv>(), MEM_WARP_SET_CAP, x->cwork.as<Cand>(), 1024u, &dc->queue2, x->ovf2.as<uint32_t>(), 0u,
+                &dc->still_ovf, 1u, nullptr, &dc->n_wrp};
+    k_mems_warp<false><<<wgrid, 128, 0, x->stream>>>(Fw.d, Rv.d, cfw, crv, c.d_q, c.d_qoff, P, ivp, hp, o, Ww);
+    CK(cudaGetLastError());
+  }
+  // CSR of MemHits (hits past the count stay zero, so their position counts add nothing)
+  RET(SCAN(x->hit_count.as<uint32_t>(), 1, nq, x->hit_base.as<uint64_t>()));
+  if (launch) {
+    CK(cudaMemsetAsync(x->hits.p, 0, (hcap + 1) * 32, x->stream));
+    k_gather_hits<<<(nq + 255) / 256, 256, 0, x->stream>>>(x->hitpool.as<uint4>(), x->hit_start.as<uint64_t>(),
+                                                          x->hit_count.as<uint32_t>(), x->hit_base.as<uint64_t>(), nq,
+                                                          x->hits.as<uint4>());
+    CK(cudaGetLastError());
+  }
+  RET(SCAN(x->hits.as<uint32_t>() + 5, 8, hcap, x->npos_scan.as<uint64_t>()));
+  if (launch) {
+    k_set_pos_off<<<(unsigned)((hcap + 255) / 256), 256, 0, x->stream>>>(x->hits.as<uint32_t>(), x->npos_scan.as<uint64_t>(),
+                                                                        hcap);
+    CK(cudaGetLastError());
+  }
+  const uint32_t* seg_row = x->hits.as<uint32_t>() + 4;
+  const uint64_t* seg_off = x->npos_scan.as<uint64_t>();
+  const uint32_t* d_bounds = x->ref_bounds.as<uint32_t>();
+  const uint32_t guard = Fw.rate ? Fw.rate : Fw.text_len;
+  if (c.dedup) {
+    if (launch) {
+      CK(cudaMemsetAsync(x->hkeys.p, 0xFF, hsize * 8, x->stream));
+      k_dedup_insert<<<(unsigned)((hcap + 255) / 256), 256, 0, x->stream>>>(seg_row, 8, seg_off, (uint32_t)hcap,
+                                                                           x->hkeys.as<unsigned long long>(), hsize - 1,
+                                                                           x->hslot.as<uint32_t>());
+      k_dedup_flags<<<(unsigned)((hsize + 255) / 256), 256, 0, x->stream>>>(x->hkeys.as<unsigned long long>(), hsize,
+                                                                           x->hflags.as<uint32_t>());
+      CK(cudaGetLastError());
+    }
+    RET(SCAN(x->hflags.as<uint32_t>(), 1, hsize, x->huid.as<uint64_t>()));
+    if (launch) {
+      CK(cudaMemsetAsync(x->ulen.p, 0, hcap * 4 + 4, x->stream));
+      k_dedup_compact<<<(unsigned)((hsize + 255) / 256), 256, 0, x->stream>>>(x->hkeys.as<unsigned long long>(), hsize,
+                                                                             x->huid.as<uint64_t>(), x->urow.as<uint32_t>(),
+                                                                             x->ulen.as<uint32_t>());
+      CK(cudaGetLastError());
+    }
+    RET(SCAN(x->ulen.as<uint32_t>(), 1, hcap, x->uoff.as<uint64_t>()));     // uoff[hcap] = distinct positions
+    if (launch) {
+      k_graph_totals<<<1, 32, 0, x->stream>>>(x->hit_base.as<uint64_t>(), nq, seg_off + hcap,
+                                              x->uoff.as<uint64_t>() + hcap, pcap, c.d_tot);
+      k_block_first<<<(unsigned)((hcap + 255) / 256), 256, 0, x->stream>>>(x->uoff.as<uint64_t>(), (uint32_t)hcap, RES_T,
+                                                                          x->blockmap.as<uint32_t>(), rblocks);
+      ResolveArgs A{x->urow.as<uint32_t>(), 1, x->uoff.as<uint64_t>(), (uint32_t)hcap, pcap, d_bounds, c.nb, guard,
+                    x->uout.as<uint32_t>(), &dc->walk_err, &dc->steps, x->blockmap.as<uint32_t>(), &c.d_tot->upos};
+      k_resolve<false><<<(unsigned)((pcap + RES_T - 1) / RES_T), RES_T, 0, x->stream>>>(Fw.d, A);
+      k_block_first<<<(unsigned)((hcap + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)hcap, EXP_BLK,
+                                                                          x->blockmap2.as<uint32_t>(), eblocks);
+      k_dedup_expand<<<(unsigned)((pcap + EXP_BLK - 1) / EXP_BLK), EXP_T, 0, x->stream>>>(
+          seg_off, (uint32_t)hcap, pcap, x->hslot.as<uint32_t>(), x->huid.as<uint64_t>(), x->uoff.as<uint64_t>(),
+          x->uout.as<uint2>(), reinterpret_cast<uint2*>(x->out_pairs.p), x->blockmap2.as<uint32_t>(), &c.d_tot->npos);
+      CK(cudaGetLastError());
+    }
+  } else if (launch) {
+    k_graph_totals<<<1, 32, 0, x->stream>>>(x->hit_base.as<uint64_t>(), nq, seg_off + hcap, nullptr, pcap, c.d_tot);
+    k_block_first<<<(unsigned)((hcap + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)hcap, RES_T,
+                                                                        x->blockmap.as<uint32_t>(), rblocks);
+    ResolveArgs A{seg_row, 8, seg_off, (uint32_t)hcap, pcap, d_bounds, c.nb, guard, x->out_pairs.as<uint32_t>(),
+                  &dc->walk_err, &dc->steps, x->blockmap.as<uint32_t>(), &c.d_tot->npos};
+    k_resolve<false><<<(unsigned)((pcap + RES_T - 1) / RES_T), RES_T, 0, x->stream>>>(Fw.d, A);
+    CK(cudaGetLastError());
+  }
+  if (launch) {
+    CK(cudaMemcpyAsync(c.h_tot, c.d_tot, sizeof(GraphTotals), cudaMemcpyDeviceToHost, x->stream));
+    CK(cudaMemcpyAsync(x->h_ctr, x->ctr.p, sizeof(Counters), cudaMemcpyDeviceToHost, x->stream));
+  }
+  return HFM_OK;
+}
+
 // H2D of a host query batch into the handle's buffers.
 static int stage_queries(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32_t nq) {
   if (nq && (!q_off)) return set_error(HFM_E_ARG, "q_off is NULL");
@@ -970,6 +1217,33 @@ struct Guard {
   }
 };
 
+// A handle on the same device-resident index with its own stream and work buffers (the
+// index's buffers are not copied and stay owned by `x`).
+static int make_shadow(hfm_index* x, hfm_index** out) {
+  std::unique_ptr<hfm_index> sh(new hfm_index());
+  sh->device = x->device; sh->kind = x->kind; sh->flags = x->flags; sh->num_sms = x->num_sms;
+  sh->seg_len = x->seg_len; sh->mems_variant = x->mems_variant; sh->count_work = x->count_work;
+  sh->timeout_ms = x->timeout_ms;
+  sh->shared_index = true;
+  for (int k = 0; k < 2; k++) {
+    const FmDev& src = k ? x->rev : x->fwd;
+    FmDev& dst = k ? sh->rev : sh->fwd;
+    dst.d = src.d; dst.occ = src.occ; dst.sb = src.sb; dst.ssa = src.ssa; dst.sa_vals = src.sa_vals; dst.lut = src.lut;
+    dst.bounds = src.bounds; dst.compat = src.compat; dst.text_len = src.text_len; dst.num_seqs = src.num_seqs;
+    dst.lookup_depth = src.lookup_depth; dst.tag = src.tag; dst.num_lanes = src.num_lanes; dst.encoding = src.encoding;
+    dst.rate = src.rate; dst.fmt = src.fmt; dst.seq_boundaries = src.seq_boundaries;
+  }
+  CK(cudaSetDevice(x->device));
+  CK(cudaStreamCreateWithFlags(&sh->stream, cudaStreamNonBlocking));
+  for (auto& e : sh->ev) CK(cudaEventCreate(&e));
+  for (auto& e : sh->evk) CK(cudaEventCreate(&e));
+  CK(cudaEventCreateWithFlags(&sh->ev_wait, cudaEventDisableTiming));
+  CK(cudaMallocHost((void**)&sh->h_ctr, sizeof(Counters)));
+  RET(sh->ctr.ensure(sizeof(Counters)));
+  *out = sh.release();
+  return HFM_OK;
+}
+
 }  // namespace hfm
 
 // ===========================================================================
@@ -1023,6 +1297,9 @@ void hfm_index_free(hfm_index* x) {
   cudaSetDevice(x->device);
   if (x->stream) cudaStreamSynchronize(x->stream);
   for (void* p : x->orphans) host_result_free(p);
+  if (x->shared_index)                // the index layout belongs to the handle this one shares
+    for (FmDev* f : {&x->fwd, &x->rev})
+      for (DevBuf* b : {&f->occ, &f->sb, &f->ssa, &f->sa_vals, &f->lut, &f->bounds, &f->compat}) { b->p = nullptr; b->cap = 0; }
   for (DevBuf* b : {&x->fwd.occ, &x->fwd.sb, &x->rev.sb, &x->fwd.ssa, &x->fwd.sa_vals, &x->fwd.lut, &x->fwd.bounds,
                     &x->fwd.compat, &x->rev.occ, &x->rev.ssa, &x->rev.sa_vals, &x->rev.lut,
                     &x->rev.bounds, &x->rev.compat, &x->q, &x->qoff, &x->counts, &x->nhits, &x->niv, &x->ivoff,
@@ -1233,6 +1510,142 @@ int hfm_mems_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32
   }
   *out = m;
   return HFM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// CUDA-graph-captured SMEM/MEM pass chain
+// ---------------------------------------------------------------------------
+struct hfm_graph {
+  hfm_index* sh = nullptr;           // shadow handle: the index's device layout, own buffers and stream
+  cudaGraphExec_t exec = nullptr;
+  FixedChain c{};
+  bool stale = true;                 // capture (again) before the next replay
+  uint64_t* h_bases = nullptr;       // pinned: the batch's total codes, read before each replay
+  uint32_t replays = 0, fallbacks = 0;
+  DevBuf tot;
+  std::vector<uint32_t> bounds;      // host copy of the reference bounds (for the adaptive rerun)
+};
+
+namespace hfm {
+
+static void free_graph(hfm_graph* g) {
+  if (!g) return;
+  if (g->sh) {
+    cudaSetDevice(g->sh->device);
+    if (g->sh->stream) cudaStreamSynchronize(g->sh->stream);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    g->tot.release();
+    hfm_index_free(g->sh);             // a shadow: the index buffers stay with their handle
+  }
+  if (g->h_bases) cudaFreeHost(g->h_bases);
+  delete g;
+}
+
+static int capture(hfm_graph* g) {
+  hfm_index* x = g->sh;
+  if (g->exec) { cudaGraphExecDestroy(g->exec); g->exec = nullptr; }
+  RET(fixed_chain(x, g->c, false));                // every allocation, outside the capture
+  CK(cudaStreamSynchronize(x->stream));
+  CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = fixed_chain(x, g->c, true);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(x->stream, &graph);
+  if (rc != HFM_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
+  if (e != cudaSuccess) return set_error(HFM_E_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&g->exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) { g->exec = nullptr; return set_error(HFM_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e)); }
+  g->stale = false;
+  return HFM_OK;
+}
+
+}  // namespace hfm
+
+extern "C" int hfm_mems_graph_create(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq,
+                                     uint64_t max_bases, uint32_t min_len, uint32_t mode, const uint32_t* ref_bounds,
+                                     uint32_t nb, uint32_t max_hits, uint64_t max_positions, hfm_graph** out) {
+  if (!x || !out || !d_qoff || !nq || (nb && !ref_bounds)) return set_error(HFM_E_ARG, "NULL argument or empty batch");
+  if (x->kind != HFM_KIND_BIDIR) return set_error(HFM_E_ARG, "MEM/SMEM search needs a bidirectional index");
+  if (mode > 1) return set_error(HFM_E_ARG, "mode must be 0 (SMEM) or 1 (MEM)");
+  *out = nullptr;
+  std::unique_lock<std::mutex> lk(x->mu);
+  CK(cudaSetDevice(x->device));
+  std::unique_ptr<hfm_graph, void (*)(hfm_graph*)> g(new hfm_graph(), free_graph);
+  RET(make_shadow(x, &g->sh));
+  hfm_index* sh = g->sh;
+  if (sh->mems_variant == MEMS_PLAIN) sh->mems_variant = 3;
+  sh->miv_cap = std::max<uint64_t>(x->miv_cap, (uint64_t)nq * 24 + 4096);
+  sh->hit_cap = std::max<uint64_t>(x->hit_cap, (uint64_t)nq * 24 + 4096);
+  sh->seg_cap = x->seg_cap;
+  CK(cudaMallocHost((void**)&g->h_bases, 64));
+  RET(g->tot.ensure(64));
+  RET(sh->ref_bounds.ensure((size_t)nb * 4 + 4));
+  if (nb) CK(cudaMemcpy(sh->ref_bounds.p, ref_bounds, (size_t)nb * 4, cudaMemcpyHostToDevice));
+  g->bounds.assign(ref_bounds, ref_bounds + nb);
+  FixedChain& c = g->c;
+  c.d_q = d_q; c.d_qoff = d_qoff; c.nq = nq; c.max_bases = max_bases;
+  c.P = MemsParams{min_len, mode, max_hits, nb ? 1u : 0u};
+  c.nb = nb;
+  c.dedup = !(x->flags & HFM_FLAG_DEDUP_NEVER);
+  c.pos_cap = std::max<uint64_t>(max_positions, 4096);
+  c.d_tot = g->tot.as<GraphTotals>();
+  c.h_tot = reinterpret_cast<GraphTotals*>(g->h_bases + 1);
+  lk.unlock();
+  {
+    std::lock_guard<std::mutex> lg(sh->mu);
+    RET(capture(g.get()));
+  }
+  *out = g.release();
+  return HFM_OK;
+}
+
+extern "C" int hfm_mems_graph_launch(hfm_graph* g, hfm_dev_mems* out, uint32_t* replayed) {
+  if (!g || !out) return set_error(HFM_E_ARG, "NULL argument");
+  hfm_index* x = g->sh;
+  std::lock_guard<std::mutex> lk(x->mu);
+  CK(cudaSetDevice(x->device));
+  FixedChain& c = g->c;
+  // the one read before the replay: the batch must fit the captured segment capacity
+  CK(cudaMemcpyAsync(g->h_bases, c.d_qoff + c.nq, 8, cudaMemcpyDeviceToHost, x->stream));
+  RET(wait_stream(x));
+  bool ok = g->h_bases[0] <= c.max_bases;
+  if (ok) {
+    if (g->stale) RET(capture(g));
+    CK(cudaGraphLaunch(g->exec, x->stream));
+    RET(wait_stream(x));
+    const Counters& k = *x->h_ctr;
+    const GraphTotals& t = *c.h_tot;
+    ok = k.iv_used <= x->miv_cap && k.hit_used <= x->hit_cap && k.seg_used <= x->seg_cap && k.still_ovf == 0 &&
+         t.ovf == 0;
+    if (k.walk_err) return set_error(HFM_E_WALK, "LF walk exceeded sample_rate steps: index inconsistent");
+    if (ok) {
+      g->replays++;
+      out->nq = c.nq; out->n_hits = t.nh; out->n_positions = t.npos;
+      out->d_hit_offsets = x->hit_base.as<uint64_t>(); out->d_hits = x->hits.as<hfm_mem_hit>();
+      out->d_positions = x->out_pairs.as<uint32_t>();
+      if (replayed) *replayed = 1;
+      return HFM_OK;
+    }
+  }
+  // a capacity was outgrown: the adaptive chain (same results), then capture again with
+  // the capacities it grew to
+  g->fallbacks++;
+  g->stale = true;
+  c.max_bases = std::max<uint64_t>(c.max_bases, g->h_bases[0] + g->h_bases[0] / 4);
+  RET(mems_device(x, c.d_q, c.d_qoff, c.nq, c.P.min_len, c.P.mode, g->bounds.empty() ? nullptr : g->bounds.data(),
+                  c.nb, c.P.max_hits, out));
+  c.pos_cap = std::max<uint64_t>(c.pos_cap, out->n_positions + out->n_positions / 4 + 4096);
+  if (replayed) *replayed = 0;
+  return HFM_OK;
+}
+
+extern "C" void hfm_mems_graph_free(hfm_graph* g) { free_graph(g); }
+
+extern "C" int hfm_index_share(hfm_index* x, hfm_index** out) {
+  if (!x || !out) return set_error(HFM_E_ARG, "NULL argument");
+  *out = nullptr;
+  std::lock_guard<std::mutex> lk(x->mu);
+  return make_shadow(x, out);
 }
 
 }  // extern "C"

@@ -24,16 +24,20 @@ struct ResolveArgs {
   uint32_t* walk_err;
   unsigned long long* steps;    // LF steps (nullptr: not counted)
   const uint32_t* block_first;  // segment containing the first position of each block
+  const uint64_t* total_dev;    // when set (graph-captured chains), the position count is read here
 };
 
 // block_first[b] = segment holding position b * blk (positions are CSR over segments).
+// Blocks at or past max_blocks (the map's size) are skipped: a chain with fixed capacities
+// runs this before it knows whether the positions fit.
 __global__ void k_block_first(const uint64_t* __restrict__ seg_off, uint32_t nseg, uint32_t blk,
-                              uint32_t* __restrict__ block_first) {
+                              uint32_t* __restrict__ block_first, uint64_t max_blocks = ~0ull) {
   uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nseg) return;
   uint64_t a = seg_off[s], e = seg_off[s + 1];
   if (a == e) return;
-  for (uint64_t b = (a + blk - 1) / blk; b <= (e - 1) / blk; b++) block_first[b] = s;
+  const uint64_t last = min((e - 1) / blk, max_blocks - 1);
+  for (uint64_t b = (a + blk - 1) / blk; b <= last; b++) block_first[b] = s;
 }
 
 // Segments [first, first + cnt) cover positions [b * blk, (b + 1) * blk) of block b.
@@ -56,11 +60,13 @@ __global__ void __launch_bounds__(RES_T) k_resolve(DevFm F, ResolveArgs A) {
   __shared__ uint32_t s_b[RES_BOUNDS_SMEM];
   __shared__ uint32_t s_first, s_cnt;
   if (threadIdx.x < 16) { S.C[threadIdx.x] = F.C[threadIdx.x]; }
+  const uint64_t total = A.total_dev ? *A.total_dev : A.total;
   uint64_t p0 = (uint64_t)blockIdx.x * RES_T;
-  uint64_t p1 = min(p0 + RES_T, A.total);
+  if (p0 >= total) return;                 // a grid sized for a capacity: blocks past the positions
+  uint64_t p1 = min(p0 + RES_T, total);
   if (threadIdx.x == 0) {
     uint32_t f, c;
-    block_segments(A.block_first, (A.total + RES_T - 1) / RES_T, A.nseg, f, c);
+    block_segments(A.block_first, (total + RES_T - 1) / RES_T, A.nseg, f, c);
     s_first = f; s_cnt = c;
   }
   bool smem_b = A.nb <= RES_BOUNDS_SMEM;
@@ -163,11 +169,14 @@ __global__ void __launch_bounds__(EXP_T) k_dedup_expand(const uint64_t* __restri
                                                         const uint64_t* __restrict__ uid,
                                                         const uint64_t* __restrict__ uoff,
                                                         const uint2* __restrict__ uout, uint2* __restrict__ out,
-                                                        const uint32_t* __restrict__ block_first) {
+                                                        const uint32_t* __restrict__ block_first,
+                                                        const uint64_t* __restrict__ total_dev = nullptr) {
   __shared__ uint64_t s_off[EXP_BLK + 1];
   __shared__ uint64_t s_src[EXP_BLK];
   __shared__ uint32_t s_first, s_cnt;
+  if (total_dev) total = *total_dev;
   uint64_t p0 = (uint64_t)blockIdx.x * EXP_BLK;
+  if (p0 >= total) return;                 // a grid sized for a capacity: blocks past the positions
   uint64_t p1 = min(p0 + EXP_BLK, total);
   if (threadIdx.x == 0) {
     uint32_t f, c;

@@ -607,6 +607,8 @@ struct MemsWork {
   uint32_t rerun;                     // 1: a rerun of overflowed reads (counted in still_ovf)
   uint32_t* work_log;                 // COUNT_TOUCH only: 4 u32 per read, [0] += Occ touches, [3] |= 1 on overflow
                                       // (the warp-per-read kernel also sets bit 1)
+  const uint32_t* n_dev;              // when set, the number of reads is read here (graph-captured chains)
+  __device__ __forceinline__ uint32_t count() const { return n_dev ? *n_dev : n; }
 };
 
 // Splits the fast pass's overflow list: the first `first_warp` entries (reads a schedule
@@ -614,9 +616,10 @@ struct MemsWork {
 // outgrew only the candidate list go to the per-thread rerun with a larger global list.
 __global__ void k_split_ovf(const uint32_t* __restrict__ list, uint32_t n, uint32_t first_warp,
                             const uint32_t* __restrict__ status, uint32_t* __restrict__ mid,
-                            uint32_t* __restrict__ n_mid, uint32_t* __restrict__ wrp, uint32_t* __restrict__ n_wrp) {
+                            uint32_t* __restrict__ n_mid, uint32_t* __restrict__ wrp, uint32_t* __restrict__ n_wrp,
+                            const uint32_t* __restrict__ n_dev = nullptr) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= n) return;
+  if (k >= (n_dev ? *n_dev : n)) return;
   uint32_t i = list[k];
   if (k < first_warp || (status[i] & ST_SET_OVF)) wrp[atomicAdd(n_wrp, 1u)] = i;
   else mid[atomicAdd(n_mid, 1u)] = i;
@@ -644,7 +647,8 @@ __global__ void __launch_bounds__(128, MINB) k_mems(DevFm Fw, DevFm Rv, const ui
   }
   uint64_t touches = 0;
   uint32_t i;
-  while (next_read(W.queue, W.n, W.ids, i)) {
+  const uint32_t nreads = W.count();
+  while (next_read(W.queue, nreads, W.ids, i)) {
     uint32_t st = ST_OK;
     uint64_t o = qoff[i];
     uint64_t t0 = touches;
@@ -803,6 +807,14 @@ struct SegWork {
   uint32_t* fx_exit;              // first pivot past the segment when it did not meet it
   uint64_t* fx_off;               // its own candidates (pivots before fx_conv) in the pool
   uint32_t* fx_cnt;
+  // when set (graph-captured chains), the counts are read here: units = *n_units_dev,
+  // long reads = *n_long_dev, short reads = n_fast - *n_long_dev
+  const uint64_t* n_units_dev;
+  const uint64_t* n_long_dev;
+  uint32_t n_fast;
+  __device__ __forceinline__ uint32_t units() const { return n_units_dev ? (uint32_t)*n_units_dev : n_units; }
+  __device__ __forceinline__ uint32_t longs() const { return n_long_dev ? (uint32_t)*n_long_dev : n_long; }
+  __device__ __forceinline__ uint32_t shorts() const { return n_long_dev ? n_fast - (uint32_t)*n_long_dev : n_short; }
 };
 
 // flags[k] = 1 when read ids[k] (k itself without ids) is longer than min_len.
@@ -834,9 +846,9 @@ __global__ void k_split_ids(const uint32_t* __restrict__ ids, uint32_t n, const 
 
 __global__ void k_unit_fill(const uint32_t* __restrict__ long_ids, uint32_t n_long,
                             const uint64_t* __restrict__ unit_base, uint32_t* __restrict__ unit_read,
-                            uint32_t* __restrict__ unit_k) {
+                            uint32_t* __restrict__ unit_k, const uint64_t* __restrict__ n_long_dev = nullptr) {
   uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= n_long) return;
+  if (r >= (n_long_dev ? (uint32_t)*n_long_dev : n_long)) return;
   uint64_t b = unit_base[r], e = unit_base[r + 1];
   for (uint64_t u = b; u < e; u++) { unit_read[u] = long_ids[r]; unit_k[u] = (uint32_t)(u - b); }
 }
@@ -858,14 +870,15 @@ __global__ void __launch_bounds__(128, MINB) k_mems_seg(DevFm Fw, DevFm Rv, cons
   uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   Cand* cands = W.cands + tid * W.cand_cap;
   uint64_t touches = 0;
-  const uint32_t njobs = G.n_units + G.n_short;
+  const uint32_t n_units = G.units();
+  const uint32_t njobs = n_units + G.shorts();
   uint32_t u;
   while (next_read(W.queue, njobs, nullptr, u)) {
-    const bool unit = u < G.n_units;
+    const bool unit = u < n_units;
     uint32_t i, s, e;
     uint32_t* bits = nullptr;
     if (unit) i = G.unit_read[u];
-    else i = G.short_ids[u - G.n_units];
+    else i = G.short_ids[u - n_units];
     uint64_t o = qoff[i];
     uint32_t n = (uint32_t)(qoff[i + 1] - o);
     if (unit) {
@@ -940,7 +953,8 @@ __global__ void __launch_bounds__(128, MINB) k_mems_fix(DevFm Fw, DevFm Rv, cons
   Cand* cands = W.cands + tid * W.cand_cap;
   uint64_t touches = 0;
   uint32_t u;
-  while (next_read(W.queue, G.n_units, nullptr, u)) {
+  const uint32_t n_units = G.units();
+  while (next_read(W.queue, n_units, nullptr, u)) {
     uint32_t i = G.unit_read[u], k = G.unit_k[u];
     G.fx_entry[u] = ~0u; G.fx_conv[u] = ~0u; G.fx_exit[u] = ~0u; G.fx_off[u] = 0; G.fx_cnt[u] = 0;
     if (k == 0 || G.exit_pivot[u - 1] == ~0u || G.exit_pivot[u] == ~0u) continue;
@@ -992,7 +1006,8 @@ __global__ void __launch_bounds__(128, MINB) k_mems_merge(DevFm Fw, DevFm Rv, co
   Cand* cands = W.cands + tid * W.cand_cap;
   uint64_t touches = 0;
   uint32_t r;
-  while (next_read(G.merge_queue, G.n_long, nullptr, r)) {
+  const uint32_t n_long = G.longs();
+  while (next_read(G.merge_queue, n_long, nullptr, r)) {
     uint32_t i = G.long_ids[r];
     uint64_t o = qoff[i];
     uint32_t n = (uint32_t)(qoff[i + 1] - o);
@@ -1398,7 +1413,7 @@ __global__ void __launch_bounds__(128) k_mems_warp(DevFm Fw, DevFm Rv, const uin
     uint32_t k = 0;
     if (lane == 0) k = atomicAdd(W.queue, 1u);
     k = __shfl_sync(0xFFFFFFFFu, k, 0);
-    if (k >= W.n) break;
+    if (k >= W.count()) break;
     uint32_t i = W.ids[k];
     uint32_t st = ST_OK;
     uint64_t o = qoff[i];

@@ -131,6 +131,15 @@ class _Handle:
         if getattr(self, "h", None) and self.h.value and L._lib is not None:
             L._lib.hfm_index_free(self.h)
             self.h = None
+        self._src = None
+
+    def share(self) -> "_Handle":
+        """hfm_index_share: another handle on this index (own stream and work buffers)."""
+        o = _Handle.__new__(_Handle)
+        h = C.c_void_p()
+        L.check(L.lib().hfm_index_share(self.h, C.byref(h)))
+        o.h, o.kind, o.device, o._buf, o._src = h, self.kind, self.device, self._buf, self
+        return o
 
     def info(self) -> L.HfmIndexInfo:
         info = L.HfmIndexInfo()

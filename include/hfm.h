@@ -135,6 +135,12 @@ int hfm_build_index_gpu(const uint8_t* codes, const uint64_t* seq_off, uint32_t 
 int hfm_index_load(const uint8_t* bincode, size_t len, int kind, const hfm_opts* opts, hfm_index** out);
 void hfm_index_free(hfm_index* idx);
 int hfm_index_info_get(const hfm_index* idx, hfm_index_info* out);
+/* A second handle on the same device-resident index, with its own stream and work buffers
+ * (no counterpart in the reference, whose process-wide context serialises every call,
+ * src/gpu/context_cache.rs:5-19): calls on the two handles run concurrently without a
+ * second copy of the index in HBM.  `idx` must outlive the shares; free each share with
+ * hfm_index_free (it leaves the index's buffers to `idx`). */
+int hfm_index_share(hfm_index* idx, hfm_index** out);
 
 /* ---- queries, host buffers (the drop-in boundary) ------------------------ */
 
@@ -218,6 +224,28 @@ typedef struct hfm_sched {
 int hfm_mems_batch_device_sched(hfm_index* idx, const uint8_t* d_q, const uint64_t* d_q_off, uint32_t nq,
                                 uint32_t min_len, uint32_t mode, const uint32_t* ref_bounds, uint32_t n_bounds,
                                 uint32_t max_hits, const hfm_sched* sched, hfm_dev_mems* out);
+
+/* CUDA-graph-captured SMEM/MEM pass chain (no counterpart in the reference, whose batch
+ * search reads counts back to the host between its passes, src/gpu/mem_find.rs:213-244).
+ * hfm_mems_graph_create captures, for batches of nq reads at the fixed device addresses
+ * d_q / d_q_off, the whole search-CSR-resolve chain of hfm_mems_batch_device into one CUDA
+ * graph: every pass runs over capacities fixed at capture (the handle's pool capacities,
+ * as hfm_mems_reserve set them; max_positions resolved positions; long-read segments for
+ * up to max_bases codes per batch) and reads its counts from device memory, so nothing
+ * waits on the host inside the chain.  The graph works on a private copy of the handle's
+ * buffers and stream and shares the index.  hfm_mems_graph_launch replays it for the reads
+ * the caller has written to d_q / d_q_off (nq reads, offsets from 0): it reads the batch's
+ * length first, replays, and checks the overflow flags; a batch that outgrew a capacity is
+ * rerun on the adaptive chain (same results) and the graph is captured again with the
+ * grown capacities (*replayed = 0; 1 when the replay's outputs were returned).  Outputs
+ * are those of hfm_mems_batch_device, in the graph's own buffers, valid until the next
+ * launch.  Calls on one graph must not overlap. */
+typedef struct hfm_graph hfm_graph;
+int hfm_mems_graph_create(hfm_index* idx, const uint8_t* d_q, const uint64_t* d_q_off, uint32_t nq, uint64_t max_bases,
+                          uint32_t min_len, uint32_t mode, const uint32_t* ref_bounds, uint32_t n_bounds,
+                          uint32_t max_hits, uint64_t max_positions, hfm_graph** out);
+int hfm_mems_graph_launch(hfm_graph* g, hfm_dev_mems* out, uint32_t* replayed);
+void hfm_mems_graph_free(hfm_graph* g);
 
 /* Pre-sizes a handle's SMEM/MEM work pools and result arrays for a batch of nq reads
  * expected to produce `intervals` candidate intervals, `hits` MemHits and `positions`
