@@ -165,31 +165,28 @@ __device__ __forceinline__ void split_by_symbol(const DevFm& F, uint32_t lo, uin
 #pragma unroll
     for (int s = 0; s <= 4; s++) f(s, d[s], r[s], L.sbi);
   } else {
-    // Wide records: the codes in a rolled loop up to `last` (the highest code the caller
-    // needs), planes in registers and each count word read again from L1 when used, so
-    // the two borders do not hold 32 registers of counts through the loop.
-    const uint32_t pl = lo ? lo - 1 : 0u, ph = hi ? hi - 1 : 0u;
-    const uint32_t bl = pl >> 6, bh = ph >> 6;
-    const uint32_t* rl = reinterpret_cast<const uint32_t*>(F.occ + (size_t)bl * OCC_WIDE_U4);
-    const uint32_t* rh = reinterpret_cast<const uint32_t*>(F.occ + (size_t)bh * OCC_WIDE_U4);
-    const uint4 l0 = __ldg(F.occ + (size_t)bl * OCC_WIDE_U4 + 2), l1 = __ldg(F.occ + (size_t)bl * OCC_WIDE_U4 + 3);
-    const uint4 h0 = __ldg(F.occ + (size_t)bh * OCC_WIDE_U4 + 2), h1 = __ldg(F.occ + (size_t)bh * OCC_WIDE_U4 + 3);
-    const uint64_t lowl = lo ? (2ull << (pl & 63)) - 1ull : 0ull, lowh = hi ? (2ull << (ph & 63)) - 1ull : 0ull;
-    const uint64_t lp0 = u2to64(l0.x, l0.y), lp1 = u2to64(l0.z, l0.w), lp2 = u2to64(l1.x, l1.y), lp3 = u2to64(l1.z, l1.w);
-    const uint64_t hp0 = u2to64(h0.x, h0.y), hp1 = u2to64(h0.z, h0.w), hp2 = u2to64(h1.x, h1.y), hp3 = u2to64(h1.z, h1.w);
-    const uint32_t sbl = bl >> SB_BLOCK_SHIFT, sbh = bh >> SB_BLOCK_SHIFT;
-#pragma unroll 1
-    for (uint32_t s = 0; s <= last; s++) {
-      const uint64_t sel0 = (s & 1) ? 0ull : ~0ull, sel1 = (s & 2) ? 0ull : ~0ull;
-      const uint64_t sel2 = (s & 4) ? 0ull : ~0ull, sel3 = (s & 8) ? 0ull : ~0ull;
-      const uint64_t ml = lowl & (lp0 ^ sel0) & (lp1 ^ sel1) & (lp2 ^ sel2) & (lp3 ^ sel3);
-      const uint64_t mh = lowh & (hp0 ^ sel0) & (hp1 ^ sel1) & (hp2 ^ sel2) & (hp3 ^ sel3);
-      const uint32_t sh = (s & 1) * 16;
-      const uint32_t dl = (__ldg(rl + (s >> 1)) >> sh) & 0xFFFFu, dh = (__ldg(rh + (s >> 1)) >> sh) & 0xFFFFu;
-      const uint32_t a = dl + (uint32_t)__popcll(ml);
-      uint32_t v = (dh + (uint32_t)__popcll(mh)) - a;
-      if (sbl != sbh) v += sb_count(F, sbh, s) - sb_count(F, sbl, s);
-      f((int)s, v, a, sbl);
+    // Wide records: the codes in groups of four sharing bits 3 and 2 (a split tree over the
+    // planes, consumed as it is formed: no array of 16 masks or counts), groups past `last`
+    // (the highest code the caller needs) skipped.
+    const Border<FMT> L = load_border<FMT>(F, lo), H = load_border<FMT>(F, hi);
+    const bool same_sb = L.sbi == H.sbi;
+    const uint64_t lp0 = L.plane(0), lp1 = L.plane(1), lp2 = L.plane(2), lp3 = L.plane(3);
+    const uint64_t hp0 = H.plane(0), hp1 = H.plane(1), hp2 = H.plane(2), hp3 = H.plane(3);
+#pragma unroll
+    for (int g = 0; g < 4; g++) {
+      if (4u * g > last) break;
+      const uint64_t gl = L.low & ((g & 2) ? lp3 : ~lp3) & ((g & 1) ? lp2 : ~lp2);
+      const uint64_t gh = H.low & ((g & 2) ? hp3 : ~hp3) & ((g & 1) ? hp2 : ~hp2);
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        const int s = 4 * g + k;
+        const uint64_t ml = gl & ((k & 2) ? lp1 : ~lp1) & ((k & 1) ? lp0 : ~lp0);
+        const uint64_t mh = gh & ((k & 2) ? hp1 : ~hp1) & ((k & 1) ? hp0 : ~hp0);
+        const uint32_t a = L.delta(s) + (uint32_t)__popcll(ml);
+        uint32_t v = (H.delta(s) + (uint32_t)__popcll(mh)) - a;
+        if (!same_sb) v += sb_count(F, H.sbi, s) - sb_count(F, L.sbi, s);
+        f(s, v, a, L.sbi);
+      }
     }
   }
 }

@@ -125,7 +125,7 @@ def test_autotune_keeps_results(oracle):
     assert (res["mems_variant"], res["seg_len"]) in [(3, 512), (3, 256), (3, 1024), (2, 512)]
     assert h.tuning() == {"mems_variant": res["mems_variant"], "seg_len": res["seg_len"]}
     assert len(res["candidates_ms"]) == 4 and all(v > 0 for v in res["candidates_ms"].values())
-    for v, sl in [(3, 64), (3, 4096), (2, 512), (0, 512)]:
+    for v, sl in [(3, 64), (3, 4096), (2, 512), (4, 512)]:
         h.set_tuning(v, sl)
         _same(h.mems_sched_packed(flat, off, 19, 0, bounds, 128), want)
     with pytest.raises(FmIndexError):
