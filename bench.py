@@ -515,11 +515,11 @@ def genome_workloads(args, device, torch):
 
     def with_tuning(variant, fn):
         saved = h.tuning()
-        h.set_tuning(variant, saved["seg_len"])
+        h.set_tuning(variant, saved["seg_len"], saved["queue_chunk"], saved["threads_per_read"])
         try:
             return fn()
         finally:
-            h.set_tuning(saved["mems_variant"], saved["seg_len"])
+            h.set_tuning(saved["mems_variant"], saved["seg_len"], saved["queue_chunk"], saved["threads_per_read"])
 
     n3 = args.genome_reads
     steps = args.genome_steps
@@ -773,7 +773,7 @@ def main():
     plain_launch = None
     if not args.no_plain_launch:
         saved = h.tuning()
-        h.set_tuning(4, saved["seg_len"])
+        h.set_tuning(4, saved["seg_len"], 1, 1)
         for _ in range(max(1, args.warmup // 2)):
             step(plain=True)
         torch.cuda.synchronize()
@@ -786,7 +786,7 @@ def main():
         ev1.record(stream)
         torch.cuda.synchronize()
         lms = ev0.elapsed_time(ev1)
-        h.set_tuning(saved["mems_variant"], saved["seg_len"])
+        h.set_tuning(saved["mems_variant"], saved["seg_len"], saved["queue_chunk"], saved["threads_per_read"])
         if dist:
             t = torch.tensor([lms], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)

@@ -65,7 +65,13 @@ class HfmSched(C.Structure):
 
 
 class HfmTuning(C.Structure):
-    _fields_ = [("mems_variant", C.c_uint32), ("seg_len", C.c_uint32)]
+    _fields_ = [("mems_variant", C.c_uint32), ("seg_len", C.c_uint32), ("queue_chunk", C.c_uint32),
+                ("threads_per_read", C.c_uint32)]
+
+
+# hfm_autotune_mems candidates {variant, seg_len, queue_chunk, threads_per_read}, in order
+TUNE_CANDIDATES = [(3, 512, 1, 1), (3, 256, 1, 1), (3, 1024, 1, 1), (2, 512, 1, 1), (3, 512, 4, 1), (3, 512, 16, 1),
+                   (3, 512, 1, 32)]
 
 
 class HfmStats(C.Structure):
@@ -135,6 +141,8 @@ SIGNATURES = {
                                         C.POINTER(C.c_void_p)]),
     "hfm_mems_graph_launch": (C.c_int, [C.c_void_p, C.POINTER(HfmDevMems), C.POINTER(C.c_uint32)]),
     "hfm_mems_graph_free": (None, [C.c_void_p]),
+    "hfm_mems_graph_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                      C.POINTER(C.c_uint32)]),
     "hfm_mems_reserve": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64]),
     "hfm_probe_gather": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
 }

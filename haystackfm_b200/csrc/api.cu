@@ -125,6 +125,9 @@ struct hfm_index {
       fxo, fxn, npos;
   uint32_t flags = 0;
   uint32_t seg_len = 512;  // SMEM reads longer than 2 * seg_len take the segmented sweep
+  uint32_t queue_chunk = 1;       // reads a per-thread kernel takes from its queue per atomic
+  uint32_t threads_per_read = 1;  // 32: every read on the warp-per-read kernel
+  DevBuf iota;                    // 0..nq-1 (the order of a batch sent whole to the warp kernel)
   int mems_variant = 3;   // SMEM fast-kernel variant (see mems_device): 2 local 32-entry
                           // candidate lists; 3 global 1024-entry lists
   int num_sms = 0;
@@ -168,8 +171,8 @@ static int build_device_fm(const HostFm& h, FmDev& f, cudaStream_t s) {
   const uint64_t width = h.encoding == 0 ? h.num_planes : L;
   // Decode the reference records (compacted lanes, u32 superblock count + u16 delta per
   // lane) into whole per-symbol counts and 4 symbol-code bitplanes, then re-encode them as
-  // the device records.  Superblocks of the device layout are 1024 records, so every
-  // count within one fits a u16.
+  // the device records: whole counts (wide) or counts from the start of the device
+  // superblock of 1024 records, which fit a u16 (narrow).
   auto decode = [&](uint64_t b, uint32_t cnt[16], uint64_t planes[4]) {
     const uint8_t* r = h.block_data + b * h.block_stride;
     uint64_t words[16] = {0};
@@ -212,8 +215,8 @@ static int build_device_fm(const HostFm& h, FmDev& f, cudaStream_t s) {
         rec[0] = d[1] | (d[2] << 16); rec[1] = d[3] | (d[4] << 16);
         std::memcpy(rec + 2, &planes[0], 8); std::memcpy(rec + 4, &planes[1], 8); std::memcpy(rec + 6, &planes[2], 8);
       } else {
-        for (int c = 0; c < 16; c += 2) rec[c / 2] = d[c] | (d[c + 1] << 16);
-        std::memcpy(rec + 8, planes, 32);
+        std::memcpy(rec, cnt, 64);           // whole counts before the record
+        std::memcpy(rec + 16, planes, 32);
       }
       // sampled-SA record: bits + rank before (validated equal to the stored sb + delta)
       uint64_t word; uint32_t sbs; uint16_t dd;
@@ -317,7 +320,7 @@ static int read_u64(hfm_index* x, const uint64_t* dsrc, uint64_t& v) {
 
 static constexpr uint32_t BS_SET_CAP = 64;     // fast-path interval-set capacity (backward search)
 static constexpr uint32_t BS_WARP_SET_CAP = 8192;   // long-tail pass, per warp
-static constexpr uint32_t MEM_SET_CAP = 768;   // fast-path interval-set capacity (SMEM / MEM)
+static constexpr uint32_t MEM_SET_CAP = FAST_SET_CAP;   // fast-path interval-set capacity (SMEM / MEM)
 static constexpr uint32_t MEM_WARP_SET_CAP = 8192;  // long-tail pass, per warp
 static constexpr int MEM_KC = 32;              // fast-path candidate capacity (thread-local)
 static constexpr uint32_t MID_CAND_CAP = 1024;  // candidate list of the per-thread rerun (global memory)
@@ -554,6 +557,14 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   if (mode > 1) return set_error(HFM_E_ARG, "mode must be 0 (SMEM) or 1 (MEM)");
   const uint32_t* order = sc ? sc->d_order : nullptr;
   uint32_t n_warp = sc ? sc->n_warp : 0;
+  if (!sc && x->threads_per_read == 32 && x->mems_variant != MEMS_PLAIN && nq) {
+    // every read on the warp-per-read kernel: the identity order, all of it routed
+    RET(x->iota.ensure((size_t)nq * 4));
+    k_iota<<<(nq + 255) / 256, 256, 0, x->stream>>>(x->iota.as<uint32_t>(), nq);
+    CK(cudaGetLastError());
+    order = x->iota.as<uint32_t>();
+    n_warp = nq;
+  }
   uint32_t* wlog = sc ? sc->d_work_log : nullptr;
   if (n_warp > nq) return set_error(HFM_E_ARG, "sched.n_warp exceeds nq");
   if (n_warp && !order) return set_error(HFM_E_ARG, "sched.n_warp needs sched.d_order");
@@ -710,6 +721,7 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
     if (!plain && n_fast > 0 && n_long == 0) {     // with long reads, k_mems_seg runs the short reads too
       MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, variant == 3 ? x->cwork.as<Cand>() : nullptr,
                  variant == 3 ? FAST_CAND_CAP : 0u, &dctr(x)->queue, fast_ids, n_fast, &dctr(x)->still_ovf, 0u, wlog};
+      W.chunk = x->queue_chunk;
       unsigned grid = (unsigned)(threads / 128);
       if (x->memwork.cap < (size_t)grid * 128 * 4 * MEM_SET_CAP * 16) return set_error(HFM_E_ARG, "internal: work area too small");
       if (variant == 3 && x->cwork.cap < (size_t)grid * 128 * FAST_CAND_CAP * sizeof(Cand))
@@ -742,6 +754,7 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
                 x->fxc.as<uint32_t>(), x->fxx.as<uint32_t>(), x->fxo.as<uint64_t>(), x->fxn.as<uint32_t>()};
       MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), FAST_CAND_CAP, &dctr(x)->seg_queue, nullptr,
                  0u, &dctr(x)->still_ovf, 0u, wlog};
+      W.chunk = x->queue_chunk;
       MemsWork Wf = W;
       Wf.queue = &dctr(x)->fix_queue;
       uint64_t ts = std::min<uint64_t>(threads / 128 * 128, (n_units + n_fast + 127) / 128 * 128);
@@ -941,6 +954,7 @@ struct FixedChain {
   uint64_t pos_cap;
   GraphTotals* d_tot; GraphTotals* h_tot;     // device / pinned host
   uint64_t threads;            // resident threads of the persistent kernels
+  uint32_t warp_cap = MEM_WARP_SET_CAP, warp_cands = 1024;   // warp tier: intervals per set, candidates
 };
 
 static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
@@ -984,8 +998,12 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
     x->seg_cap = std::max<uint64_t>(x->seg_cap, ucap * 24 + 65536);
     RET(x->segpool.ensure(x->seg_cap * sizeof(Cand)));
   }
-  const uint32_t wgrid = (uint32_t)x->num_sms * 4;                  // warp tier: 16 warps per SM
-  RET(x->work.ensure((size_t)wgrid * 4 * MEM_WARP_SET_CAP * 4 * 16));
+  // warp tier: up to 16 warps per SM, at most 2 GB of sets
+  const uint64_t per_warp = (uint64_t)c.warp_cap * 4 * 16;
+  const uint64_t wwarps = std::max<uint64_t>(4, std::min<uint64_t>((uint64_t)x->num_sms * 16, (2ull << 30) / per_warp));
+  const uint32_t wgrid = (uint32_t)((wwarps + 3) / 4);
+  RET(x->work.ensure((size_t)wgrid * 4 * per_warp));
+  RET(x->cwork.ensure(std::max<size_t>((size_t)threads * FAST_CAND_CAP, (size_t)wgrid * 4 * c.warp_cands) * sizeof(Cand)));
   RET(x->hit_base.ensure(((size_t)nq + 1) * 8));
   RET(x->hits.ensure((hcap + 1) * 32));
   RET(x->npos_scan.ensure((hcap + 1) * 8));
@@ -1038,6 +1056,7 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
                 n_units_dev, n_long_dev, nq};
       MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), FAST_CAND_CAP, &dc->seg_queue, nullptr,
                  0u, &dc->still_ovf, 0u, nullptr, nullptr};
+      W.chunk = x->queue_chunk;
       MemsWork Wf = W;
       Wf.queue = &dc->fix_queue;
       const unsigned g = (unsigned)(threads / 128);
@@ -1052,6 +1071,7 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
   } else if (launch) {
     MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), FAST_CAND_CAP, &dc->queue, nullptr, nq,
                &dc->still_ovf, 0u, nullptr, nullptr};
+    W.chunk = x->queue_chunk;
     WITH_FMT(fmt, {
       k_mems<false, 32, 0, 8, FM><<<(unsigned)(threads / 128), 128, 0, x->stream>>>(Fw.d, Rv.d, cfw, crv, c.d_q,
                                                                                     c.d_qoff, P, ivp, hp, o, W);
@@ -1075,7 +1095,7 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
       k_mems<false, 32, 0, 8, FM><<<(unsigned)(tm / 128), 128, 0, x->stream>>>(Fw.d, Rv.d, cfw, crv, c.d_q, c.d_qoff, P,
                                                                                 ivp, hp, o2, Wm);
     });
-    MemsWork Ww{x->work.as<BIv>(), MEM_WARP_SET_CAP, x->cwork.as<Cand>(), 1024u, &dc->queue2, x->ovf2.as<uint32_t>(), 0u,
+    MemsWork Ww{x->work.as<BIv>(), c.warp_cap, x->cwork.as<Cand>(), c.warp_cands, &dc->queue2, x->ovf2.as<uint32_t>(), 0u,
                 &dc->still_ovf, 1u, nullptr, &dc->n_wrp};
     k_mems_warp<false><<<wgrid, 128, 0, x->stream>>>(Fw.d, Rv.d, cfw, crv, c.d_q, c.d_qoff, P, ivp, hp, o, Ww);
     CK(cudaGetLastError());
@@ -1223,6 +1243,7 @@ static int make_shadow(hfm_index* x, hfm_index** out) {
   std::unique_ptr<hfm_index> sh(new hfm_index());
   sh->device = x->device; sh->kind = x->kind; sh->flags = x->flags; sh->num_sms = x->num_sms;
   sh->seg_len = x->seg_len; sh->mems_variant = x->mems_variant; sh->count_work = x->count_work;
+  sh->queue_chunk = x->queue_chunk; sh->threads_per_read = x->threads_per_read;
   sh->timeout_ms = x->timeout_ms;
   sh->shared_index = true;
   for (int k = 0; k < 2; k++) {
@@ -1309,7 +1330,7 @@ void hfm_index_free(hfm_index* x) {
                     &x->hkeys, &x->hslot, &x->hflags, &x->huid, &x->urow, &x->ulen, &x->uoff, &x->uout,
                     &x->blockmap, &x->blockmap2, &x->ovf2, &x->ovf3, &x->lflag, &x->lpos, &x->sids, &x->lids,
                     &x->ucount, &x->ubase, &x->uread, &x->uk, &x->ubits, &x->uexit, &x->ust, &x->ucoff, &x->ucnt,
-                    &x->segpool, &x->fxe, &x->fxc, &x->fxx, &x->fxo, &x->fxn, &x->npos})
+                    &x->segpool, &x->fxe, &x->fxc, &x->fxx, &x->fxo, &x->fxn, &x->npos, &x->iota})
     b->release();
   for (auto& e : x->ev) if (e) cudaEventDestroy(e);
   for (auto& e : x->evk) if (e) cudaEventDestroy(e);
@@ -1340,6 +1361,8 @@ int hfm_get_tuning(const hfm_index* x, hfm_tuning* t) {
   if (!x || !t) return set_error(HFM_E_ARG, "NULL argument");
   t->mems_variant = (uint32_t)x->mems_variant;
   t->seg_len = x->seg_len;
+  t->queue_chunk = x->queue_chunk;
+  t->threads_per_read = x->threads_per_read;
   return HFM_OK;
 }
 
@@ -1347,9 +1370,13 @@ int hfm_set_tuning(hfm_index* x, const hfm_tuning* t) {
   if (!x || !t) return set_error(HFM_E_ARG, "NULL argument");
   if (t->mems_variant < 2 || t->mems_variant > 4) return set_error(HFM_E_ARG, "mems_variant must be 2, 3 or 4");
   if (t->seg_len < 64 || t->seg_len > SEG_MAX || t->seg_len % 32) return set_error(HFM_E_ARG, "seg_len must be a multiple of 32 in 64..4096");
+  if (t->queue_chunk < 1 || t->queue_chunk > 64) return set_error(HFM_E_ARG, "queue_chunk must be in 1..64");
+  if (t->threads_per_read != 1 && t->threads_per_read != 32) return set_error(HFM_E_ARG, "threads_per_read must be 1 or 32");
   std::lock_guard<std::mutex> lk(x->mu);
   x->mems_variant = (int)t->mems_variant;
   x->seg_len = t->seg_len;
+  x->queue_chunk = t->queue_chunk;
+  x->threads_per_read = t->threads_per_read;
   return HFM_OK;
 }
 
@@ -1360,52 +1387,30 @@ int hfm_autotune_mems(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, 
   if (x->kind != HFM_KIND_BIDIR) return set_error(HFM_E_ARG, "MEM/SMEM search needs a bidirectional index");
   reps = std::max(1u, reps);
   Guard g(x);
-  const hfm_tuning cands[] = {{3, 512}, {3, 256}, {3, 1024}, {2, 512}};
-  const int nc = (int)(sizeof(cands) / sizeof(cands[0]));
-  int saved_v = x->mems_variant;
-  uint32_t saved_s = x->seg_len;
+  // HFM_TUNE_CANDIDATES settings, in the order include/hfm.h lists them
+  const hfm_tuning cands[HFM_TUNE_CANDIDATES] = {{3, 512, 1, 1}, {3, 256, 1, 1}, {3, 1024, 1, 1}, {2, 512, 1, 1},
+                                                 {3, 512, 4, 1}, {3, 512, 16, 1}, {3, 512, 1, 32}};
+  const hfm_tuning saved{(uint32_t)x->mems_variant, x->seg_len, x->queue_chunk, x->threads_per_read};
+  auto apply = [&](const hfm_tuning& t) {
+    x->mems_variant = (int)t.mems_variant; x->seg_len = t.seg_len;
+    x->queue_chunk = t.queue_chunk; x->threads_per_read = t.threads_per_read;
+  };
   float best_ms = 0.f;
   int best_k = -1;
-  for (int k = 0; k < nc; k++) {
-    x->mems_variant = (int)cands[k].mems_variant;
-    x->seg_len = cands[k].seg_len;
+  for (int k = 0; k < HFM_TUNE_CANDIDATES; k++) {
+    apply(cands[k]);
     float t = 0.f;
     for (uint32_t r = 0; r <= reps; r++) {       // first run warms the pools
       hfm_dev_mems out;
       int rc = mems_device(x, d_q, d_qoff, nq, min_len, mode, ref_bounds, nb, cap, &out);
-      if (rc) { x->mems_variant = saved_v; x->seg_len = saved_s; return rc; }
+      if (rc) { apply(saved); return rc; }
       if (r > 0) t = r == 1 ? x->stats.ms_total : std::min(t, x->stats.ms_total);
     }
     if (times_ms) times_ms[k] = t;
     if (best_k < 0 || t < best_ms) { best_ms = t; best_k = k; }
   }
-  x->mems_variant = (int)cands[best_k].mems_variant;
-  x->seg_len = cands[best_k].seg_len;
+  apply(cands[best_k]);
   *best = cands[best_k];
-  return HFM_OK;
-}
-
-int hfm_mems_reserve(hfm_index* x, uint32_t nq, uint64_t intervals, uint64_t hits, uint64_t positions) {
-  if (!x) return set_error(HFM_E_ARG, "NULL argument");
-  Guard g(x);
-  // the search pools (intervals of every candidate, MemHits) and the result arrays
-  x->miv_cap = std::max<uint64_t>(x->miv_cap, intervals + 4096);
-  x->hit_cap = std::max<uint64_t>(x->hit_cap, hits + 4096);
-  RET(x->mivpool.ensure(x->miv_cap * 16)); x->miv_cap = x->mivpool.cap / 16;
-  RET(x->hitpool.ensure(x->hit_cap * 32)); x->hit_cap = x->hitpool.cap / 32;
-  RET(x->hits.ensure(hits * 32 + 32));
-  RET(x->npos_scan.ensure((hits + 1) * 8));
-  RET(x->out_pairs.ensure(positions * 8 + 8));
-  RET(x->hit_start.ensure((size_t)nq * 8 + 8)); RET(x->hit_count.ensure((size_t)nq * 4 + 4));
-  RET(x->hit_base.ensure(((size_t)nq + 1) * 8));
-  RET(x->status.ensure((size_t)nq * 4 + 4)); RET(x->ovf.ensure((size_t)nq * 4 + 4));
-  return HFM_OK;
-}
-
-int hfm_set_timeout(hfm_index* x, uint32_t ms) {
-  if (!x) return set_error(HFM_E_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lk(x->mu);
-  x->timeout_ms = ms;
   return HFM_OK;
 }
 
@@ -1521,7 +1526,7 @@ struct hfm_graph {
   FixedChain c{};
   bool stale = true;                 // capture (again) before the next replay
   uint64_t* h_bases = nullptr;       // pinned: the batch's total codes, read before each replay
-  uint32_t replays = 0, fallbacks = 0;
+  uint32_t replays = 0, fallbacks = 0, last_reason = 0;
   DevBuf tot;
   std::vector<uint32_t> bounds;      // host copy of the reference bounds (for the adaptive rerun)
 };
@@ -1608,17 +1613,23 @@ extern "C" int hfm_mems_graph_launch(hfm_graph* g, hfm_dev_mems* out, uint32_t* 
   // the one read before the replay: the batch must fit the captured segment capacity
   CK(cudaMemcpyAsync(g->h_bases, c.d_qoff + c.nq, 8, cudaMemcpyDeviceToHost, x->stream));
   RET(wait_stream(x));
-  bool ok = g->h_bases[0] <= c.max_bases;
-  if (ok) {
+  uint32_t reason = g->h_bases[0] <= c.max_bases ? 0u : HFM_GRAPH_BASES;
+  if (!reason) {
     if (g->stale) RET(capture(g));
     CK(cudaGraphLaunch(g->exec, x->stream));
     RET(wait_stream(x));
     const Counters& k = *x->h_ctr;
     const GraphTotals& t = *c.h_tot;
-    ok = k.iv_used <= x->miv_cap && k.hit_used <= x->hit_cap && k.seg_used <= x->seg_cap && k.still_ovf == 0 &&
-         t.ovf == 0;
     if (k.walk_err) return set_error(HFM_E_WALK, "LF walk exceeded sample_rate steps: index inconsistent");
-    if (ok) {
+    reason = (k.iv_used > x->miv_cap ? HFM_GRAPH_INTERVALS : 0u) | (k.hit_used > x->hit_cap ? HFM_GRAPH_HITS : 0u) |
+             (k.seg_used > x->seg_cap ? HFM_GRAPH_SEGMENTS : 0u) | (k.still_ovf ? HFM_GRAPH_WARP_SETS : 0u) |
+             (t.ovf ? HFM_GRAPH_POSITIONS : 0u);
+    if (reason & HFM_GRAPH_WARP_SETS) {       // the next capture gets larger warp-tier sets
+      c.warp_cap = std::min<uint32_t>(c.warp_cap * 4, 1u << 22);
+      c.warp_cands = std::min<uint32_t>(c.warp_cands * 4, 1u << 20);
+    }
+    g->last_reason = reason;
+    if (!reason) {
       g->replays++;
       out->nq = c.nq; out->n_hits = t.nh; out->n_positions = t.npos;
       out->d_hit_offsets = x->hit_base.as<uint64_t>(); out->d_hits = x->hits.as<hfm_mem_hit>();
@@ -1629,6 +1640,7 @@ extern "C" int hfm_mems_graph_launch(hfm_graph* g, hfm_dev_mems* out, uint32_t* 
   }
   // a capacity was outgrown: the adaptive chain (same results), then capture again with
   // the capacities it grew to
+  g->last_reason = reason;
   g->fallbacks++;
   g->stale = true;
   c.max_bases = std::max<uint64_t>(c.max_bases, g->h_bases[0] + g->h_bases[0] / 4);
@@ -1640,6 +1652,14 @@ extern "C" int hfm_mems_graph_launch(hfm_graph* g, hfm_dev_mems* out, uint32_t* 
 }
 
 extern "C" void hfm_mems_graph_free(hfm_graph* g) { free_graph(g); }
+
+extern "C" int hfm_mems_graph_info(const hfm_graph* g, uint32_t* replays, uint32_t* fallbacks, uint32_t* last_reason) {
+  if (!g) return set_error(HFM_E_ARG, "NULL argument");
+  if (replays) *replays = g->replays;
+  if (fallbacks) *fallbacks = g->fallbacks;
+  if (last_reason) *last_reason = g->last_reason;
+  return HFM_OK;
+}
 
 extern "C" int hfm_index_share(hfm_index* x, hfm_index** out) {
   if (!x || !out) return set_error(HFM_E_ARG, "NULL argument");

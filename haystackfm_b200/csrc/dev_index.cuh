@@ -2,22 +2,25 @@
 // primitives every kernel uses.
 //
 // Device layout (built once by hfm_index_load from the reference's bincode records):
-//   occ   : one record per 64 BWT rows holding, per symbol code, the count of that code
-//           from the start of the record's superblock (1,024 records = 65,536 rows) to the
-//           start of the record as a u16, and the rows' 4-bit codes as bitplanes:
-//             wide   (64 B, any text): 16 x u16 counts (codes 0..15), 4 x u64 planes;
-//             narrow (32 B, texts of codes 0..4 only — ExactDna and ACGT-only IUPAC
-//                    texts): 4 x u16 counts (codes 1..4), 3 x u64 planes; the count of
-//                    code 0 is the rows before the border minus the other four.
-//           One rank reads one or two 32-byte sectors.
-//   sb    : 16 x u32 per superblock: count of every code before the superblock (a few MB at
-//           3.1 Gbp; it stays in L2).
+//   occ   : one record per 64 BWT rows, two formats:
+//             wide   (96 B, any text): 16 x u32 counts of every code before the record, then
+//                    4 x u64 planes of the rows' 4-bit codes (three 32-byte sectors);
+//             narrow (32 B, texts of codes 0..4 only — ExactDna and ACGT-only IUPAC texts):
+//                    4 x u16 counts of codes 1..4 from the start of the record's superblock
+//                    (1,024 records = 65,536 rows) to the record, then 3 x u64 planes (one
+//                    sector); the count of code 0 is the rows before the border minus the
+//                    other four.
+//   sb    : (narrow) 16 x u32 per superblock: count of every code before the superblock
+//           (a few MB at 3.1 Gbp; it stays in L2).
 //   ssa   : one 16-byte record per 64 rows: u64 "row is sampled" bits + u32 count of
 //           sampled rows before the word (SampledSuffixArray, src/suffix_array/mod.rs:54-63).
 //   sa_vals, seq_boundaries, lookup intervals: as in the reference.
-// rank(c, i) = sb[(i-1)/65536][c] + rec[(i-1)/64].count[c] + popc(rows of code c <= (i-1)%64),
-// identical to OccTable::rank (src/occ/mod.rs:330-363), whose records instead hold
-// compacted lanes with a u32 superblock count and a u16 delta per lane (src/occ/mod.rs:144).
+// rank(c, i) = count[(i-1)/64][c] (+ sb[(i-1)/65536][c], narrow) + popc(rows of code c <=
+// (i-1)%64), identical to OccTable::rank (src/occ/mod.rs:330-363), whose records instead
+// hold compacted lanes with a u32 superblock count and a u16 delta per lane
+// (src/occ/mod.rs:144).  Wide records keep whole counts: on IUPAC texts an extension emits
+// many intervals, and each would otherwise need one more dependent load for its superblock
+// count (measured: 173 ms against 199 ms for the SMEM search of 1M reads).
 #pragma once
 #include <cstdint>
 
@@ -25,12 +28,12 @@ namespace hfm {
 
 enum : uint32_t { OCC_WIDE = 0, OCC_NARROW = 1 };
 constexpr uint32_t SB_BLOCK_SHIFT = 10;           // records per superblock: 1024 (65,536 rows)
-constexpr uint32_t OCC_WIDE_U4 = 4;               // uint4 per wide record
+constexpr uint32_t OCC_WIDE_U4 = 6;               // uint4 per wide record
 constexpr uint32_t OCC_NARROW_U4 = 2;             // uint4 per narrow record
 
 struct DevFm {
   const uint4* occ;          // OCC_WIDE_U4 or OCC_NARROW_U4 uint4 per record
-  const uint32_t* sb;        // 16 x u32 per superblock
+  const uint32_t* sb;        // 16 x u32 per superblock (narrow records)
   const uint4* ssa;          // 1 x uint4 per block
   const uint32_t* sa_vals;
   const uint2* lut;          // nullptr when the index has no lookup table
@@ -72,13 +75,13 @@ __device__ __forceinline__ uint32_t sel4(uint4 x, uint32_t i) {
 // (border 0: record 0 with no row selected; its counts and superblock entry are 0).
 template <uint32_t FMT>
 struct Border {
-  uint4 a, b, c, d;       // wide: a, b = counts, c, d = planes; narrow: a = counts + p0, b = p1, p2
-  uint64_t low;           // selected rows
-  uint32_t sbi, i;        // superblock, the border itself
+  uint4 a, b, c, d, e, f;  // wide: a..d = counts, e, f = planes; narrow: a = counts + p0, b = p1, p2
+  uint64_t low;            // selected rows
+  uint32_t sbi, i;         // superblock (narrow), the border itself
 
   __device__ __forceinline__ uint64_t plane(int k) const {
-    if (FMT == OCC_WIDE) return k == 0 ? u2to64(c.x, c.y) : k == 1 ? u2to64(c.z, c.w) : k == 2 ? u2to64(d.x, d.y)
-                                                                                                  : u2to64(d.z, d.w);
+    if (FMT == OCC_WIDE) return k == 0 ? u2to64(e.x, e.y) : k == 1 ? u2to64(e.z, e.w) : k == 2 ? u2to64(f.x, f.y)
+                                                                                                  : u2to64(f.z, f.w);
     return k == 0 ? u2to64(a.z, a.w) : k == 1 ? u2to64(b.x, b.y) : k == 2 ? u2to64(b.z, b.w) : 0ull;
   }
   // rows of code s among the selected ones (s a compile-time constant after unrolling)
@@ -88,15 +91,16 @@ struct Border {
     if (FMT == OCC_WIDE) m &= (s & 8) ? plane(3) : ~plane(3);
     return m;
   }
-  // count of code s from the superblock start to the record start (narrow: s in 1..4)
+  // wide: count of code s before the record; narrow (s in 1..4): from the superblock start
   __device__ __forceinline__ uint32_t delta(int s) const {
-    uint32_t w;
-    if (FMT == OCC_WIDE) w = s < 8 ? sel4(a, (uint32_t)s >> 1) : sel4(b, ((uint32_t)s - 8) >> 1);
-    else w = s <= 2 ? a.x : a.y;
-    const int half = FMT == OCC_WIDE ? (s & 1) : ((s - 1) & 1);
-    return half ? (w >> 16) : (w & 0xFFFFu);
+    if (FMT == OCC_WIDE) {
+      const uint4 w = s < 4 ? a : s < 8 ? b : s < 12 ? c : d;
+      return sel4(w, (uint32_t)s & 3);
+    }
+    const uint32_t w = s <= 2 ? a.x : a.y;
+    return ((s - 1) & 1) ? (w >> 16) : (w & 0xFFFFu);
   }
-  // rank within the superblock: count of code s in rows [superblock start, i)
+  // wide: rank of code s at the border; narrow: rank within the superblock
   __device__ __forceinline__ uint32_t local(int s) const { return delta(s) + (uint32_t)__popcll(eq(s)); }
 };
 
@@ -109,10 +113,10 @@ __device__ __forceinline__ Border<FMT> load_border(const DevFm& F, uint32_t i) {
   r.i = i;
   if (FMT == OCC_WIDE) {
     const uint4* p = F.occ + (size_t)blk * OCC_WIDE_U4;
-    r.a = __ldg(p); r.b = __ldg(p + 1); r.c = __ldg(p + 2); r.d = __ldg(p + 3);
+    r.a = __ldg(p); r.b = __ldg(p + 1); r.c = __ldg(p + 2); r.d = __ldg(p + 3); r.e = __ldg(p + 4); r.f = __ldg(p + 5);
   } else {
     const uint4* p = F.occ + (size_t)blk * OCC_NARROW_U4;
-    r.a = __ldg(p); r.b = __ldg(p + 1); r.c = make_uint4(0, 0, 0, 0); r.d = r.c;
+    r.a = __ldg(p); r.b = __ldg(p + 1); r.c = make_uint4(0, 0, 0, 0); r.d = r.c; r.e = r.c; r.f = r.c;
   }
   return r;
 }
@@ -136,16 +140,16 @@ __device__ __forceinline__ uint32_t border_rank(const DevFm& F, const Border<FMT
     const uint64_t sel0 = (s & 1) ? 0ull : ~0ull, sel1 = (s & 2) ? 0ull : ~0ull;
     const uint64_t sel2 = (s & 4) ? 0ull : ~0ull, sel3 = (s & 8) ? 0ull : ~0ull;
     const uint64_t m = B.low & (B.plane(0) ^ sel0) & (B.plane(1) ^ sel1) & (B.plane(2) ^ sel2) & (B.plane(3) ^ sel3);
-    const uint32_t w = sel4(s < 8 ? B.a : B.b, ((uint32_t)s & 7) >> 1);
-    return sb_count(F, B.sbi, s) + ((s & 1) ? (w >> 16) : (w & 0xFFFFu)) + (uint32_t)__popcll(m);
+    const uint4 w = s < 4 ? B.a : s < 8 ? B.b : s < 12 ? B.c : B.d;
+    return sel4(w, (uint32_t)s & 3) + (uint32_t)__popcll(m);
   }
 }
 
 // The interval [lo, hi) of the BWT split by symbol: calls f(s, d, r, sbi) for every code s
-// in ascending order (0..4 narrow, 0..last wide), d = occ(s, hi) - occ(s, lo), and the lo
-// border's rank within its superblock r, so that occ(s, lo) = sb_count(F, sbi, s) + r (one
-// L2-resident load, made only for the codes the caller keeps).  No per-symbol arrays: each
-// code's count is formed and consumed in turn.
+// in ascending order (0..4 narrow, 0..15 wide), d = occ(s, hi) - occ(s, lo), and the lo
+// border's count r: occ(s, lo) = r (wide) or sb_count(F, sbi, s) + r (narrow; one
+// L2-resident load, made only for the codes the caller keeps).  `last` = the highest code
+// the caller needs.
 template <uint32_t FMT, class Fn>
 __device__ __forceinline__ void split_by_symbol(const DevFm& F, uint32_t lo, uint32_t hi, uint32_t last, Fn&& f) {
   if constexpr (FMT == OCC_NARROW) {
@@ -165,28 +169,37 @@ __device__ __forceinline__ void split_by_symbol(const DevFm& F, uint32_t lo, uin
 #pragma unroll
     for (int s = 0; s <= 4; s++) f(s, d[s], r[s], L.sbi);
   } else {
-    // Wide records: the codes in groups of four sharing bits 3 and 2 (a split tree over the
-    // planes, consumed as it is formed: no array of 16 masks or counts), groups past `last`
-    // (the highest code the caller needs) skipped.
+    // Wide records: the 16 masks of each border by a split tree over its planes, then the
+    // counts; groups of codes past `last` are not formed.
     const Border<FMT> L = load_border<FMT>(F, lo), H = load_border<FMT>(F, hi);
-    const bool same_sb = L.sbi == H.sbi;
-    const uint64_t lp0 = L.plane(0), lp1 = L.plane(1), lp2 = L.plane(2), lp3 = L.plane(3);
-    const uint64_t hp0 = H.plane(0), hp1 = H.plane(1), hp2 = H.plane(2), hp3 = H.plane(3);
+    uint32_t rl[16], rh[16];
+    {
+      uint64_t m[16];
+      m[0] = L.low;
 #pragma unroll
-    for (int g = 0; g < 4; g++) {
-      if (4u * g > last) break;
-      const uint64_t gl = L.low & ((g & 2) ? lp3 : ~lp3) & ((g & 1) ? lp2 : ~lp2);
-      const uint64_t gh = H.low & ((g & 2) ? hp3 : ~hp3) & ((g & 1) ? hp2 : ~hp2);
+      for (int p = 3; p >= 0; --p) {
+        const int cnt = 1 << (3 - p);
+        const uint64_t pv = L.plane(p);
 #pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const int s = 4 * g + k;
-        const uint64_t ml = gl & ((k & 2) ? lp1 : ~lp1) & ((k & 1) ? lp0 : ~lp0);
-        const uint64_t mh = gh & ((k & 2) ? hp1 : ~hp1) & ((k & 1) ? hp0 : ~hp0);
-        const uint32_t a = L.delta(s) + (uint32_t)__popcll(ml);
-        uint32_t v = (H.delta(s) + (uint32_t)__popcll(mh)) - a;
-        if (!same_sb) v += sb_count(F, H.sbi, s) - sb_count(F, L.sbi, s);
-        f(s, v, a, L.sbi);
+        for (int k = cnt - 1; k >= 0; --k) { uint64_t v = m[k]; m[2 * k + 1] = v & pv; m[2 * k] = v & ~pv; }
       }
+#pragma unroll
+      for (int t = 0; t < 16; t++) rl[t] = L.delta(t) + (uint32_t)__popcll(m[t]);
+      m[0] = H.low;
+#pragma unroll
+      for (int p = 3; p >= 0; --p) {
+        const int cnt = 1 << (3 - p);
+        const uint64_t pv = H.plane(p);
+#pragma unroll
+        for (int k = cnt - 1; k >= 0; --k) { uint64_t v = m[k]; m[2 * k + 1] = v & pv; m[2 * k] = v & ~pv; }
+      }
+#pragma unroll
+      for (int t = 0; t < 16; t++) rh[t] = H.delta(t) + (uint32_t)__popcll(m[t]);
+    }
+#pragma unroll
+    for (int t = 0; t < 16; t++) {
+      if ((uint32_t)t > last) break;
+      f(t, rh[t] - rl[t], rl[t], 0u);
     }
   }
 }
@@ -207,8 +220,8 @@ __device__ __forceinline__ void row_code_rank(const DevFm& F, uint32_t row, uint
   if (FMT == OCC_WIDE) {
     uint64_t m = B.low & ((c & 1) ? B.plane(0) : ~B.plane(0)) & ((c & 2) ? B.plane(1) : ~B.plane(1)) &
                  ((c & 4) ? B.plane(2) : ~B.plane(2)) & ((c & 8) ? B.plane(3) : ~B.plane(3));
-    uint32_t w = sel4(c < 8 ? B.a : B.b, (c & 7) >> 1);
-    r = sb_count(F, B.sbi, c) + ((c & 1) ? (w >> 16) : (w & 0xFFFFu)) + (uint32_t)__popcll(m);
+    const uint4 w = c < 4 ? B.a : c < 8 ? B.b : c < 12 ? B.c : B.d;
+    r = sel4(w, c & 3) + (uint32_t)__popcll(m);
   } else if (c == 0) {
     r = border_rank<FMT>(F, B, 0);
   } else {
@@ -234,7 +247,7 @@ __device__ __forceinline__ void sym_ranks_t(const DevFm& F, uint32_t i, uint32_t
     for (int s = 5; s < 16; s++) r[s] = 0;
   } else {
 #pragma unroll
-    for (int s = 0; s < 16; s++) r[s] = sb_count(F, B.sbi, s) + B.local(s);
+    for (int s = 0; s < 16; s++) r[s] = B.local(s);
   }
 }
 

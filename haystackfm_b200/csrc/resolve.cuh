@@ -323,6 +323,11 @@ __global__ void k_work_log(const uint64_t* __restrict__ hit_base, const uint64_t
   log[4 * (size_t)i + 2] = np > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)np;
 }
 
+__global__ void k_iota(uint32_t* __restrict__ ids, uint32_t n) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) ids[k] = k;
+}
+
 // seen[] zeroed by the caller; *bad set when ids is not a permutation of 0..n-1.
 __global__ void k_check_perm(const uint32_t* __restrict__ ids, uint32_t n, uint32_t* __restrict__ seen,
                              uint32_t* __restrict__ bad) {

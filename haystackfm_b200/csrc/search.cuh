@@ -19,6 +19,9 @@
 
 namespace hfm {
 
+// Interval-set capacity of the per-thread SMEM kernels (warp-interleaved sets, STRIDE 32).
+constexpr uint32_t FAST_SET_CAP = 768;
+
 // Results are bump-allocated in pools; per-read (offset, count) record where they went.
 struct Pool {
   void* base;
@@ -49,7 +52,8 @@ struct SetRef {
 template <int STRIDE>
 struct SetRef<BIv, STRIDE> {
   uint32_t* p;          // this thread's slot: field f of element i at p[(f * cap + i) * STRIDE]
-  uint32_t plane;       // cap * STRIDE
+  uint32_t plane_;      // cap * STRIDE (warp-interleaved sets: always FAST_SET_CAP * 32)
+  __device__ __forceinline__ uint32_t pl() const { return STRIDE == 32 ? FAST_SET_CAP * 32 : plane_; }
   struct Ref {
     uint32_t* a; uint32_t plane;
     __device__ __forceinline__ operator BIv() const {
@@ -61,15 +65,15 @@ struct SetRef<BIv, STRIDE> {
       return *this;
     }
   };
-  __device__ __forceinline__ Ref operator[](uint32_t i) const { return Ref{p + (size_t)i * STRIDE, plane}; }
+  __device__ __forceinline__ Ref operator[](uint32_t i) const { return Ref{p + (size_t)i * STRIDE, pl()}; }
   __device__ __forceinline__ BIv single(uint32_t i) const {
     const uint32_t* a = p + (size_t)i * STRIDE;
-    uint32_t f = a[0], r = a[plane];
+    uint32_t f = a[0], r = a[pl()];
     return BIv{f, f + 1, r, r + 1};
   }
   __device__ __forceinline__ void set_single(uint32_t i, uint32_t flo, uint32_t rlo) const {
     uint32_t* a = p + (size_t)i * STRIDE;
-    a[0] = flo; a[plane] = rlo;
+    a[0] = flo; a[pl()] = rlo;
   }
 };
 
@@ -98,6 +102,22 @@ __device__ __forceinline__ SetRef<T, STRIDE> thread_set(T* work, uint32_t cap, i
 __device__ __forceinline__ bool next_read(unsigned int* ctr, uint32_t n, const uint32_t* ids, uint32_t& i) {
   uint32_t k = atomicAdd(ctr, 1u);
   if (k >= n) return false;
+  i = ids ? ids[k] : k;
+  return true;
+}
+
+// The same queue taken `chunk` consecutive entries per atomic: the thread works through its
+// chunk before it takes the next one (a tunable; 1 = one entry per atomic).
+struct QueueCursor { uint32_t next = 0, end = 0; };
+__device__ __forceinline__ bool next_read_chunked(unsigned int* ctr, uint32_t n, const uint32_t* ids, uint32_t chunk,
+                                                  QueueCursor& c, uint32_t& i) {
+  if (c.next >= c.end) {
+    const uint32_t k = atomicAdd(ctr, chunk);
+    if (k >= n) return false;
+    c.next = k;
+    c.end = min(n, k + chunk);
+  }
+  const uint32_t k = c.next++;
   i = ids ? ids[k] : k;
   return true;
 }
@@ -322,7 +342,7 @@ __device__ __forceinline__ void extend_set(const DevFm& X, const SmemFm& S, uint
     split_by_symbol<FMT>(X, a, b, top, [&](int s, uint32_t d, uint32_t r, uint32_t sbi) {
       if (!ovf && ((mask >> s) & 1) && d) {
         if (out.n1 + out.nb >= cap) { ovf = true; return; }
-        const uint32_t lo = S.C[s] + sb_count(X, sbi, s) + r;
+        const uint32_t lo = S.C[s] + (FMT == OCC_WIDE ? r : sb_count(X, sbi, s) + r);
         if (d == 1) {
           if (DIR == 0) out.s.set_single(out.n1++, base + run, lo);
           else out.s.set_single(out.n1++, lo, base + run);
@@ -608,7 +628,9 @@ struct MemsWork {
   uint32_t* work_log;                 // COUNT_TOUCH only: 4 u32 per read, [0] += Occ touches, [3] |= 1 on overflow
                                       // (the warp-per-read kernel also sets bit 1)
   const uint32_t* n_dev;              // when set, the number of reads is read here (graph-captured chains)
+  uint32_t chunk;                     // queue entries taken per atomic (0 or 1: one)
   __device__ __forceinline__ uint32_t count() const { return n_dev ? *n_dev : n; }
+  __device__ __forceinline__ uint32_t step() const { return chunk > 1 ? chunk : 1u; }
 };
 
 // Splits the fast pass's overflow list: the first `first_warp` entries (reads a schedule
@@ -634,9 +656,10 @@ __global__ void __launch_bounds__(128, MINB) k_mems(DevFm Fw, DevFm Rv, const ui
   smem_fm_init(Sf, Fw, compat_fw);
   smem_fm_init(Sr, Rv, compat_rv);
   __syncthreads();
+  const uint32_t SCAP = STRIDE == 32 ? FAST_SET_CAP : W.set_cap;
   using SR = SetRef<BIv, STRIDE>;
-  SR s0 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 0), s1 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 1);
-  SR s2 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 2), s3 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 3);
+  SR s0 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 0), s1 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 1);
+  SR s2 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 2), s3 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 3);
   Cand local_c[KC > 0 ? KC : 1];
   Cand* cands = local_c;
   uint32_t cand_cap = KC;
@@ -647,13 +670,14 @@ __global__ void __launch_bounds__(128, MINB) k_mems(DevFm Fw, DevFm Rv, const ui
   }
   uint64_t touches = 0;
   uint32_t i;
-  const uint32_t nreads = W.count();
-  while (next_read(W.queue, nreads, W.ids, i)) {
+  const uint32_t nreads = W.count(), chunk = W.step();
+  QueueCursor qc;
+  while (next_read_chunked(W.queue, nreads, W.ids, chunk, qc, i)) {
     uint32_t st = ST_OK;
     uint64_t o = qoff[i];
     uint64_t t0 = touches;
     uint32_t nc = mems_one<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, (uint32_t)(qoff[i + 1] - o), P, s0, s1, s2, s3,
-                                        W.set_cap, cands, cand_cap, ivpool, st, touches);
+                                        SCAP, cands, cand_cap, ivpool, st, touches);
     uint64_t hs = 0; uint32_t hc = 0;
     if (nc != ~0u) {
       if (P.mode == 0) nc = finalize_smems(cands, nc);
@@ -864,16 +888,19 @@ __global__ void __launch_bounds__(128, MINB) k_mems_seg(DevFm Fw, DevFm Rv, cons
   smem_fm_init(Sf, Fw, compat_fw);
   smem_fm_init(Sr, Rv, compat_rv);
   __syncthreads();
+  const uint32_t SCAP = STRIDE == 32 ? FAST_SET_CAP : W.set_cap;
   using SR = SetRef<BIv, STRIDE>;
-  SR s0 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 0), s1 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 1);
-  SR s2 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 2), s3 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 3);
+  SR s0 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 0), s1 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 1);
+  SR s2 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 2), s3 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 3);
   uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   Cand* cands = W.cands + tid * W.cand_cap;
   uint64_t touches = 0;
   const uint32_t n_units = G.units();
   const uint32_t njobs = n_units + G.shorts();
   uint32_t u;
-  while (next_read(W.queue, njobs, nullptr, u)) {
+  const uint32_t chunk = W.step();
+  QueueCursor qc;
+  while (next_read_chunked(W.queue, njobs, nullptr, chunk, qc, u)) {
     const bool unit = u < n_units;
     uint32_t i, s, e;
     uint32_t* bits = nullptr;
@@ -892,11 +919,11 @@ __global__ void __launch_bounds__(128, MINB) k_mems_seg(DevFm Fw, DevFm Rv, cons
     }
     uint32_t st = ST_OK;
     uint64_t t0 = touches;
-    CandSink<SR> sink{cands, 0, W.cand_cap, &ivpool, &st, W.set_cap};
+    CandSink<SR> sink{cands, 0, W.cand_cap, &ivpool, &st, SCAP};
     uint32_t p = s;
     while (p < e) {
       if (unit) { uint32_t d = p - s; bits[d >> 5] |= 1u << (d & 31); }
-      p = smem_pivot<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
+      p = smem_pivot<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, SCAP, st, touches, sink);
       if (p == ~0u) break;
     }
     uint32_t nc = sink.nc;
@@ -946,9 +973,10 @@ __global__ void __launch_bounds__(128, MINB) k_mems_fix(DevFm Fw, DevFm Rv, cons
   smem_fm_init(Sf, Fw, compat_fw);
   smem_fm_init(Sr, Rv, compat_rv);
   __syncthreads();
+  const uint32_t SCAP = STRIDE == 32 ? FAST_SET_CAP : W.set_cap;
   using SR = SetRef<BIv, STRIDE>;
-  SR s0 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 0), s1 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 1);
-  SR s2 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 2), s3 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 3);
+  SR s0 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 0), s1 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 1);
+  SR s2 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 2), s3 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 3);
   uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   Cand* cands = W.cands + tid * W.cand_cap;
   uint64_t touches = 0;
@@ -966,10 +994,10 @@ __global__ void __launch_bounds__(128, MINB) k_mems_fix(DevFm Fw, DevFm Rv, cons
     const uint32_t* bits = G.bits + (size_t)u * G.seg_words;
     uint32_t st = ST_OK;
     uint64_t t0 = touches;
-    CandSink<SR> sink{cands, 0, W.cand_cap, &ivpool, &st, W.set_cap};
+    CandSink<SR> sink{cands, 0, W.cand_cap, &ivpool, &st, SCAP};
     uint32_t p = entry;
     while (p < e && !((bits[(p - s) >> 5] >> ((p - s) & 31)) & 1u)) {
-      p = smem_pivot<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
+      p = smem_pivot<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, SCAP, st, touches, sink);
       if (p == ~0u) break;
     }
     if (COUNT_TOUCH && W.work_log) atomicAdd(W.work_log + 4 * (size_t)i, (uint32_t)(touches - t0));
@@ -999,9 +1027,10 @@ __global__ void __launch_bounds__(128, MINB) k_mems_merge(DevFm Fw, DevFm Rv, co
   smem_fm_init(Sf, Fw, compat_fw);
   smem_fm_init(Sr, Rv, compat_rv);
   __syncthreads();
+  const uint32_t SCAP = STRIDE == 32 ? FAST_SET_CAP : W.set_cap;
   using SR = SetRef<BIv, STRIDE>;
-  SR s0 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 0), s1 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 1);
-  SR s2 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 2), s3 = thread_set<BIv, STRIDE>(W.sets, W.set_cap, 4, 3);
+  SR s0 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 0), s1 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 1);
+  SR s2 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 2), s3 = thread_set<BIv, STRIDE>(W.sets, SCAP, 4, 3);
   uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   Cand* cands = W.cands + tid * W.cand_cap;
   uint64_t touches = 0;
@@ -1014,7 +1043,7 @@ __global__ void __launch_bounds__(128, MINB) k_mems_merge(DevFm Fw, DevFm Rv, co
     uint64_t u0 = G.unit_base[r], u1 = G.unit_base[r + 1];
     uint32_t st = ST_OK;
     uint64_t t0 = touches;
-    CandSink<SR> sink{cands, 0, W.cand_cap, &ivpool, &st, W.set_cap};
+    CandSink<SR> sink{cands, 0, W.cand_cap, &ivpool, &st, SCAP};
     bool fail = false;
     uint32_t t = 0;                                   // the true chain's next pivot
     for (uint64_t u = u0; u < u1 && !fail; u++) {
@@ -1048,7 +1077,7 @@ __global__ void __launch_bounds__(128, MINB) k_mems_merge(DevFm Fw, DevFm Rv, co
       uint32_t p = t;
       const uint32_t* bits = G.bits + u * G.seg_words;
       while (p < e && !((bits[(p - s) >> 5] >> ((p - s) & 31)) & 1u)) {
-        p = smem_pivot<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, W.set_cap, st, touches, sink);
+        p = smem_pivot<COUNT_TOUCH, FMT>(Fw, Rv, Sf, Sr, q + o, n, p, P, s0, s1, s2, s3, SCAP, st, touches, sink);
         if (p == ~0u) { fail = true; break; }
       }
       if (fail) break;

@@ -234,23 +234,27 @@ class _Handle:
     def tuning(self) -> dict:
         t = L.HfmTuning()
         L.check(L.lib().hfm_get_tuning(self.h, C.byref(t)))
-        return {"mems_variant": t.mems_variant, "seg_len": t.seg_len}
+        return {"mems_variant": t.mems_variant, "seg_len": t.seg_len, "queue_chunk": t.queue_chunk,
+                "threads_per_read": t.threads_per_read}
 
-    def set_tuning(self, mems_variant: int, seg_len: int):
-        t = L.HfmTuning(mems_variant, seg_len)
+    def set_tuning(self, mems_variant: int, seg_len: int, queue_chunk: int = None, threads_per_read: int = None):
+        cur = self.tuning()
+        t = L.HfmTuning(mems_variant, seg_len, cur["queue_chunk"] if queue_chunk is None else queue_chunk,
+                        cur["threads_per_read"] if threads_per_read is None else threads_per_read)
         L.check(L.lib().hfm_set_tuning(self.h, C.byref(t)))
 
     def autotune_mems(self, q_d, off_d, nq: int, min_len: int, mode: int, ref_bounds, max_hits: int, reps: int = 2):
         """hfm_autotune_mems on a device batch (torch tensors) -> {chosen setting, candidates' ms}."""
         rb = np.ascontiguousarray(ref_bounds if ref_bounds is not None else [], dtype=np.uint32)
         best = L.HfmTuning()
-        times = np.zeros(4, dtype=np.float32)
+        times = np.zeros(len(L.TUNE_CANDIDATES), dtype=np.float32)
         L.check(L.lib().hfm_autotune_mems(self.h, q_d.data_ptr(), off_d.data_ptr(), nq, min_len, mode,
                                           L.ptr(rb, L.u32p) if len(rb) else None, len(rb), max_hits, reps,
                                           C.byref(best), times.ctypes.data_as(C.POINTER(C.c_float))))
-        cands = [(3, 512), (3, 256), (3, 1024), (2, 512)]
-        return {"mems_variant": best.mems_variant, "seg_len": best.seg_len,
-                "candidates_ms": {f"v{v}/seg{sl}": round(float(t), 3) for (v, sl), t in zip(cands, times)}}
+        return {"mems_variant": best.mems_variant, "seg_len": best.seg_len, "queue_chunk": best.queue_chunk,
+                "threads_per_read": best.threads_per_read,
+                "candidates_ms": {f"v{v}/seg{sl}/chunk{ch}/tpr{tp}": round(float(t), 3)
+                                  for (v, sl, ch, tp), t in zip(L.TUNE_CANDIDATES, times)}}
 
 
 class _DeviceArray:

@@ -246,6 +246,16 @@ int hfm_mems_graph_create(hfm_index* idx, const uint8_t* d_q, const uint64_t* d_
                           uint32_t max_hits, uint64_t max_positions, hfm_graph** out);
 int hfm_mems_graph_launch(hfm_graph* g, hfm_dev_mems* out, uint32_t* replayed);
 void hfm_mems_graph_free(hfm_graph* g);
+/* Replays and fallbacks so far, and the reasons of the last launch's fallback (0: it was
+ * replayed): HFM_GRAPH_* bits.  A warp-tier set overflow also quadruples that tier's set
+ * capacity for the next capture. */
+#define HFM_GRAPH_BASES 1u        /* the batch has more codes than the segment capacity   */
+#define HFM_GRAPH_INTERVALS 2u    /* candidate-interval pool                              */
+#define HFM_GRAPH_HITS 4u         /* MemHit pool                                          */
+#define HFM_GRAPH_SEGMENTS 8u     /* long-read segment candidate pool                     */
+#define HFM_GRAPH_WARP_SETS 16u   /* a read's interval set outgrew the warp tier          */
+#define HFM_GRAPH_POSITIONS 32u   /* positions (or distinct positions) past the capacity  */
+int hfm_mems_graph_info(const hfm_graph* g, uint32_t* replays, uint32_t* fallbacks, uint32_t* last_reason);
 
 /* Pre-sizes a handle's SMEM/MEM work pools and result arrays for a batch of nq reads
  * expected to produce `intervals` candidate intervals, `hits` MemHits and `positions`
@@ -319,20 +329,32 @@ int hfm_set_counters(hfm_index* idx, int enable);  /* per-read work counters on/
 int hfm_set_timeout(hfm_index* idx, uint32_t ms);
 
 /* Tunable parameters of the SMEM/MEM search and their autotuner (no counterpart in the
- * reference).  mems_variant: persistent fast pass with 32-entry candidate lists in local
- * memory (2) or 1024-entry lists in global memory (3, default), 8 resident blocks per SM;
- * 4: the plain launch — one thread per read over a grid the size of the batch, sets and
- * candidates in local memory, a count pass whose totals are read back to size the outputs
- * before the write pass (the reference GPU search's structure, shaders/mem_find.wgsl,
- * src/gpu/mem_find.rs:213-244), kept as the baseline.  seg_len: SMEM reads longer than 2*seg_len are swept in seg_len-position
- * segments (multiple of 32 in 64..4096, default 512).  Results never depend on them.
- * hfm_autotune_mems times the search of a sample batch under each candidate setting
- * (variant 3 with seg_len 512, 256, 1024; variant 2), best of `reps` runs after a warm-up
+ * reference, whose shaders run a fixed workgroup_size(64), shaders/mem_find.wgsl:364-372).
+ * Results never depend on them.
+ *   mems_variant      persistent fast pass with 32-entry candidate lists in local memory (2)
+ *                     or 1024-entry lists in global memory (3, default), 8 resident blocks
+ *                     per SM; 4: the plain launch — one thread per read over a grid the size
+ *                     of the batch, sets and candidates in local memory, a count pass whose
+ *                     totals are read back to size the outputs before the write pass (the
+ *                     reference GPU search's structure, src/gpu/mem_find.rs:213-244), kept
+ *                     as the baseline.
+ *   seg_len           SMEM reads longer than 2*seg_len are swept in seg_len-position segments
+ *                     (multiple of 32 in 64..4096, default 512).
+ *   queue_chunk       reads a per-thread kernel takes from its device work queue per atomic
+ *                     (1..64, default 1).
+ *   threads_per_read  1 (default): a thread per read; 32: every read on the warp-per-read
+ *                     kernel (the 32 lanes share each interval set).
+ * hfm_autotune_mems times the search of a sample batch under each of the HFM_TUNE_CANDIDATES
+ * settings {variant, seg_len, chunk, threads}: {3,512,1,1}, {3,256,1,1}, {3,1024,1,1},
+ * {2,512,1,1}, {3,512,4,1}, {3,512,16,1}, {3,512,1,32} — best of `reps` runs after a warm-up
  * run, by CUDA events on the handle's stream; it keeps the fastest on the handle, writes it
- * to *best, and the candidates' times to times_ms[4] when non-NULL. */
+ * to *best, and the candidates' times to times_ms[HFM_TUNE_CANDIDATES] when non-NULL. */
+#define HFM_TUNE_CANDIDATES 7
 typedef struct hfm_tuning {
   uint32_t mems_variant;
   uint32_t seg_len;
+  uint32_t queue_chunk;
+  uint32_t threads_per_read;
 } hfm_tuning;
 int hfm_get_tuning(const hfm_index* idx, hfm_tuning* out);
 int hfm_set_tuning(hfm_index* idx, const hfm_tuning* t);

@@ -106,7 +106,7 @@ def test_null_arguments_rejected_without_a_gpu():
     E_ARG = -4
     dm = L.HfmDevMems()
     sc = L.HfmSched(None, 0, 0, None)
-    t = L.HfmTuning(3, 512)
+    t = L.HfmTuning(3, 512, 1, 1)
     assert lib.hfm_mems_batch_device_sched(None, None, None, 0, 19, 0, None, 0, 64, C.byref(sc), C.byref(dm)) == E_ARG
     assert lib.hfm_get_tuning(None, C.byref(t)) == E_ARG
     assert lib.hfm_set_tuning(None, C.byref(t)) == E_ARG

@@ -91,7 +91,11 @@ def test_graph_replays_and_falls_back(oracle, kind):
             assert rep.value in (0, 1)
         dm = L.HfmDevMems()
         L.check(lib.hfm_mems_graph_launch(g, C.byref(dm), C.byref(rep)))
-        assert rep.value == 1                       # captured capacities hold: the replay's outputs
+        n_rep, n_fb, why = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        L.check(lib.hfm_mems_graph_info(g, C.byref(n_rep), C.byref(n_fb), C.byref(why)))
+        # captured capacities hold (re-captured after any fallback): the replay's outputs
+        assert rep.value == 1 and why.value == 0, (n_rep.value, n_fb.value, why.value)
+        _same(_host(dm, nq, 0), want)
     finally:
         lib.hfm_mems_graph_free(g)
     # a capacity too small for the batch: rerun on the adaptive chain, then captured again

@@ -5,6 +5,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
+from haystackfm_b200 import _lib as L
 from haystackfm_b200 import alphabet as al
 from haystackfm_b200 import synth
 from haystackfm_b200.errors import FmIndexError
@@ -122,16 +123,19 @@ def test_autotune_keeps_results(oracle):
     q = torch.from_numpy(flat).cuda()
     o = torch.from_numpy(off.view(np.int64)).cuda()
     res = h.autotune_mems(q, o, len(off) - 1, 19, 0, bounds, 128, reps=1)
-    assert (res["mems_variant"], res["seg_len"]) in [(3, 512), (3, 256), (3, 1024), (2, 512)]
-    assert h.tuning() == {"mems_variant": res["mems_variant"], "seg_len": res["seg_len"]}
-    assert len(res["candidates_ms"]) == 4 and all(v > 0 for v in res["candidates_ms"].values())
-    for v, sl in [(3, 64), (3, 4096), (2, 512), (4, 512)]:
-        h.set_tuning(v, sl)
+    chosen = (res["mems_variant"], res["seg_len"], res["queue_chunk"], res["threads_per_read"])
+    assert chosen in L.TUNE_CANDIDATES
+    assert h.tuning() == {"mems_variant": chosen[0], "seg_len": chosen[1], "queue_chunk": chosen[2],
+                          "threads_per_read": chosen[3]}
+    assert len(res["candidates_ms"]) == len(L.TUNE_CANDIDATES) and all(v > 0 for v in res["candidates_ms"].values())
+    for v, sl, ch, tp in [(3, 64, 1, 1), (3, 4096, 1, 1), (2, 512, 1, 1), (4, 512, 1, 1), (3, 512, 7, 1),
+                          (3, 256, 64, 1), (3, 512, 1, 32), (2, 512, 3, 32)]:
+        h.set_tuning(v, sl, ch, tp)
+        _same(h.mems_packed(flat, off, 19, 0, bounds, 128), want)
         _same(h.mems_sched_packed(flat, off, 19, 0, bounds, 128), want)
-    with pytest.raises(FmIndexError):
-        h.set_tuning(4, 512)
-    with pytest.raises(FmIndexError):
-        h.set_tuning(3, 100)
+    for bad in [(5, 512, 1, 1), (3, 100, 1, 1), (3, 512, 0, 1), (3, 512, 65, 1), (3, 512, 1, 8)]:
+        with pytest.raises(FmIndexError):
+            h.set_tuning(*bad)
 
 
 def test_plain_launch_bit_exact(mixed_case, oracle):
