@@ -1414,6 +1414,30 @@ int hfm_autotune_mems(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, 
   return HFM_OK;
 }
 
+int hfm_mems_reserve(hfm_index* x, uint32_t nq, uint64_t intervals, uint64_t hits, uint64_t positions) {
+  if (!x) return set_error(HFM_E_ARG, "NULL argument");
+  Guard g(x);
+  // the search pools (intervals of every candidate, MemHits) and the result arrays
+  x->miv_cap = std::max<uint64_t>(x->miv_cap, intervals + 4096);
+  x->hit_cap = std::max<uint64_t>(x->hit_cap, hits + 4096);
+  RET(x->mivpool.ensure(x->miv_cap * 16)); x->miv_cap = x->mivpool.cap / 16;
+  RET(x->hitpool.ensure(x->hit_cap * 32)); x->hit_cap = x->hitpool.cap / 32;
+  RET(x->hits.ensure(hits * 32 + 32));
+  RET(x->npos_scan.ensure((hits + 1) * 8));
+  RET(x->out_pairs.ensure(positions * 8 + 8));
+  RET(x->hit_start.ensure((size_t)nq * 8 + 8)); RET(x->hit_count.ensure((size_t)nq * 4 + 4));
+  RET(x->hit_base.ensure(((size_t)nq + 1) * 8));
+  RET(x->status.ensure((size_t)nq * 4 + 4)); RET(x->ovf.ensure((size_t)nq * 4 + 4));
+  return HFM_OK;
+}
+
+int hfm_set_timeout(hfm_index* x, uint32_t ms) {
+  if (!x) return set_error(HFM_E_ARG, "NULL argument");
+  std::lock_guard<std::mutex> lk(x->mu);
+  x->timeout_ms = ms;
+  return HFM_OK;
+}
+
 int hfm_set_counters(hfm_index* x, int enable) {
   if (!x) return set_error(HFM_E_ARG, "NULL argument");
   x->count_work = enable != 0;
