@@ -78,6 +78,12 @@ def _header_fields(data: bytes, base: int = 0):
     return text_len, nseq, bounds, headers
 
 
+def _take_bytes(ptr, n: int) -> bytes:
+    """Copy n bytes from a library-allocated block (ctypes.string_at takes a C int size,
+    too small for genome-scale indices)."""
+    return np.ctypeslib.as_array(ptr, shape=(n,)).tobytes() if n else b""
+
+
 def _build(sequences: Sequence[DnaSequence], config: FmIndexConfig, tag: int, kind: int) -> bytes:
     if not sequences:
         raise FmIndexError.empty_sequence()
@@ -91,7 +97,7 @@ def _build(sequences: Sequence[DnaSequence], config: FmIndexConfig, tag: int, ki
     n = C.c_size_t()
     L.check(L.lib().hfm_build_index(L.ptr(flat, L.u8p), L.ptr(off, L.u64p), len(sequences), hdr, C.byref(opts),
                                     kind, C.byref(out), C.byref(n)))
-    data = C.string_at(out, n.value)
+    data = _take_bytes(out, n.value)
     L.lib().hfm_free(out)
     return data
 
@@ -109,7 +115,7 @@ def _build_gpu(sequences: Sequence[DnaSequence], config: FmIndexConfig, tag: int
     L.check(L.lib().hfm_build_index_gpu(L.ptr(flat, L.u8p), L.ptr(off, L.u64p), len(sequences), hdr, C.byref(opts),
                                         kind, device, C.byref(out), C.byref(n)))
     try:
-        data = C.string_at(out, n.value)
+        data = _take_bytes(out, n.value)
     finally:
         L.lib().hfm_free(out)
     return data
