@@ -143,6 +143,9 @@ SIGNATURES = {
     "hfm_mems_graph_free": (None, [C.c_void_p]),
     "hfm_mems_graph_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                       C.POINTER(C.c_uint32)]),
+    "hfm_mems_graph_add_locate": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64,
+                                            C.c_uint64]),
+    "hfm_mems_graph_locate_result": (C.c_int, [C.c_void_p, C.POINTER(HfmDevHits)]),
     "hfm_mems_reserve": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint64, C.c_uint64]),
     "hfm_probe_gather": (C.c_int, [C.c_int, C.c_uint64, C.c_uint32, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
 }

@@ -122,7 +122,7 @@ struct hfm_index {
       scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr,
       mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout, blockmap, blockmap2, ovf2, ovf3,
       lflag, lpos, sids, lids, ucount, ubase, uread, uk, ubits, uexit, ust, ucoff, ucnt, segpool, fxe, fxc, fxx,
-      fxo, fxn, npos;
+      fxo, fxn, npos, loc_pairs;
   uint32_t flags = 0;
   uint32_t seg_len = 512;  // SMEM reads longer than 2 * seg_len take the segmented sweep
   uint32_t queue_chunk = 1;       // reads a per-thread kernel takes from its queue per atomic
@@ -1000,7 +1000,7 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
   }
   // warp tier: up to 16 warps per SM, at most 2 GB of sets
   const uint64_t per_warp = (uint64_t)c.warp_cap * 4 * 16;
-  const uint64_t wwarps = std::max<uint64_t>(4, std::min<uint64_t>((uint64_t)x->num_sms * 16, (2ull << 30) / per_warp));
+  const uint64_t wwarps = std::max<uint64_t>(4, std::min<uint64_t>((uint64_t)x->num_sms * 8, (2ull << 30) / per_warp));
   const uint32_t wgrid = (uint32_t)((wwarps + 3) / 4);
   RET(x->work.ensure((size_t)wgrid * 4 * per_warp));
   RET(x->cwork.ensure(std::max<size_t>((size_t)threads * FAST_CAND_CAP, (size_t)wgrid * 4 * c.warp_cands) * sizeof(Cand)));
@@ -1169,6 +1169,146 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
   return HFM_OK;
 }
 
+// The locate chain (backward search, CSR of merged intervals, resolve) with fixed
+// capacities, the same way: `iv_cap` merged intervals over the batch, `pos_cap` positions,
+// its own counters block and result array so that it can precede the SMEM chain in one
+// captured graph.
+struct FixedLocate {
+  const uint8_t* d_q; const uint64_t* d_qoff; uint32_t nq; uint32_t max_hits;
+  uint64_t iv_cap, pos_cap;
+  uint32_t warp_cap = BS_WARP_SET_CAP;
+  bool dedup;
+  uint64_t threads;
+  Counters* ctr;                // device counters of this chain
+  GraphTotals* d_tot; GraphTotals* h_tot;
+  Counters* h_ctr;              // pinned copy of ctr after the chain
+};
+
+static int fixed_locate(hfm_index* x, FixedLocate& c, bool launch) {
+  const FmDev& F = x->fwd;
+  const uint32_t nq = c.nq;
+  uint32_t dummy = 0;
+  auto SCAN = [&](auto* in, uint32_t stride, uint64_t n, uint64_t* out) -> int {
+    if (!launch) {
+      uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+      return x->scan_tmp.ensure((tiles + 1) * 8);
+    }
+    return scan(x, in, stride, n, out, dummy);
+  };
+  const uint64_t icap = c.iv_cap, pcap = c.pos_cap;
+  if (icap >= 0xFFFFFFFFull) return set_error(HFM_E_ARG, "interval capacity above 2^32");
+  RET(x->counts.ensure((size_t)nq * 4 + 4)); RET(x->nhits.ensure((size_t)nq * 8 + 8));
+  RET(x->niv.ensure((size_t)nq * 4 + 4)); RET(x->ivoff.ensure((size_t)nq * 8 + 8));
+  RET(x->status.ensure((size_t)nq * 4 + 4)); RET(x->ovf.ensure((size_t)nq * 4 + 4));
+  RET(x->ivpool.ensure(icap * 8));
+  if (!launch) {
+    int bpsm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpsm, k_bsearch<false, 32>, 256, 0));
+    c.threads = std::min<uint64_t>((uint64_t)std::max(1, bpsm) * x->num_sms * 256, ((uint64_t)nq + 255) / 256 * 256);
+  }
+  RET(x->bswork.ensure(std::max<uint64_t>(c.threads, 32) * 2 * BS_SET_CAP * 8));
+  const uint64_t per_warp = (uint64_t)c.warp_cap * 2 * 8;
+  const uint64_t wwarps = std::max<uint64_t>(4, std::min<uint64_t>((uint64_t)x->num_sms * 8, (2ull << 30) / per_warp));
+  const uint32_t wgrid = (uint32_t)((wwarps + 3) / 4);
+  RET(x->work.ensure((size_t)wgrid * 4 * per_warp));
+  RET(x->seg_base.ensure(((size_t)nq + 1) * 8)); RET(x->pos_base.ensure(((size_t)nq + 1) * 8));
+  RET(x->seg_row.ensure(icap * 4 + 4)); RET(x->seg_off.ensure((icap + 1) * 8));
+  RET(x->loc_pairs.ensure(pcap * 8 + 8));
+  const uint64_t rblocks = (pcap + RES_T - 1) / RES_T, eblocks = (pcap + EXP_BLK - 1) / EXP_BLK;
+  RET(x->blockmap.ensure(rblocks * 4 + 4));
+  uint64_t hsize = 1024;
+  while (hsize < 2 * icap) hsize <<= 1;
+  if (c.dedup) {
+    RET(x->hkeys.ensure(hsize * 8)); RET(x->hslot.ensure(icap * 4 + 4));
+    RET(x->hflags.ensure(hsize * 4)); RET(x->huid.ensure((hsize + 1) * 8));
+    RET(x->urow.ensure(icap * 4 + 4)); RET(x->ulen.ensure(icap * 4 + 4)); RET(x->uoff.ensure((icap + 1) * 8));
+    RET(x->uout.ensure(pcap * 8 + 8));
+    RET(x->blockmap2.ensure(eblocks * 4 + 4));
+  }
+  Counters* dc = c.ctr;
+  Pool pool{x->ivpool.p, &dc->iv_used, icap};
+  BsOut o{x->counts.as<uint32_t>(), x->nhits.as<uint64_t>(), x->niv.as<uint32_t>(), x->ivoff.as<uint64_t>(),
+          x->status.as<uint32_t>(), x->ovf.as<uint32_t>(), &dc->n_ovf, &dc->touches};
+  const uint16_t* cm = F.compat.as<uint16_t>();
+  if (launch) {
+    CK(cudaMemsetAsync(dc, 0, sizeof(Counters), x->stream));
+    k_bsearch<false, 32><<<(unsigned)(c.threads / 256), 256, 0, x->stream>>>(F.d, cm, c.d_q, c.d_qoff, nullptr, nq,
+                                                                            c.max_hits, x->bswork.as<uint2>(), BS_SET_CAP,
+                                                                            &dc->queue, pool, o, &dc->still_ovf);
+    k_bsearch_warp<false><<<wgrid, 128, 0, x->stream>>>(F.d, cm, c.d_q, c.d_qoff, x->ovf.as<uint32_t>(), 0u, c.max_hits,
+                                                       x->work.as<uint2>(), c.warp_cap, &dc->queue2, pool, o,
+                                                       &dc->still_ovf, &dc->n_ovf);
+    k_zero_failed<<<(nq + 255) / 256, 256, 0, x->stream>>>(x->status.as<uint32_t>(), nq, x->niv.as<uint32_t>(),
+                                                           x->nhits.as<uint64_t>());
+    CK(cudaGetLastError());
+  }
+  RET(SCAN(x->niv.as<uint32_t>(), 1, nq, x->seg_base.as<uint64_t>()));      // seg_base[nq] = intervals
+  RET(SCAN(x->nhits.as<uint64_t>(), 1, nq, x->pos_base.as<uint64_t>()));    // pos_base[nq] = positions
+  const uint64_t* seg_off = x->seg_off.as<uint64_t>();
+  const uint32_t* seg_row = x->seg_row.as<uint32_t>();
+  const uint32_t guard = F.rate ? F.rate : F.text_len;
+  const uint32_t nb = (uint32_t)F.seq_boundaries.size();
+  const uint32_t* d_bounds = F.bounds.as<uint32_t>();
+  if (launch) {
+    k_gather_locate<<<(nq + 255) / 256, 256, 0, x->stream>>>(x->ivpool.as<uint2>(), x->ivoff.as<uint64_t>(),
+                                                            x->niv.as<uint32_t>(), x->seg_base.as<uint64_t>(),
+                                                            x->pos_base.as<uint64_t>(), nq, c.max_hits,
+                                                            x->seg_row.as<uint32_t>(), x->seg_off.as<uint64_t>());
+    k_seal_segments<<<(unsigned)std::min<uint64_t>((icap + 256) / 256, 65535), 256, 0, x->stream>>>(
+        x->seg_off.as<uint64_t>(), x->seg_base.as<uint64_t>() + nq, x->pos_base.as<uint64_t>() + nq, icap);
+    CK(cudaGetLastError());
+  }
+  if (c.dedup) {
+    if (launch) {
+      CK(cudaMemsetAsync(x->hkeys.p, 0xFF, hsize * 8, x->stream));
+      k_dedup_insert<<<(unsigned)((icap + 255) / 256), 256, 0, x->stream>>>(seg_row, 1, seg_off, (uint32_t)icap,
+                                                                           x->hkeys.as<unsigned long long>(), hsize - 1,
+                                                                           x->hslot.as<uint32_t>());
+      k_dedup_flags<<<(unsigned)((hsize + 255) / 256), 256, 0, x->stream>>>(x->hkeys.as<unsigned long long>(), hsize,
+                                                                           x->hflags.as<uint32_t>());
+      CK(cudaGetLastError());
+    }
+    RET(SCAN(x->hflags.as<uint32_t>(), 1, hsize, x->huid.as<uint64_t>()));
+    if (launch) {
+      CK(cudaMemsetAsync(x->ulen.p, 0, icap * 4 + 4, x->stream));
+      k_dedup_compact<<<(unsigned)((hsize + 255) / 256), 256, 0, x->stream>>>(x->hkeys.as<unsigned long long>(), hsize,
+                                                                             x->huid.as<uint64_t>(), x->urow.as<uint32_t>(),
+                                                                             x->ulen.as<uint32_t>());
+      CK(cudaGetLastError());
+    }
+    RET(SCAN(x->ulen.as<uint32_t>(), 1, icap, x->uoff.as<uint64_t>()));
+    if (launch) {
+      k_graph_totals<<<1, 32, 0, x->stream>>>(x->seg_base.as<uint64_t>(), nq, x->pos_base.as<uint64_t>() + nq,
+                                              x->uoff.as<uint64_t>() + icap, pcap, c.d_tot);
+      k_block_first<<<(unsigned)((icap + 255) / 256), 256, 0, x->stream>>>(x->uoff.as<uint64_t>(), (uint32_t)icap, RES_T,
+                                                                          x->blockmap.as<uint32_t>(), rblocks);
+      ResolveArgs A{x->urow.as<uint32_t>(), 1, x->uoff.as<uint64_t>(), (uint32_t)icap, pcap, d_bounds, nb, guard,
+                    x->uout.as<uint32_t>(), &dc->walk_err, &dc->steps, x->blockmap.as<uint32_t>(), &c.d_tot->upos};
+      k_resolve<false><<<(unsigned)((pcap + RES_T - 1) / RES_T), RES_T, 0, x->stream>>>(F.d, A);
+      k_block_first<<<(unsigned)((icap + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)icap, EXP_BLK,
+                                                                          x->blockmap2.as<uint32_t>(), eblocks);
+      k_dedup_expand<<<(unsigned)((pcap + EXP_BLK - 1) / EXP_BLK), EXP_T, 0, x->stream>>>(
+          seg_off, (uint32_t)icap, pcap, x->hslot.as<uint32_t>(), x->huid.as<uint64_t>(), x->uoff.as<uint64_t>(),
+          x->uout.as<uint2>(), reinterpret_cast<uint2*>(x->loc_pairs.p), x->blockmap2.as<uint32_t>(), &c.d_tot->npos);
+      CK(cudaGetLastError());
+    }
+  } else if (launch) {
+    k_graph_totals<<<1, 32, 0, x->stream>>>(x->seg_base.as<uint64_t>(), nq, x->pos_base.as<uint64_t>() + nq, nullptr,
+                                            pcap, c.d_tot);
+    k_block_first<<<(unsigned)((icap + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)icap, RES_T,
+                                                                        x->blockmap.as<uint32_t>(), rblocks);
+    ResolveArgs A{seg_row, 1, seg_off, (uint32_t)icap, pcap, d_bounds, nb, guard, x->loc_pairs.as<uint32_t>(),
+                  &dc->walk_err, &dc->steps, x->blockmap.as<uint32_t>(), &c.d_tot->npos};
+    k_resolve<false><<<(unsigned)((pcap + RES_T - 1) / RES_T), RES_T, 0, x->stream>>>(F.d, A);
+    CK(cudaGetLastError());
+  }
+  if (launch) {
+    CK(cudaMemcpyAsync(c.h_tot, c.d_tot, sizeof(GraphTotals), cudaMemcpyDeviceToHost, x->stream));
+    CK(cudaMemcpyAsync(c.h_ctr, dc, sizeof(Counters), cudaMemcpyDeviceToHost, x->stream));
+  }
+  return HFM_OK;
+}
+
 // H2D of a host query batch into the handle's buffers.
 static int stage_queries(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32_t nq) {
   if (nq && (!q_off)) return set_error(HFM_E_ARG, "q_off is NULL");
@@ -1330,7 +1470,7 @@ void hfm_index_free(hfm_index* x) {
                     &x->hkeys, &x->hslot, &x->hflags, &x->huid, &x->urow, &x->ulen, &x->uoff, &x->uout,
                     &x->blockmap, &x->blockmap2, &x->ovf2, &x->ovf3, &x->lflag, &x->lpos, &x->sids, &x->lids,
                     &x->ucount, &x->ubase, &x->uread, &x->uk, &x->ubits, &x->uexit, &x->ust, &x->ucoff, &x->ucnt,
-                    &x->segpool, &x->fxe, &x->fxc, &x->fxx, &x->fxo, &x->fxn, &x->npos, &x->iota})
+                    &x->segpool, &x->fxe, &x->fxc, &x->fxx, &x->fxo, &x->fxn, &x->npos, &x->iota, &x->loc_pairs})
     b->release();
   for (auto& e : x->ev) if (e) cudaEventDestroy(e);
   for (auto& e : x->evk) if (e) cudaEventDestroy(e);
@@ -1549,10 +1689,14 @@ struct hfm_graph {
   cudaGraphExec_t exec = nullptr;
   FixedChain c{};
   bool stale = true;                 // capture (again) before the next replay
-  uint64_t* h_bases = nullptr;       // pinned: the batch's total codes, read before each replay
+  uint64_t* h_bases = nullptr;       // pinned: the batch's total codes, then both chains' totals and counters
   uint32_t replays = 0, fallbacks = 0, last_reason = 0;
-  DevBuf tot;
+  DevBuf tot;                        // GraphTotals of the SMEM chain, then of the locate chain
   std::vector<uint32_t> bounds;      // host copy of the reference bounds (for the adaptive rerun)
+  bool has_loc = false;              // a locate chain precedes the SMEM chain in the graph
+  FixedLocate lc{};
+  DevBuf lctr;                       // the locate chain's counters
+  hfm_dev_hits loc_out{};            // the locate result of the last launch
 };
 
 namespace hfm {
@@ -1564,6 +1708,7 @@ static void free_graph(hfm_graph* g) {
     if (g->sh->stream) cudaStreamSynchronize(g->sh->stream);
     if (g->exec) cudaGraphExecDestroy(g->exec);
     g->tot.release();
+    g->lctr.release();
     hfm_index_free(g->sh);             // a shadow: the index buffers stay with their handle
   }
   if (g->h_bases) cudaFreeHost(g->h_bases);
@@ -1573,10 +1718,12 @@ static void free_graph(hfm_graph* g) {
 static int capture(hfm_graph* g) {
   hfm_index* x = g->sh;
   if (g->exec) { cudaGraphExecDestroy(g->exec); g->exec = nullptr; }
-  RET(fixed_chain(x, g->c, false));                // every allocation, outside the capture
+  if (g->has_loc) RET(fixed_locate(x, g->lc, false));   // every allocation, outside the capture
+  RET(fixed_chain(x, g->c, false));
   CK(cudaStreamSynchronize(x->stream));
   CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
-  int rc = fixed_chain(x, g->c, true);
+  int rc = g->has_loc ? fixed_locate(x, g->lc, true) : HFM_OK;
+  if (rc == HFM_OK) rc = fixed_chain(x, g->c, true);
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamEndCapture(x->stream, &graph);
   if (rc != HFM_OK) { if (graph) cudaGraphDestroy(graph); return rc; }
@@ -1606,8 +1753,8 @@ extern "C" int hfm_mems_graph_create(hfm_index* x, const uint8_t* d_q, const uin
   sh->miv_cap = std::max<uint64_t>(x->miv_cap, (uint64_t)nq * 24 + 4096);
   sh->hit_cap = std::max<uint64_t>(x->hit_cap, (uint64_t)nq * 24 + 4096);
   sh->seg_cap = x->seg_cap;
-  CK(cudaMallocHost((void**)&g->h_bases, 64));
-  RET(g->tot.ensure(64));
+  CK(cudaMallocHost((void**)&g->h_bases, 512));
+  RET(g->tot.ensure(2 * sizeof(GraphTotals)));
   RET(sh->ref_bounds.ensure((size_t)nb * 4 + 4));
   if (nb) CK(cudaMemcpy(sh->ref_bounds.p, ref_bounds, (size_t)nb * 4, cudaMemcpyHostToDevice));
   g->bounds.assign(ref_bounds, ref_bounds + nb);
@@ -1652,6 +1799,19 @@ extern "C" int hfm_mems_graph_launch(hfm_graph* g, hfm_dev_mems* out, uint32_t* 
       c.warp_cap = std::min<uint32_t>(c.warp_cap * 4, 1u << 22);
       c.warp_cands = std::min<uint32_t>(c.warp_cands * 4, 1u << 20);
     }
+    if (g->has_loc) {
+      const Counters& lk = *g->lc.h_ctr;
+      const GraphTotals& lt = *g->lc.h_tot;
+      if (lk.walk_err) return set_error(HFM_E_WALK, "LF walk exceeded sample_rate steps: index inconsistent");
+      if (lk.iv_used > g->lc.iv_cap || lk.still_ovf || lt.ovf) reason |= HFM_GRAPH_LOCATE;
+      if (lk.still_ovf) g->lc.warp_cap = std::min<uint32_t>(g->lc.warp_cap * 4, 1u << 22);
+      if (lk.iv_used > g->lc.iv_cap) g->lc.iv_cap = lk.iv_used + lk.iv_used / 4 + 4096;
+      if (!(reason & HFM_GRAPH_LOCATE)) {
+        FixedLocate& l = g->lc;
+        g->loc_out = hfm_dev_hits{l.nq, 0, lt.npos, x->pos_base.as<uint64_t>(), x->counts.as<uint32_t>(),
+                                  x->loc_pairs.as<uint32_t>()};
+      }
+    }
     g->last_reason = reason;
     if (!reason) {
       g->replays++;
@@ -1662,16 +1822,57 @@ extern "C" int hfm_mems_graph_launch(hfm_graph* g, hfm_dev_mems* out, uint32_t* 
       return HFM_OK;
     }
   }
-  // a capacity was outgrown: the adaptive chain (same results), then capture again with
-  // the capacities it grew to
+  // a capacity was outgrown: the adaptive chains (same results), then capture again with
+  // the capacities they grew to.  The adaptive locate leaves its positions where the SMEM
+  // chain puts its own, so it runs first and its positions move to the locate buffer.
   g->last_reason = reason;
   g->fallbacks++;
   g->stale = true;
+  if (g->has_loc && (reason & (HFM_GRAPH_LOCATE | HFM_GRAPH_BASES))) {
+    FixedLocate& l = g->lc;
+    hfm_dev_hits h{};
+    RET(locate_device(x, l.d_q, l.d_qoff, l.nq, l.max_hits, &h));
+    RET(x->loc_pairs.ensure(h.total * 8 + 8));
+    if (h.total) CK(cudaMemcpyAsync(x->loc_pairs.p, h.d_pairs, h.total * 8, cudaMemcpyDeviceToDevice, x->stream));
+    h.d_pairs = x->loc_pairs.as<uint32_t>();
+    g->loc_out = h;
+    l.pos_cap = std::max<uint64_t>(l.pos_cap, h.total + h.total / 4 + 4096);
+  }
   c.max_bases = std::max<uint64_t>(c.max_bases, g->h_bases[0] + g->h_bases[0] / 4);
   RET(mems_device(x, c.d_q, c.d_qoff, c.nq, c.P.min_len, c.P.mode, g->bounds.empty() ? nullptr : g->bounds.data(),
                   c.nb, c.P.max_hits, out));
   c.pos_cap = std::max<uint64_t>(c.pos_cap, out->n_positions + out->n_positions / 4 + 4096);
   if (replayed) *replayed = 0;
+  return HFM_OK;
+}
+
+extern "C" int hfm_mems_graph_add_locate(hfm_graph* g, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq,
+                                         uint32_t max_hits, uint64_t max_intervals, uint64_t max_positions) {
+  if (!g || !d_qoff || !nq) return set_error(HFM_E_ARG, "NULL argument or empty batch");
+  if (g->has_loc) return set_error(HFM_E_ARG, "the graph already has a locate chain");
+  hfm_index* x = g->sh;
+  std::lock_guard<std::mutex> lk(x->mu);
+  CK(cudaSetDevice(x->device));
+  RET(g->lctr.ensure(sizeof(Counters)));
+  FixedLocate& l = g->lc;
+  l.d_q = d_q; l.d_qoff = d_qoff; l.nq = nq; l.max_hits = max_hits;
+  l.iv_cap = std::max<uint64_t>(max_intervals, (uint64_t)nq * 2 + 4096);
+  l.pos_cap = std::max<uint64_t>(max_positions, 4096);
+  l.dedup = !(x->flags & HFM_FLAG_DEDUP_NEVER);
+  l.ctr = g->lctr.as<Counters>();
+  l.d_tot = g->tot.as<GraphTotals>() + 1;
+  l.h_tot = reinterpret_cast<GraphTotals*>(g->h_bases + 8);
+  l.h_ctr = reinterpret_cast<Counters*>(g->h_bases + 16);
+  g->has_loc = true;
+  int rc = capture(g);
+  if (rc != HFM_OK) g->has_loc = false;
+  return rc;
+}
+
+extern "C" int hfm_mems_graph_locate_result(const hfm_graph* g, hfm_dev_hits* out) {
+  if (!g || !out) return set_error(HFM_E_ARG, "NULL argument");
+  if (!g->has_loc) return set_error(HFM_E_ARG, "the graph has no locate chain");
+  *out = g->loc_out;
   return HFM_OK;
 }
 

@@ -323,6 +323,22 @@ __global__ void k_work_log(const uint64_t* __restrict__ hit_base, const uint64_t
   log[4 * (size_t)i + 2] = np > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)np;
 }
 
+// Graph-captured locate chain: queries whose intervals did not fit the pool report none
+// (they are flagged; the batch is rerun), so the CSR never reaches past the pool.
+__global__ void k_zero_failed(const uint32_t* __restrict__ status, uint32_t n, uint32_t* __restrict__ niv,
+                              uint64_t* __restrict__ nhits) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n && status[k] != 0) { niv[k] = 0; nhits[k] = 0; }
+}
+
+// seg_off[k] = total for k in [nseg, cap]: segments past the count are empty.
+__global__ void k_seal_segments(uint64_t* __restrict__ seg_off, const uint64_t* __restrict__ nseg_p,
+                                const uint64_t* __restrict__ total_p, uint64_t cap) {
+  const uint64_t nseg = *nseg_p, total = *total_p;
+  for (uint64_t k = nseg + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k <= cap; k += (uint64_t)gridDim.x * blockDim.x)
+    seg_off[k] = total;
+}
+
 __global__ void k_iota(uint32_t* __restrict__ ids, uint32_t n) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n) ids[k] = k;

@@ -1223,10 +1223,12 @@ __global__ void __launch_bounds__(128) k_bsearch_warp(DevFm F, const uint16_t* _
                                                      const uint8_t* __restrict__ q, const uint64_t* __restrict__ qoff,
                                                      const uint32_t* __restrict__ ids, uint32_t n, uint32_t hit_cap,
                                                      uint2* work, uint32_t set_cap, unsigned int* queue, Pool pool,
-                                                     BsOut out, uint32_t* still_ovf) {
+                                                     BsOut out, uint32_t* still_ovf,
+                                                     const uint32_t* __restrict__ n_dev = nullptr) {
   __shared__ SmemFm S;
   smem_fm_init(S, F, compat_masks);
   __syncthreads();
+  if (n_dev) n = *n_dev;                   // graph-captured chains: the count is on the device
   const int lane = threadIdx.x & 31;
   uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   uint2* A = work + warp * 2 * set_cap;

@@ -255,7 +255,21 @@ void hfm_mems_graph_free(hfm_graph* g);
 #define HFM_GRAPH_SEGMENTS 8u     /* long-read segment candidate pool                     */
 #define HFM_GRAPH_WARP_SETS 16u   /* a read's interval set outgrew the warp tier          */
 #define HFM_GRAPH_POSITIONS 32u   /* positions (or distinct positions) past the capacity  */
+#define HFM_GRAPH_LOCATE 64u      /* the locate chain outgrew one of its capacities       */
 int hfm_mems_graph_info(const hfm_graph* g, uint32_t* replays, uint32_t* fallbacks, uint32_t* last_reason);
+/* Adds the locate chain of hfm_locate_batch_device (backward search, merged intervals,
+ * resolve) for nq queries at fixed device addresses to the graph, ahead of its SMEM chain,
+ * so that one replay runs both (the whole batched query step of the reference's
+ * `query` and `mem`/`smem` paths, fm_index.rs and bidir.rs, without a host round trip
+ * between them).  max_intervals / max_positions: capacities of the merged-interval pool and
+ * of the resolved positions; a batch past either (or past the warp tier's set) is rerun on
+ * the adaptive chain with the same results and the capacities grow.  The locate result of
+ * the last hfm_mems_graph_launch is read with hfm_mems_graph_locate_result; it is that of
+ * hfm_locate_batch_device for the same queries, in the graph's own buffers, valid until
+ * the next launch. */
+int hfm_mems_graph_add_locate(hfm_graph* g, const uint8_t* d_q, const uint64_t* d_q_off, uint32_t nq,
+                              uint32_t max_hits, uint64_t max_intervals, uint64_t max_positions);
+int hfm_mems_graph_locate_result(const hfm_graph* g, hfm_dev_hits* out);
 
 /* Pre-sizes a handle's SMEM/MEM work pools and result arrays for a batch of nq reads
  * expected to produce `intervals` candidate intervals, `hits` MemHits and `positions`

@@ -146,3 +146,79 @@ def test_shared_handles_run_concurrently(oracle):
             _same(r, want)
     del shares, got
     _same(idx.handle.mems_packed(flat, off, 19, 0, bounds, 64), want)
+
+
+def _host_hits(h, dev):
+    counts = device_to_host(h.d_counts, h.nq, "<i4", dev).view(np.uint32)
+    offs = device_to_host(h.d_offsets, h.nq + 1, "<i8", dev).view(np.uint64)
+    pairs = device_to_host(h.d_pairs, 2 * h.total, "<i4", dev).view(np.uint32).reshape(-1, 2)
+    return counts, offs, pairs
+
+
+def test_graph_with_locate_chain(oracle):
+    """The locate chain captured ahead of the SMEM chain: one replay gives the locate CSR of
+    hfm_locate_batch_device and of the oracle, and the SMEM outputs as before; a batch of
+    patterns whose positions outgrow the locate capacity (all-N runs over an IUPAC reference)
+    reruns both chains adaptively, with the same bytes, and then replays."""
+    import torch
+    ref = synth.iupac_reference(total=2_000_000, n_contigs=20, n_run_mean=60, seed=91)
+    h, lib, bounds, bp, batches, nq, q_d, o_d, load, adaptive, want0, cap_bases = _case(ref, 0, 93, oracle)
+    data = _build([al.DnaSequence(c) for c in ref.contigs], FmIndexConfig(sa_sample_rate=32, lookup_depth=10), 0,
+                  KIND_BIDIR)
+    orc = oracle.OracleIndex(data, KIND_BIDIR)
+    rng = np.random.default_rng(94)
+    reads = synth.sample_reads(ref, n_reads=2000, seed=95)
+    kmers = [r[:32] for r in reads]
+    plain = kmers[:1500] + [r[40:52] for r in reads[:500]]          # few positions each
+    heavy = kmers[:1460] + [np.full(int(k), 5, np.uint8) for k in rng.integers(2, 5, 40)] + \
+        [r[40:52] for r in reads[:500]]                               # all-N: many positions
+    lq = len(plain)
+    assert len(heavy) == lq
+    packed = [L.pack_queries(q) for q in (plain, heavy)]
+    lcap = max(int(p[1][-1]) for p in packed)
+    lq_d = torch.zeros(lcap + 16, dtype=torch.uint8, device="cuda")
+    lo_d = torch.zeros(lq + 1, dtype=torch.int64, device="cuda")
+
+    def lload(k):
+        flat, off = packed[k]
+        lq_d[:len(flat)] = torch.from_numpy(flat).cuda()
+        lo_d.copy_(torch.from_numpy(off.astype(np.int64)).cuda())
+        torch.cuda.synchronize()
+
+    def ladaptive():
+        r = L.HfmDevHits()
+        torch.cuda.synchronize()
+        L.check(lib.hfm_locate_batch_device(h.h, lq_d.data_ptr(), lo_d.data_ptr(), lq, 256, C.byref(r)))
+        return _host_hits(r, 0)
+
+    lload(0)
+    lwant = ladaptive()
+    _same(lwant, orc.locate_packed(*packed[0], 256, threads=8))
+    g = C.c_void_p()
+    L.check(lib.hfm_mems_graph_create(h.h, q_d.data_ptr(), o_d.data_ptr(), nq, cap_bases, 19, 0, bp, len(bounds), 64,
+                                      2 * len(want0[2]) + 4096, C.byref(g)))
+    try:
+        L.check(lib.hfm_mems_graph_add_locate(g, lq_d.data_ptr(), lo_d.data_ptr(), lq, 256, 0,
+                                              2 * len(lwant[2]) + 1024))
+        rep = C.c_uint32()
+        why = C.c_uint32()
+        load(batches[0])
+        for k in (0, 1, 1, 0):
+            lload(k)
+            lw = ladaptive()
+            if k == 1:
+                _same(lw, orc.locate_packed(*packed[1], 256, threads=8))
+                assert len(lw[2]) > 2 * len(lwant[2]) + 1024
+            dm = L.HfmDevMems()
+            L.check(lib.hfm_mems_graph_launch(g, C.byref(dm), C.byref(rep)))
+            L.check(lib.hfm_mems_graph_info(g, None, None, C.byref(why)))
+            lr = L.HfmDevHits()
+            L.check(lib.hfm_mems_graph_locate_result(g, C.byref(lr)))
+            _same(_host_hits(lr, 0), lw)
+            _same(_host(dm, nq, 0), want0)
+            if k == 1 and rep.value == 0:
+                assert why.value & 64       # HFM_GRAPH_LOCATE
+        assert rep.value == 1 and why.value == 0
+        assert lib.hfm_mems_graph_add_locate(g, lq_d.data_ptr(), lo_d.data_ptr(), lq, 256, 0, 0) != 0
+    finally:
+        lib.hfm_mems_graph_free(g)
