@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the batch-latency measurement")
     ap.add_argument("--serving-batches", type=int, default=1000)
     ap.add_argument("--serving-workers", type=int, default=3)
+    ap.add_argument("--profile-step", action="store_true",
+                    help="only the W + K headline steps (the launch-list command)")
     ap.add_argument("--profile-smem", action="store_true",
                     help="one SMEM search launch (no position resolve) for ncu, then its work counters")
     return ap.parse_args()
@@ -313,6 +315,37 @@ def profile_smem(args):
     print(json.dumps({"profile": "smem_search", "reads": n, "k_mems_ms": s.ms_search_kernel,
                       "fallback_reads": s.fallback_reads, "mem_hits": dm.n_hits,
                       "occ_touches": h.stats().occ_touches}), flush=True)
+
+
+def profile_step(args):
+    """W untimed and K timed headline steps (locate of the 32-mer + find_smems over the
+    batch, plain order, default tuning) and nothing else: the command the launch list
+    (one ncu metric, every launch) is taken from."""
+    import torch
+    from haystackfm_b200 import _lib as L
+    from haystackfm_b200.fm_index import BidirFmIndex
+    _, data, reads, _, _ = workload(args)
+    idx = BidirFmIndex.from_bytes(data)
+    h, lib, n = idx.handle, L.lib(), args.reads
+    bounds = np.ascontiguousarray(idx.seq_boundaries(), dtype=np.uint32)
+    rd = torch.from_numpy(reads.reshape(-1)).cuda()
+    off = torch.arange(0, (n + 1) * 150, 150, dtype=torch.int64, device="cuda")
+    k32 = torch.from_numpy(np.ascontiguousarray(reads[:, :32]).reshape(-1)).cuda()
+    off32 = torch.arange(0, (n + 1) * 32, 32, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    launches = []
+    for k in range(args.warmup + args.steps):
+        dh, dm = L.HfmDevHits(), L.HfmDevMems()
+        L.check(lib.hfm_locate_batch_device(h.h, k32.data_ptr(), off32.data_ptr(), n, 1024, C.byref(dh)))
+        s1 = h.stats()
+        L.check(lib.hfm_mems_batch_device(h.h, rd.data_ptr(), off.data_ptr(), n, 19, 0, L.ptr(bounds, L.u32p),
+                                          len(bounds), 1024, C.byref(dm)))
+        s2 = h.stats()
+        launches.append(sum(s.search_launches + s.resolve_launches + s.other_launches for s in (s1, s2)))
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": "headline_step", "reads": n, "warmup": args.warmup, "steps": args.steps,
+                      "launches_per_step": launches, "mem_hits": dm.n_hits, "mem_positions": dm.n_positions,
+                      "locate_positions": dh.total}), flush=True)
 
 
 def serving_latency(h, lib, L, kp, rp, bounds, n, n_batches, seed=17):
@@ -638,6 +671,8 @@ def main():
         return run_reference(args)
     if args.profile_smem:
         return profile_smem(args)
+    if args.profile_step:
+        return profile_step(args)
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
