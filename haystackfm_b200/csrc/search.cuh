@@ -424,18 +424,6 @@ __device__ __forceinline__ uint32_t qmask(const SmemFm& S, uint8_t c) { return c
 // emit(qs, qe, count, set, pivot).  Returns the next pivot, max(reach, pivot + 1), or ~0u
 // on overflow (flags in st).  The sweep is a chain pivot -> next(pivot) that depends only
 // on the read, which is what lets a long read be cut into independently swept segments.
-//
-// Left-maximal starts without the full walk back.  start(e), the smallest j with q[j, e)
-// occurring, never decreases in e (an occurrence of q[j, e') contains one of q[j, e) for
-// e < e').  So at record point e, after record point e' < e with start s' and left-maximal
-// set S' (the intervals of q[s', e')): if S' extended right over q[e', e) is non-empty,
-// q[s', e) occurs, start(e) = s' and that extension is the set of q[s', e) — the same
-// intervals the walk back from the pivot ends with (one per distinct compatible text
-// string; their order differs, and the hits of a candidate are sorted by fwd_lo when
-// written).  If s' is the pivot, start(e) is the pivot and the set is the forward set.
-// Only when the extension dies does the walk back from the pivot run.  The candidates are
-// exactly those of the walk; the walk back's cost per record point (pivot - start steps
-// over the whole set) becomes e - e' steps over a set that is usually smaller.
 template <bool COUNT_TOUCH, uint32_t FMT, class SR, class Emit>
 __device__ __forceinline__ uint32_t smem_pivot(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf, const SmemFm& Sr,
                                                const uint8_t* q, uint32_t n, uint32_t pivot, const MemsParams& P,
@@ -451,12 +439,6 @@ __device__ __forceinline__ uint32_t smem_pivot(const DevFm& Fw, const DevFm& Rv,
   if (ovf) { st |= ST_SET_OVF; return ~0u; }
   if (c.size() == 0) return pivot + 1;
   uint32_t j = pivot + 1, reach = pivot + 1;
-  // the previous record point: its end, start, and left-maximal set (in wa/wb when
-  // pstart < pivot; pset holds its list sizes, pbuf which of the two buffers)
-  bool have_prev = false;
-  uint32_t pend = 0, pstart = 0, pcov = 0;
-  TL pset{wa, 0, 0};
-  int pbuf = 0;
   for (;;) {
     uint32_t end, ncov = 0;
     bool next_empty, record;
@@ -472,37 +454,15 @@ __device__ __forceinline__ uint32_t smem_pivot(const DevFm& Fw, const DevFm& Rv,
       reach = end;
       TL b = c;
       uint32_t start = pivot, bcov = cov;
-      bool found = false;
-      if (have_prev) {
-        if (pstart == pivot) found = true;           // start(end) = pivot: the forward set
-        else {
-          TL cur = pset, oth{pbuf ? wa : wb, 0, 0};
-          int cb = pbuf;
-          uint32_t ccov = pcov;
-          bool alive = true;
-          for (uint32_t k = pend; k < end; k++) {
-            uint32_t rcov;
-            extend_set<0, COUNT_TOUCH, FMT>(Rv, Sr, qmask(Sr, q[k]), cur, oth, set_cap, rcov, ovf, touches);
-            if (ovf) { st |= ST_SET_OVF; return ~0u; }
-            if (oth.size() == 0) { alive = false; break; }
-            const TL t = cur; cur = oth; oth = t; ccov = rcov; cb ^= 1;
-          }
-          if (alive) { b = cur; start = pstart; bcov = ccov; pbuf = cb; found = true; }
-        }
+      TL bufs[2] = {TL{wa, 0, 0}, TL{wb, 0, 0}};
+      int t = 0;
+      while (start > 0) {
+        uint32_t lcov;
+        extend_set<1, COUNT_TOUCH, FMT>(Fw, Sf, qmask(Sf, q[start - 1]), b, bufs[t], set_cap, lcov, ovf, touches);
+        if (ovf) { st |= ST_SET_OVF; return ~0u; }
+        if (bufs[t].size() == 0) break;
+        b = bufs[t]; bcov = lcov; t ^= 1; start--;
       }
-      if (!found) {
-        TL bufs[2] = {TL{wa, 0, 0}, TL{wb, 0, 0}};
-        int t = 0;
-        while (start > 0) {
-          uint32_t lcov;
-          extend_set<1, COUNT_TOUCH, FMT>(Fw, Sf, qmask(Sf, q[start - 1]), b, bufs[t], set_cap, lcov, ovf, touches);
-          if (ovf) { st |= ST_SET_OVF; return ~0u; }
-          if (bufs[t].size() == 0) break;
-          b = bufs[t]; bcov = lcov; t ^= 1; start--;
-        }
-        pbuf = t ^ 1;                                 // b's buffer when start < pivot
-      }
-      have_prev = true; pend = end; pstart = start; pcov = bcov; pset = b;
       if (end - start >= P.min_len) {
         // right-maximality (smem.rs:202-207); with no left extension it is next_empty
         bool rmax = end == n ||
