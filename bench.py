@@ -381,7 +381,7 @@ def serving_latency(h, lib, L, kp, rp, bounds, n, n_batches, seed=17):
 
 
 def serving_loop(h, lib, L, torch, dev, q, off, pool, bounds, n_batches, model, workers, rate=2000.0, seed=17):
-    """batches arrive as a Poisson stream (mean `rate` per second) with sizes
+    """The serving loop: batches arrive as a Poisson stream (mean `rate` per second) with sizes
     log-uniform in 1..100,000 reads, taken from a pool of mixed-length reads (80% 150 bp, 20%
     long) held in HBM.  A batch is admitted once the predicted output bytes of the batches in
     flight plus its own fit the HBM budget (the free device memory at the start, less a
@@ -478,7 +478,7 @@ def serving_loop(h, lib, L, torch, dev, q, off, pool, bounds, n_batches, model, 
 
 
 def genome_workloads(args, device, torch):
-    """configs[2] and configs[3] on a 3.1 Gbp repeat-rich ACGT genome (ExactDna
+    """The uneven-read and learned-predictor workloads on a 3.1 Gbp repeat-rich ACGT genome (ExactDna
     bidirectional index, sa_sample_rate 32, lookup_depth 10, built on the GPU):
 
     * uneven: 2M mixed-length reads, find_smems (min_len 19, max_hits 1024, positions
@@ -630,7 +630,7 @@ def genome_workloads(args, device, torch):
                          "mem_positions": int(dm.n_positions)}
         del got, ref
     out["learned"] = learned
-    # serving loop (configs[4]) on the same device-resident index
+    # serving loop on the same device-resident index
     if not args.no_serving and args.serving_batches > 0:
         out["serving"] = serving_loop(h, lib, L, torch, dev, em_q, em_o, args.eval_mixed, bounds, args.serving_batches,
                                       ls, args.serving_workers)
