@@ -936,14 +936,14 @@ def main():
         tj = json.load(open(tpath))
         if dom in tj:
             traffic = tj[dom]["dram_bytes_per_unit"] * units
-    # the random-access ceiling: independent 32 B / 64 B loads over 8 GB on every SM (the
-    # access pattern of Occ records, which a streaming copy does not have)
+    # the random-access ceiling: independent 32 B / 64 B / 96 B loads over 8 GB on every SM
+    # (the access pattern of Occ records, which a streaming copy does not have)
     gather = {}
-    for span in (32, 64):
+    for span in (32, 64, 96):
         gbs, gms = C.c_float(), C.c_float()
         L.check(lib.hfm_probe_gather(local, 8 << 30, span, C.byref(gbs), C.byref(gms)))
         gather[f"random_{span}B_gbs"] = round(gbs.value, 1)
-    rec_span = 32 if h.info().num_lanes <= 5 else 64
+    rec_span = 32 if h.info().num_lanes <= 5 else 96      # narrow / wide Occ record
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
                 "random_gather_ceiling": gather, "record_bytes": rec_span,

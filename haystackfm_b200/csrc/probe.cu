@@ -1,12 +1,12 @@
 // probe.cu — the random-access ceiling of the GPU this library runs on.
 //
 // The search and resolve kernels are chains of dependent random reads of 32-byte (narrow
-// Occ record, sampled-SA record) or 64-byte (wide Occ record) pieces of a table far larger
+// Occ record, sampled-SA record) or 96-byte (wide Occ record) pieces of a table far larger
 // than L2.  A streaming copy's bandwidth is not reachable by that pattern; this probe
-// measures what is: every thread issues independent loads of `span` bytes (32 or 64) at
-// uniformly random span-aligned offsets of a buffer of several GB, 256 bytes of them in
-// flight per thread, over a grid of resident threads on every SM.  No counterpart in the
-// reference.
+// measures what is: every thread issues independent loads of `span` bytes (32, 64 or 96)
+// at uniformly random span-aligned offsets of a buffer of several GB, 256-288 bytes of
+// them in flight per thread, over a grid of resident threads on every SM.  No counterpart
+// in the reference.
 
 #include <cuda_runtime.h>
 
@@ -53,7 +53,8 @@ __global__ void __launch_bounds__(256) k_probe_gather(const uint4* __restrict__ 
 using namespace hfm;
 
 extern "C" int hfm_probe_gather(int device, uint64_t buffer_bytes, uint32_t span, float* gbs_out, float* ms_out) {
-  if (!gbs_out || (span != 32 && span != 64)) return set_error(HFM_E_ARG, "span must be 32 or 64 and gbs_out set");
+  if (!gbs_out || (span != 32 && span != 64 && span != 96))
+    return set_error(HFM_E_ARG, "span must be 32, 64 or 96 and gbs_out set");
   if (buffer_bytes < (64ull << 20)) return set_error(HFM_E_ARG, "buffer_bytes below 64 MiB");
   if (cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); return set_error(HFM_E_ARG, "device ordinal out of range"); }
   int sms = 0;
@@ -67,12 +68,13 @@ extern "C" int hfm_probe_gather(int device, uint64_t buffer_bytes, uint32_t span
   cudaMemsetAsync(buf, 0x5a, buffer_bytes, s);
   const uint64_t nspans = buffer_bytes / span;
   const unsigned grid = (unsigned)sms * 8, block = 256;
-  const uint32_t rounds = 64, depth = span == 32 ? 8 : 4;     // 256 bytes in flight per thread
+  const uint32_t rounds = 64, depth = span == 32 ? 8 : span == 64 ? 4 : 3;   // 256-288 bytes in flight per thread
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0); cudaEventCreate(&e1);
   auto launch = [&](uint64_t seed) {
     if (span == 32) k_probe_gather<32, 8><<<grid, block, 0, s>>>((const uint4*)buf, nspans, rounds, seed, sink);
-    else k_probe_gather<64, 4><<<grid, block, 0, s>>>((const uint4*)buf, nspans, rounds, seed, sink);
+    else if (span == 64) k_probe_gather<64, 4><<<grid, block, 0, s>>>((const uint4*)buf, nspans, rounds, seed, sink);
+    else k_probe_gather<96, 3><<<grid, block, 0, s>>>((const uint4*)buf, nspans, rounds, seed, sink);
   };
   launch(1);                                   // warm-up
   cudaEventRecord(e0, s);

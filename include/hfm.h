@@ -320,9 +320,10 @@ int hfm_mlp_schedule(hfm_mlp* m, const float* d_y, uint32_t nq, float warp_min_h
                      uint32_t* n_warp);
 
 /* Random-access ceiling of GPU `device` (no counterpart in the reference): independent
- * loads of `span` (32 or 64) bytes at uniformly random span-aligned offsets of a
- * buffer_bytes device buffer (>= 64 MiB; it is allocated and freed by the call), 256 bytes
- * in flight per thread on 8 x 256 threads per SM.  *gbs_out = bytes loaded / second
+ * loads of `span` (32, 64 or 96: a narrow Occ record, a half, a wide record) bytes at
+ * uniformly random span-aligned offsets of a buffer_bytes device buffer (>= 64 MiB; it is
+ * allocated and freed by the call), 256-288 bytes in flight per thread on 8 x 256 threads
+ * per SM.  *gbs_out = bytes loaded / second
  * (CUDA events), *ms_out (may be NULL) = one launch. */
 int hfm_probe_gather(int device, uint64_t buffer_bytes, uint32_t span, float* gbs_out, float* ms_out);
 

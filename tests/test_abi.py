@@ -146,3 +146,22 @@ def test_oracle_doubling_sort_equals_comparison_sort(oracle):
 
 def test_null_handle_timeout_rejected():
     assert L.lib().hfm_set_timeout(None, 5) == HFM_E_ARG
+
+
+def test_graph_and_probe_arguments_rejected_without_a_gpu():
+    """The graph and probe entry points check their arguments before any device work: a
+    missing graph or output, an unsupported probe span, a buffer below 64 MiB."""
+    import ctypes as C
+    lib = L.lib()
+    g = C.c_void_p()
+    assert lib.hfm_mems_graph_create(None, None, None, 0, 0, 19, 0, None, 0, 64, 0, C.byref(g)) == HFM_E_ARG
+    assert lib.hfm_mems_graph_launch(None, None, None) == HFM_E_ARG
+    assert lib.hfm_mems_graph_add_locate(None, None, None, 0, 0, 0, 0) == HFM_E_ARG
+    assert lib.hfm_mems_graph_locate_result(None, None) == HFM_E_ARG
+    assert lib.hfm_mems_graph_info(None, None, None, None) == HFM_E_ARG
+    lib.hfm_mems_graph_free(None)                             # no-op
+    gbs = C.c_float()
+    assert lib.hfm_probe_gather(0, 1 << 30, 48, C.byref(gbs), None) == HFM_E_ARG
+    assert b"span" in lib.hfm_last_error()
+    assert lib.hfm_probe_gather(0, 1 << 20, 32, C.byref(gbs), None) == HFM_E_ARG
+    assert lib.hfm_probe_gather(0, 1 << 30, 32, None, None) == HFM_E_ARG

@@ -54,3 +54,18 @@ def test_gpu_builder_bytes_equal_cpu_builder_genomes():
     rep = synth.repeat_reference(total=3_000_000, n_contigs=6, seed=62)
     cpu, gpu = _both(rep.contigs, 32, 10, 1, 0, KIND_BIDIR)
     assert gpu == cpu
+
+
+def test_random_gather_probe_rates():
+    """The random-gather probe: every record span gives a finite positive rate, and the
+    wider spans move more bytes per second than the 32-byte one (more sectors per miss)."""
+    import ctypes as C
+    from haystackfm_b200 import _lib as L
+    lib = L.lib()
+    rates = {}
+    for span in (32, 64, 96):
+        gbs, ms = C.c_float(), C.c_float()
+        L.check(lib.hfm_probe_gather(0, 1 << 30, span, C.byref(gbs), C.byref(ms)))
+        assert 0 < gbs.value < 1e5 and ms.value > 0
+        rates[span] = gbs.value
+    assert rates[64] > rates[32] * 0.8 and rates[96] > rates[32] * 0.8
