@@ -411,13 +411,14 @@ static int run_bsearch(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
 
 static int resolve(hfm_index* x, const FmDev& F, const uint32_t* seg_row, uint32_t stride, const uint64_t* seg_off,
                    uint64_t nseg, uint64_t total, const uint32_t* d_bounds, uint32_t nb, uint32_t* out,
-                   uint32_t& launches) {
+                   uint32_t& launches, uint32_t& other) {
   if (total == 0) return HFM_OK;
   if (nseg >= 0xFFFFFFFFull) return set_error(HFM_E_ARG, "too many intervals in one call");
   uint64_t blocks = (total + RES_T - 1) / RES_T;
   RET(x->blockmap.ensure(blocks * 4 + 4));
   k_block_first<<<(unsigned)((nseg + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)nseg, RES_T,
                                                                      x->blockmap.as<uint32_t>());
+  other++;
   ResolveArgs A{seg_row, stride, seg_off, (uint32_t)nseg, total, d_bounds, nb,
                 F.rate ? F.rate : F.text_len, out, &dctr(x)->walk_err, &dctr(x)->steps, x->blockmap.as<uint32_t>()};
   // grid.x limit 2^31-1 blocks covers 5e11 positions
@@ -438,7 +439,7 @@ static int resolve_segments(hfm_index* x, const FmDev& F, const uint32_t* seg_ro
                             uint32_t nb, uint32_t* out, uint32_t& launches, uint32_t& other) {
   if (total == 0) return HFM_OK;
   bool dedup = (x->flags & HFM_FLAG_DEDUP_ALWAYS) || (!(x->flags & HFM_FLAG_DEDUP_NEVER) && total >= 4 * nseg);
-  if (!dedup || nseg < 2) return resolve(x, F, seg_row, stride, seg_off, nseg, total, d_bounds, nb, out, launches);
+  if (!dedup || nseg < 2) return resolve(x, F, seg_row, stride, seg_off, nseg, total, d_bounds, nb, out, launches, other);
   uint64_t size = 1024;
   while (size < 2 * nseg) size <<= 1;
   RET(x->hkeys.ensure(size * 8)); RET(x->hslot.ensure(nseg * 4 + 4));
@@ -465,7 +466,7 @@ static int resolve_segments(hfm_index* x, const FmDev& F, const uint32_t* seg_ro
   RET(read_u64(x, x->uoff.as<uint64_t>() + nuniq, utotal));
   RET(x->uout.ensure(utotal * 8 + 8));
   RET(resolve(x, F, x->urow.as<uint32_t>(), 1, x->uoff.as<uint64_t>(), nuniq, utotal, d_bounds, nb,
-              x->uout.as<uint32_t>(), launches));
+              x->uout.as<uint32_t>(), launches, other));
   RET(x->blockmap2.ensure(((total + EXP_BLK - 1) / EXP_BLK) * 4 + 4));
   k_block_first<<<(unsigned)((nseg + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)nseg, EXP_BLK,
                                                                      x->blockmap2.as<uint32_t>());
