@@ -71,7 +71,7 @@ class HfmTuning(C.Structure):
 
 # hfm_autotune_mems candidates {variant, seg_len, queue_chunk, threads_per_read}, in order
 TUNE_CANDIDATES = [(3, 512, 1, 1), (3, 256, 1, 1), (3, 1024, 1, 1), (2, 512, 1, 1), (3, 512, 4, 1), (3, 512, 16, 1),
-                   (3, 512, 1, 32)]
+                   (3, 512, 1, 4), (3, 512, 1, 8), (3, 512, 1, 32)]
 
 
 class HfmStats(C.Structure):

@@ -558,8 +558,9 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   if (mode > 1) return set_error(HFM_E_ARG, "mode must be 0 (SMEM) or 1 (MEM)");
   const uint32_t* order = sc ? sc->d_order : nullptr;
   uint32_t n_warp = sc ? sc->n_warp : 0;
-  if (!sc && x->threads_per_read == 32 && x->mems_variant != MEMS_PLAIN && nq) {
-    // every read on the warp-per-read kernel: the identity order, all of it routed
+  if (!sc && x->threads_per_read > 1 && x->mems_variant != MEMS_PLAIN && nq) {
+    // every read on the lane-group kernels (a warp or 4, 8, 16 lanes per read): the
+    // identity order, all of it routed
     RET(x->iota.ensure((size_t)nq * 4));
     k_iota<<<(nq + 255) / 256, 256, 0, x->stream>>>(x->iota.as<uint32_t>(), nq);
     CK(cudaGetLastError());
@@ -836,6 +837,38 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
       }
       n_ovf = x->h_ctr->n_wrp;
       wlist = x->ovf2.as<uint32_t>();
+    }
+    const uint32_t G = (!sc && n_warp == nq && x->threads_per_read > 1) ? x->threads_per_read : 32u;
+    if (n_ovf && G < 32) {
+      // sub-warp pass over every read (threads_per_read 4, 8 or 16): one read per group of
+      // G lanes with the fast pass's set and candidate capacities; reads that outgrow them
+      // go on to the warp tier below
+      const uint64_t per_group = (uint64_t)MEM_SET_CAP * 4 * 16 + (uint64_t)FAST_CAND_CAP * sizeof(Cand);
+      const uint64_t groups = std::min<uint64_t>({(uint64_t)n_ovf, (uint64_t)x->num_sms * (2048 / G),
+                                                  std::max<uint64_t>(128 / G, (8ull << 30) / per_group)});
+      const unsigned grid = (unsigned)((groups * G + 127) / 128);
+      RET(x->work.ensure((size_t)grid * (128 / G) * MEM_SET_CAP * 4 * 16));
+      RET(x->cwork.ensure((size_t)grid * (128 / G) * FAST_CAND_CAP * sizeof(Cand)));
+      RET(x->ovf3.ensure((size_t)nq * 4 + 4));
+      CK(cudaMemsetAsync(&dctr(x)->n_mid, 0, 4, x->stream));
+      CK(cudaMemsetAsync(&dctr(x)->queue2, 0, 4, x->stream));
+      MemsWork W{x->work.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), FAST_CAND_CAP, &dctr(x)->queue2, wlist,
+                 n_ovf, &dctr(x)->still_ovf, 0u, wlog};
+      MemsOut o3 = o;
+      o3.ovf_list = x->ovf3.as<uint32_t>();
+      o3.n_ovf = &dctr(x)->n_mid;
+      auto sub = [&](auto kern) {
+        kern<<<grid, 128, 0, x->stream>>>(Fw.d, Rv.d, Fw.compat.as<uint16_t>(), Rv.compat.as<uint16_t>(), d_q, d_qoff,
+                                          P, ivp, hp, o3, W);
+      };
+      if (G == 4) { if (counting) sub(k_mems_warp<true, 4>); else sub(k_mems_warp<false, 4>); }
+      else if (G == 8) { if (counting) sub(k_mems_warp<true, 8>); else sub(k_mems_warp<false, 8>); }
+      else { if (counting) sub(k_mems_warp<true, 16>); else sub(k_mems_warp<false, 16>); }
+      launches++;
+      CK(cudaGetLastError());
+      RET(read_ctr(x));
+      n_ovf = x->h_ctr->n_mid;
+      wlist = x->ovf3.as<uint32_t>();
     }
     if (n_ovf) {
       // long tail: one warp per overflowed read, 4 sets and a candidate list per warp,
@@ -1512,7 +1545,9 @@ int hfm_set_tuning(hfm_index* x, const hfm_tuning* t) {
   if (t->mems_variant < 2 || t->mems_variant > 4) return set_error(HFM_E_ARG, "mems_variant must be 2, 3 or 4");
   if (t->seg_len < 64 || t->seg_len > SEG_MAX || t->seg_len % 32) return set_error(HFM_E_ARG, "seg_len must be a multiple of 32 in 64..4096");
   if (t->queue_chunk < 1 || t->queue_chunk > 64) return set_error(HFM_E_ARG, "queue_chunk must be in 1..64");
-  if (t->threads_per_read != 1 && t->threads_per_read != 32) return set_error(HFM_E_ARG, "threads_per_read must be 1 or 32");
+  if (t->threads_per_read != 1 && t->threads_per_read != 4 && t->threads_per_read != 8 && t->threads_per_read != 16 &&
+      t->threads_per_read != 32)
+    return set_error(HFM_E_ARG, "threads_per_read must be 1, 4, 8, 16 or 32");
   std::lock_guard<std::mutex> lk(x->mu);
   x->mems_variant = (int)t->mems_variant;
   x->seg_len = t->seg_len;
@@ -1530,7 +1565,8 @@ int hfm_autotune_mems(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, 
   Guard g(x);
   // HFM_TUNE_CANDIDATES settings, in the order include/hfm.h lists them
   const hfm_tuning cands[HFM_TUNE_CANDIDATES] = {{3, 512, 1, 1}, {3, 256, 1, 1}, {3, 1024, 1, 1}, {2, 512, 1, 1},
-                                                 {3, 512, 4, 1}, {3, 512, 16, 1}, {3, 512, 1, 32}};
+                                                 {3, 512, 4, 1}, {3, 512, 16, 1}, {3, 512, 1, 4},  {3, 512, 1, 8},
+                                                 {3, 512, 1, 32}};
   const hfm_tuning saved{(uint32_t)x->mems_variant, x->seg_len, x->queue_chunk, x->threads_per_read};
   auto apply = [&](const hfm_tuning& t) {
     x->mems_variant = (int)t.mems_variant; x->seg_len = t.seg_len;

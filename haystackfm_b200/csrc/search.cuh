@@ -1140,6 +1140,31 @@ __device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, uint32_t& total) 
   return x - v;
 }
 
+// Lane groups of G = 4, 8, 16 or 32 lanes (one read per group in the sub-warp and
+// warp-per-read SMEM kernels): the group's member mask, sum and exclusive scan.
+template <int G>
+__device__ __forceinline__ uint32_t grp_mask() {
+  if (G == 32) return 0xFFFFFFFFu;
+  return ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(uint32_t)(G - 1));
+}
+template <int G>
+__device__ __forceinline__ uint32_t grp_sum(uint32_t v) {
+  const uint32_t m = grp_mask<G>();
+#pragma unroll
+  for (int d = G / 2; d > 0; d >>= 1) v += __shfl_xor_sync(m, v, d, G);
+  return v;
+}
+template <int G>
+__device__ __forceinline__ uint32_t grp_excl_scan(uint32_t v, uint32_t& total) {
+  const uint32_t m = grp_mask<G>();
+  const int gl = threadIdx.x & (G - 1);
+  uint32_t x = v;
+#pragma unroll
+  for (int d = 1; d < G; d <<= 1) { uint32_t y = __shfl_up_sync(m, x, d, G); if (gl >= d) x += y; }
+  total = __shfl_sync(m, x, G - 1, G);
+  return x - v;
+}
+
 // Backward-search step set (sorted, coalesced) with the warp: counting sort by symbol
 // (pass 1 counts with ballots, pass 2 places), then lane 0 coalesces touching neighbours.
 template <bool COUNT_TOUCH>
@@ -1272,13 +1297,13 @@ __global__ void __launch_bounds__(128) k_bsearch_warp(DevFm F, const uint16_t* _
   if (COUNT_TOUCH && touches) atomicAdd(out.touches, (unsigned long long)touches);
 }
 
-// One extension of the whole set by the warp (outputs in lane-chunk order).
-template <int DIR, bool COUNT_TOUCH>
+// One extension of the whole set by a group of G lanes (outputs in lane-chunk order).
+template <int DIR, bool COUNT_TOUCH, int G = 32>
 __device__ uint32_t warp_extend_set(const DevFm& X, const SmemFm& S, uint32_t mask, const BIv* in, uint32_t nin,
                                     BIv* out, uint32_t cap, uint32_t& cov, bool& ovf, uint64_t& touches) {
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & (G - 1);
   uint32_t nout = 0, covl = 0;
-  for (uint32_t b = 0; b < nin; b += 32) {
+  for (uint32_t b = 0; b < nin; b += G) {
     uint32_t i = b + lane;
     BIv iv = i < nin ? in[i] : BIv{0, 0, 0, 0};
     uint32_t a = DIR == 0 ? iv.rlo : iv.flo, e = DIR == 0 ? iv.rhi : iv.fhi;
@@ -1291,7 +1316,7 @@ __device__ uint32_t warp_extend_set(const DevFm& X, const SmemFm& S, uint32_t ma
 #pragma unroll
     for (int s = 0; s < 16; s++) k += (i < nin && ((mask >> s) & 1) && rh[s] > rl[s]) ? 1u : 0u;
     uint32_t total;
-    uint32_t pos = nout + warp_excl_scan(k, total);
+    uint32_t pos = nout + grp_excl_scan<G>(k, total);
     if (nout + total > cap) { ovf = true; return nout; }
     uint32_t run = 0;
 #pragma unroll
@@ -1308,17 +1333,17 @@ __device__ uint32_t warp_extend_set(const DevFm& X, const SmemFm& S, uint32_t ma
     }
     nout += total;
   }
-  cov = warp_sum(covl);
-  __syncwarp();
+  cov = grp_sum<G>(covl);
+  __syncwarp(grp_mask<G>());
   return nout;
 }
 
-template <int DIR, bool COUNT_TOUCH>
+template <int DIR, bool COUNT_TOUCH, int G = 32>
 __device__ bool warp_any_extend(const DevFm& X, const SmemFm& S, uint32_t mask, const BIv* in, uint32_t nin,
                                 uint64_t& touches) {
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & (G - 1);
   bool any = false;
-  for (uint32_t b = 0; b < nin && !any; b += 32) {
+  for (uint32_t b = 0; b < nin && !any; b += G) {
     uint32_t i = b + lane;
     BIv iv = i < nin ? in[i] : BIv{0, 0, 0, 0};
     uint32_t a = DIR == 0 ? iv.rlo : iv.flo, e = DIR == 0 ? iv.rhi : iv.fhi;
@@ -1329,18 +1354,19 @@ __device__ bool warp_any_extend(const DevFm& X, const SmemFm& S, uint32_t mask, 
     bool mine = false;
 #pragma unroll
     for (int s = 0; s < 16; s++) mine |= i < nin && ((mask >> s) & 1) && rh[s] != rl[s];
-    any = __any_sync(0xFFFFFFFFu, mine);
+    any = __any_sync(grp_mask<G>(), mine);
   }
   return any;
 }
 
-// Candidate search of one read by the warp; control flow is warp-uniform.
-template <bool COUNT_TOUCH>
+// Candidate search of one read by a group of G lanes; control flow is group-uniform.
+template <bool COUNT_TOUCH, int G = 32>
 __device__ uint32_t warp_mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm& Sf, const SmemFm& Sr,
                                   const uint8_t* q, uint32_t n, const MemsParams& P, BIv* curr, BIv* nxt, BIv* wa,
                                   BIv* wb, uint32_t set_cap, Cand* cands, uint32_t cand_cap, Pool& ivpool,
                                   uint32_t& st, uint64_t& touches) {
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & (G - 1);
+  const uint32_t gm = grp_mask<G>();
   uint32_t nc = 0;
   if (n == 0 || P.min_len == 0) return 0;
   const BIv full = {0, Fw.text_len, 0, Fw.text_len};
@@ -1350,31 +1376,31 @@ __device__ uint32_t warp_mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm
     if (nc >= cand_cap) { st |= ST_CAND_OVF; return false; }
     uint64_t off = 0;
     if (lane == 0) off = thread_reserve(ivpool, niv);
-    off = __shfl_sync(0xFFFFFFFFu, off, 0);
+    off = __shfl_sync(gm, off, 0, G);
     if (off == ~0ull) { st |= ST_POOL_OVF; return false; }
     BIv* dst = (BIv*)ivpool.base + off;
-    for (uint32_t k = lane; k < niv; k += 32) dst[k] = ivs[k];
+    for (uint32_t k = lane; k < niv; k += G) dst[k] = ivs[k];
     if (lane == 0) cands[nc] = Cand{qs, qe, count, niv, off};
     nc++;
-    __syncwarp();
+    __syncwarp(gm);
     return true;
   };
   if (P.mode == 1) {
     for (uint32_t i = 0; i < n; i++) {
       BIv* c = curr; BIv* x = nxt;
       if (lane == 0) c[0] = full;
-      __syncwarp();
+      __syncwarp(gm);
       uint32_t ncur = 1, cov = 0, j = i;
       bool matched = false;
       while (j < n) {
         uint32_t ncov;
-        uint32_t nn = warp_extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, ncur, x, set_cap, ncov, ovf, touches);
+        uint32_t nn = warp_extend_set<0, COUNT_TOUCH, G>(Rv, Sr, qmask(Sr, q[j]), c, ncur, x, set_cap, ncov, ovf, touches);
         if (ovf) { st |= ST_SET_OVF; return ~0u; }
         if (nn == 0) break;
         BIv* t = c; c = x; x = t; ncur = nn; cov = ncov; j++; matched = true;
       }
       if (!matched || j - i < P.min_len) continue;
-      bool lmax = i == 0 || !warp_any_extend<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[i - 1]), c, ncur, touches);
+      bool lmax = i == 0 || !warp_any_extend<1, COUNT_TOUCH, G>(Fw, Sf, qmask(Sf, q[i - 1]), c, ncur, touches);
       if (!lmax) continue;
       if (!emit(i, j, cov, c, ncur)) return ~0u;
     }
@@ -1384,9 +1410,9 @@ __device__ uint32_t warp_mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm
   while (pivot < n) {
     BIv* c = curr; BIv* x = nxt;
     if (lane == 0) x[0] = full;
-    __syncwarp();
+    __syncwarp(gm);
     uint32_t cov;
-    uint32_t ncur = warp_extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[pivot]), x, 1, c, set_cap, cov, ovf, touches);
+    uint32_t ncur = warp_extend_set<0, COUNT_TOUCH, G>(Rv, Sr, qmask(Sr, q[pivot]), x, 1, c, set_cap, cov, ovf, touches);
     if (ovf) { st |= ST_SET_OVF; return ~0u; }
     if (ncur == 0) { pivot++; continue; }
     uint32_t j = pivot + 1, reach = pivot + 1;
@@ -1395,7 +1421,7 @@ __device__ uint32_t warp_mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm
       bool next_empty, record;
       if (j == n) { end = n; next_empty = true; record = true; }
       else {
-        nn = warp_extend_set<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[j]), c, ncur, x, set_cap, ncov, ovf, touches);
+        nn = warp_extend_set<0, COUNT_TOUCH, G>(Rv, Sr, qmask(Sr, q[j]), c, ncur, x, set_cap, ncov, ovf, touches);
         if (ovf) { st |= ST_SET_OVF; return ~0u; }
         end = j; next_empty = nn == 0; record = ncov != cov;
       }
@@ -1407,14 +1433,14 @@ __device__ uint32_t warp_mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm
         int t = 0;
         while (start > 0) {
           uint32_t lcov;
-          uint32_t nl = warp_extend_set<1, COUNT_TOUCH>(Fw, Sf, qmask(Sf, q[start - 1]), b, nb, bufs[t], set_cap, lcov, ovf, touches);
+          uint32_t nl = warp_extend_set<1, COUNT_TOUCH, G>(Fw, Sf, qmask(Sf, q[start - 1]), b, nb, bufs[t], set_cap, lcov, ovf, touches);
           if (ovf) { st |= ST_SET_OVF; return ~0u; }
           if (nl == 0) break;
           b = bufs[t]; nb = nl; bcov = lcov; t ^= 1; start--;
         }
         if (end - start >= P.min_len) {
           bool rmax = end == n ||
-                      (start == pivot ? next_empty : !warp_any_extend<0, COUNT_TOUCH>(Rv, Sr, qmask(Sr, q[end]), b, nb, touches));
+                      (start == pivot ? next_empty : !warp_any_extend<0, COUNT_TOUCH, G>(Rv, Sr, qmask(Sr, q[end]), b, nb, touches));
           if (rmax && !emit(start, end, bcov, b, nb)) return ~0u;
         }
       }
@@ -1426,7 +1452,11 @@ __device__ uint32_t warp_mems_one(const DevFm& Fw, const DevFm& Rv, const SmemFm
   return nc;
 }
 
-template <bool COUNT_TOUCH>
+// Persistent SMEM / MEM search with one read per group of G lanes (G = 32: the warp tier
+// of reads whose sets outgrew the per-thread kernels; G = 4, 8, 16: the sub-warp
+// candidates of the autotuner).  Group g of the grid owns sets and a candidate list at
+// g * 4 * set_cap / g * cand_cap.
+template <bool COUNT_TOUCH, int G = 32>
 __global__ void __launch_bounds__(128) k_mems_warp(DevFm Fw, DevFm Rv, const uint16_t* __restrict__ compat_fw,
                                                   const uint16_t* __restrict__ compat_rv, const uint8_t* __restrict__ q,
                                                   const uint64_t* __restrict__ qoff, MemsParams P, Pool ivpool,
@@ -1435,26 +1465,27 @@ __global__ void __launch_bounds__(128) k_mems_warp(DevFm Fw, DevFm Rv, const uin
   smem_fm_init(Sf, Fw, compat_fw);
   smem_fm_init(Sr, Rv, compat_rv);
   __syncthreads();
-  const int lane = threadIdx.x & 31;
-  uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  BIv* base = W.sets + warp * 4 * W.set_cap;
-  Cand* cands = W.cands + warp * W.cand_cap;
+  const int lane = threadIdx.x & (G - 1);
+  const uint32_t gm = grp_mask<G>();
+  uint64_t grp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / G;
+  BIv* base = W.sets + grp * 4 * W.set_cap;
+  Cand* cands = W.cands + grp * W.cand_cap;
   uint64_t touches = 0;
   for (;;) {
     uint32_t k = 0;
     if (lane == 0) k = atomicAdd(W.queue, 1u);
-    k = __shfl_sync(0xFFFFFFFFu, k, 0);
+    k = __shfl_sync(gm, k, 0, G);
     if (k >= W.count()) break;
     uint32_t i = W.ids[k];
     uint32_t st = ST_OK;
     uint64_t o = qoff[i];
     uint64_t t0 = touches;
-    uint32_t nc = warp_mems_one<COUNT_TOUCH>(Fw, Rv, Sf, Sr, q + o, (uint32_t)(qoff[i + 1] - o), P, base,
-                                             base + W.set_cap, base + 2 * W.set_cap, base + 3 * W.set_cap, W.set_cap,
-                                             cands, W.cand_cap, ivpool, st, touches);
-    __syncwarp();
+    uint32_t nc = warp_mems_one<COUNT_TOUCH, G>(Fw, Rv, Sf, Sr, q + o, (uint32_t)(qoff[i + 1] - o), P, base,
+                                                base + W.set_cap, base + 2 * W.set_cap, base + 3 * W.set_cap,
+                                                W.set_cap, cands, W.cand_cap, ivpool, st, touches);
+    __syncwarp(gm);
     if (COUNT_TOUCH && W.work_log) {
-      uint32_t d = warp_sum((uint32_t)(touches - t0));
+      uint32_t d = grp_sum<G>((uint32_t)(touches - t0));
       if (lane == 0) { W.work_log[4 * (size_t)i] += d; W.work_log[4 * (size_t)i + 3] |= 3u; }
     }
     if (lane == 0) {
@@ -1465,9 +1496,12 @@ __global__ void __launch_bounds__(128) k_mems_warp(DevFm Fw, DevFm Rv, const uin
       }
       if (st) { hs = 0; hc = 0; }
       out.hit_start[i] = hs; out.hit_count[i] = hc; out.status[i] = st;
-      if (st & (ST_SET_OVF | ST_CAND_OVF)) atomicAdd(W.still_ovf, 1u);
+      if (st & (ST_SET_OVF | ST_CAND_OVF)) {
+        if (W.rerun) atomicAdd(W.still_ovf, 1u);
+        else out.ovf_list[atomicAdd(out.n_ovf, 1u)] = i;      // on to the warp tier
+      }
     }
-    __syncwarp();
+    __syncwarp(gm);
   }
   if (COUNT_TOUCH && touches) atomicAdd(out.touches, (unsigned long long)touches);
 }

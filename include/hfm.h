@@ -357,14 +357,17 @@ int hfm_set_timeout(hfm_index* idx, uint32_t ms);
  *                     (multiple of 32 in 64..4096, default 512).
  *   queue_chunk       reads a per-thread kernel takes from its device work queue per atomic
  *                     (1..64, default 1).
- *   threads_per_read  1 (default): a thread per read; 32: every read on the warp-per-read
- *                     kernel (the 32 lanes share each interval set).
+ *   threads_per_read  1 (default): a thread per read; 4, 8 or 16: every read on a group of
+ *                     that many lanes (sub-warp kernel, the fast pass's set capacities; a
+ *                     read that outgrows them goes on to the warp tier); 32: every read on
+ *                     the warp-per-read kernel (the lanes of a group share each interval set).
  * hfm_autotune_mems times the search of a sample batch under each of the HFM_TUNE_CANDIDATES
  * settings {variant, seg_len, chunk, threads}: {3,512,1,1}, {3,256,1,1}, {3,1024,1,1},
- * {2,512,1,1}, {3,512,4,1}, {3,512,16,1}, {3,512,1,32} — best of `reps` runs after a warm-up
- * run, by CUDA events on the handle's stream; it keeps the fastest on the handle, writes it
- * to *best, and the candidates' times to times_ms[HFM_TUNE_CANDIDATES] when non-NULL. */
-#define HFM_TUNE_CANDIDATES 7
+ * {2,512,1,1}, {3,512,4,1}, {3,512,16,1}, {3,512,1,4}, {3,512,1,8}, {3,512,1,32} — best of
+ * `reps` runs after a warm-up run, by CUDA events on the handle's stream; it keeps the
+ * fastest on the handle, writes it to *best, and the candidates' times to
+ * times_ms[HFM_TUNE_CANDIDATES] when non-NULL. */
+#define HFM_TUNE_CANDIDATES 9
 typedef struct hfm_tuning {
   uint32_t mems_variant;
   uint32_t seg_len;

@@ -129,11 +129,12 @@ def test_autotune_keeps_results(oracle):
                           "threads_per_read": chosen[3]}
     assert len(res["candidates_ms"]) == len(L.TUNE_CANDIDATES) and all(v > 0 for v in res["candidates_ms"].values())
     for v, sl, ch, tp in [(3, 64, 1, 1), (3, 4096, 1, 1), (2, 512, 1, 1), (4, 512, 1, 1), (3, 512, 7, 1),
-                          (3, 256, 64, 1), (3, 512, 1, 32), (2, 512, 3, 32)]:
+                          (3, 256, 64, 1), (3, 512, 1, 32), (2, 512, 3, 32), (3, 512, 1, 4), (3, 512, 1, 8),
+                          (3, 512, 1, 16), (2, 512, 3, 4)]:
         h.set_tuning(v, sl, ch, tp)
         _same(h.mems_packed(flat, off, 19, 0, bounds, 128), want)
         _same(h.mems_sched_packed(flat, off, 19, 0, bounds, 128), want)
-    for bad in [(5, 512, 1, 1), (3, 100, 1, 1), (3, 512, 0, 1), (3, 512, 65, 1), (3, 512, 1, 8)]:
+    for bad in [(5, 512, 1, 1), (3, 100, 1, 1), (3, 512, 0, 1), (3, 512, 65, 1), (3, 512, 1, 2), (3, 512, 1, 12)]:
         with pytest.raises(FmIndexError):
             h.set_tuning(*bad)
 
@@ -158,3 +159,31 @@ def test_plain_launch_bit_exact(mixed_case, oracle):
         _same(h.mems_packed(sub_flat, sub_off, 19, 0, [], 8), o.mems_packed(sub_flat, sub_off, 19, 0, [], 8))
     finally:
         h.set_tuning(saved["mems_variant"], saved["seg_len"])
+
+
+@pytest.mark.parametrize("tpr", [4, 8, 16])
+def test_sub_warp_groups_bit_exact(oracle, tpr):
+    """Every read on a group of 4, 8 or 16 lanes (threads_per_read): the oracle's bytes on
+    an IUPAC reference in SMEM and MEM mode, including reads whose interval sets outgrow the
+    group's capacity (N stretches) and go on to the warp tier, and reads up to 3 kbp."""
+    ref = synth.iupac_reference(total=1_000_000, n_contigs=12, n_run_mean=60, seed=61)
+    flat, off, lens = synth.sample_mixed_reads(ref, n_reads=300, short_frac=0.8, long_median=1200, max_len=3000,
+                                               seed=62, n_rate=0.002)
+    nfl = np.concatenate([flat, np.full(6, 5, np.uint8), flat[:60]])      # a 6-N stretch: ~5k intervals
+    noff = np.concatenate([off, [off[-1] + 66]]).astype(np.uint64)
+    b = _build([al.DnaSequence(c) for c in ref.contigs], FmIndexConfig(sa_sample_rate=32, lookup_depth=8), 0,
+               KIND_BIDIR)
+    idx = BidirFmIndex.from_bytes(b)
+    h = idx.handle
+    bounds = idx.seq_boundaries()
+    o = oracle.OracleIndex(b, KIND_BIDIR)
+    saved = h.tuning()
+    h.set_tuning(3, 512, 1, tpr)
+    try:
+        _same(h.mems_packed(nfl, noff, 19, 0, bounds, 64), o.mems_packed(nfl, noff, 19, 0, bounds, 64, threads=8))
+        short = np.nonzero(lens <= 300)[0][:80]
+        sf = np.concatenate([flat[int(off[i]):int(off[i + 1])] for i in short])
+        so = np.concatenate([[0], np.cumsum(lens[short])]).astype(np.uint64)
+        _same(h.mems_packed(sf, so, 15, 1, bounds, 16), o.mems_packed(sf, so, 15, 1, bounds, 16, threads=8))
+    finally:
+        h.set_tuning(saved["mems_variant"], saved["seg_len"], saved["queue_chunk"], saved["threads_per_read"])
