@@ -930,12 +930,18 @@ def main():
     except Exception:
         peak, peak_src = FALLBACK_HBM_GBS, "fallback"
     achieved = kbytes / (kms / 1000.0) / 1e9 if kms > 0 else 0.0
-    traffic = None
+    traffic, sectors = None, {}
     tpath = os.path.join(ROOT, "profiles", "traffic_per_unit.json")
     if os.path.exists(tpath):
         tj = json.load(open(tpath))
         if dom in tj:
             traffic = tj[dom]["dram_bytes_per_unit"] * units
+            if "l1_global_sectors_per_unit" in tj[dom]:
+                # from the same ncu capture: algorithmic bytes over the 32 B sectors the
+                # kernel's global loads and stores moved, and the L2 / L1 sector hit rates
+                sectors = {"sector_efficiency": round((kbytes / units) / (32 * tj[dom]["l1_global_sectors_per_unit"]), 3),
+                           "l2_hit_rate": tj[dom]["l2_sector_hit_rate"], "l1_hit_rate": tj[dom]["l1_sector_hit_rate"],
+                           "source": tj[dom]["source"]}
     # the random-access ceiling: independent 32 B / 64 B / 96 B loads over 8 GB on every SM
     # (the access pattern of Occ records, which a streaming copy does not have)
     gather = {}
@@ -946,7 +952,7 @@ def main():
     rec_span = 32 if h.info().num_lanes <= 5 else 96      # narrow / wide Occ record
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                "random_gather_ceiling": gather, "record_bytes": rec_span,
+                "random_gather_ceiling": gather, "record_bytes": rec_span, "sectors": sectors,
                 # touches/s of the kernel (32 algorithmic bytes each) over record fetches/s of the probe
                 "frac_of_random_gather": (achieved / 32) / (gather[f"random_{rec_span}B_gbs"] / rec_span),
                 "kernel_ms": kms, "alg_bytes": kbytes, "units": units, "unit_name": unit_name,
