@@ -102,6 +102,7 @@ struct Counters {                    // device-side counters, one block per hand
 struct FmDev {
   DevFm d{};
   DevBuf occ, sb, ssa, sa_vals, lut, bounds, compat;
+  size_t nbytes[7] = {0, 0, 0, 0, 0, 0, 0};   // bytes in use of the seven buffers above, in that order
   uint32_t text_len = 0, num_seqs = 0, lookup_depth = 0, tag = 0, num_lanes = 0, encoding = 0, rate = 0, fmt = 0;
   std::vector<uint32_t> seq_boundaries;
   size_t bytes() const { return occ.cap + sb.cap + ssa.cap + sa_vals.cap + lut.cap + bounds.cap + compat.cap; }
@@ -237,15 +238,18 @@ static int build_device_fm(const HostFm& h, FmDev& f, cudaStream_t s) {
     }
     for (auto& x : th) x.join();
   }
-  RET(upload(f.occ, occ.data(), occ.size() * 4, s));
-  RET(upload(f.sb, sb.data(), sb.size() * 4, s));
-  RET(upload(f.ssa, ssa.data(), ssa.size() * 4, s));
-  RET(upload(f.sa_vals, h.sa_vals, h.n_sa_vals * 4, s));
-  RET(upload(f.bounds, h.seq_boundaries.data(), h.seq_boundaries.size() * 4, s));
-  if (h.has_lookup) RET(upload(f.lut, h.lookup_intervals, h.n_lookup * 8, s));
   uint16_t cm[16];
   compat_masks(h.tag, cm);
-  RET(upload(f.compat, cm, sizeof(cm), s));
+  const void* srcs[7] = {occ.data(), sb.data(), ssa.data(), h.sa_vals, h.has_lookup ? h.lookup_intervals : nullptr,
+                         h.seq_boundaries.data(), cm};
+  const size_t sizes[7] = {occ.size() * 4, sb.size() * 4, ssa.size() * 4, (size_t)h.n_sa_vals * 4,
+                           h.has_lookup ? (size_t)h.n_lookup * 8 : 0, h.seq_boundaries.size() * 4, sizeof(cm)};
+  DevBuf* bufs[7] = {&f.occ, &f.sb, &f.ssa, &f.sa_vals, &f.lut, &f.bounds, &f.compat};
+  for (int k = 0; k < 7; k++) {
+    if (k == 4 && !h.has_lookup) continue;
+    RET(upload(*bufs[k], srcs[k], sizes[k], s));
+    f.nbytes[k] = sizes[k];
+  }
   CK(cudaStreamSynchronize(s));      // host vectors die at return
   DevFm& d = f.d;
   d.occ = f.occ.as<uint4>(); d.sb = f.sb.as<uint32_t>(); d.ssa = f.ssa.as<uint4>();
@@ -1427,6 +1431,7 @@ static int make_shadow(hfm_index* x, hfm_index** out) {
     dst.bounds = src.bounds; dst.compat = src.compat; dst.text_len = src.text_len; dst.num_seqs = src.num_seqs;
     dst.lookup_depth = src.lookup_depth; dst.tag = src.tag; dst.num_lanes = src.num_lanes; dst.encoding = src.encoding;
     dst.rate = src.rate; dst.fmt = src.fmt; dst.seq_boundaries = src.seq_boundaries;
+    std::memcpy(dst.nbytes, src.nbytes, sizeof(dst.nbytes));
   }
   CK(cudaSetDevice(x->device));
   CK(cudaStreamCreateWithFlags(&sh->stream, cudaStreamNonBlocking));
@@ -1483,6 +1488,135 @@ int hfm_index_load(const uint8_t* bytes, size_t len, int kind, const hfm_opts* o
   RET(x->ctr.ensure(sizeof(Counters)));
   RET(build_device_fm(hf, x->fwd, x->stream));
   if (kind == HFM_KIND_BIDIR) RET(build_device_fm(hr, x->rev, x->stream));
+  *out = x.release();
+  return HFM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Device-layout blob: the handle's device records (after the transform from the bincode
+// records that hfm_index_load makes on the host), so that a later load is a read and an
+// upload.  No counterpart in the reference.  Layout, all little-endian:
+//   "HFMD" | u32 version 1 | u32 kind | u32 directions
+//   per direction: DevFm (pointers zero) | 8 x u32 FmDev scalars | u32 nbounds | nbounds x u32
+//                  | 7 x u64 buffer bytes | the 7 buffers' bytes
+// ---------------------------------------------------------------------------
+static constexpr uint32_t LAYOUT_VERSION = 1;
+
+int hfm_index_export_layout(hfm_index* x, uint8_t** bytes_out, uint64_t* len_out) {
+  if (!x || !bytes_out || !len_out) return set_error(HFM_E_ARG, "NULL argument");
+  *bytes_out = nullptr; *len_out = 0;
+  Guard g(x);
+  const int nd = x->kind == HFM_KIND_BIDIR ? 2 : 1;
+  const FmDev* dirs[2] = {&x->fwd, &x->rev};
+  uint64_t total = 16;
+  for (int k = 0; k < nd; k++) {
+    total += sizeof(DevFm) + 8 * 4 + 4 + dirs[k]->seq_boundaries.size() * 4 + 7 * 8;
+    for (size_t b : dirs[k]->nbytes) total += b;
+  }
+  uint8_t* out = (uint8_t*)std::malloc(total);
+  if (!out) return set_error(HFM_E_OOM, "host allocation failed");
+  uint8_t* w = out;
+  auto put = [&](const void* src, size_t n) { std::memcpy(w, src, n); w += n; };
+  const uint32_t hdr[4] = {0x444D4648u, LAYOUT_VERSION, (uint32_t)x->kind, (uint32_t)nd};
+  put(hdr, 16);
+  for (int k = 0; k < nd; k++) {
+    const FmDev& f = *dirs[k];
+    DevFm d = f.d;
+    d.occ = nullptr; d.sb = nullptr; d.ssa = nullptr; d.sa_vals = nullptr; d.lut = nullptr; d.seq_bounds = nullptr;
+    put(&d, sizeof(d));
+    const uint32_t sc[8] = {f.text_len, f.num_seqs, f.lookup_depth, f.tag, f.num_lanes, f.encoding, f.rate, f.fmt};
+    put(sc, 32);
+    const uint32_t nbnd = (uint32_t)f.seq_boundaries.size();
+    put(&nbnd, 4);
+    put(f.seq_boundaries.data(), (size_t)nbnd * 4);
+    put(f.nbytes, 7 * 8);
+    const DevBuf* bufs[7] = {&f.occ, &f.sb, &f.ssa, &f.sa_vals, &f.lut, &f.bounds, &f.compat};
+    for (int b = 0; b < 7; b++) {
+      if (f.nbytes[b]) {
+        cudaError_t e = cudaMemcpy(w, bufs[b]->p, f.nbytes[b], cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) { std::free(out); cudaGetLastError(); return set_error(HFM_E_CUDA, "layout copy failed"); }
+      }
+      w += f.nbytes[b];
+    }
+  }
+  *bytes_out = out; *len_out = total;
+  return HFM_OK;
+}
+
+int hfm_index_load_layout(const uint8_t* bytes, uint64_t len, const hfm_opts* opts, hfm_index** out) {
+  if (!bytes || !out) return set_error(HFM_E_ARG, "NULL argument");
+  *out = nullptr;
+  // validate every length against the blob before any device work
+  uint64_t r = 0;
+  auto need = [&](uint64_t n) { return n <= len && r <= len - n; };
+  if (!need(16)) return set_error(HFM_E_FORMAT, "truncated layout header");
+  uint32_t hdr[4];
+  std::memcpy(hdr, bytes, 16); r = 16;
+  if (hdr[0] != 0x444D4648u) return set_error(HFM_E_FORMAT, "not a device-layout blob (magic)");
+  if (hdr[1] != LAYOUT_VERSION) return set_error(HFM_E_FORMAT, "unsupported device-layout version");
+  const int kind = (int)hdr[2];
+  if ((kind != HFM_KIND_FM && kind != HFM_KIND_BIDIR) || hdr[3] != (kind == HFM_KIND_BIDIR ? 2u : 1u))
+    return set_error(HFM_E_FORMAT, "bad kind or direction count");
+  struct Dir { DevFm d; uint32_t sc[8]; std::vector<uint32_t> bnd; uint64_t nb[7]; uint64_t at[7]; };
+  Dir dirs[2];
+  for (uint32_t k = 0; k < hdr[3]; k++) {
+    Dir& D = dirs[k];
+    if (!need(sizeof(DevFm) + 36)) return set_error(HFM_E_FORMAT, "truncated direction header");
+    std::memcpy(&D.d, bytes + r, sizeof(DevFm)); r += sizeof(DevFm);
+    std::memcpy(D.sc, bytes + r, 32); r += 32;
+    uint32_t nbnd; std::memcpy(&nbnd, bytes + r, 4); r += 4;
+    if (!need((uint64_t)nbnd * 4 + 56)) return set_error(HFM_E_FORMAT, "truncated sequence bounds");
+    D.bnd.resize(nbnd);
+    std::memcpy(D.bnd.data(), bytes + r, (size_t)nbnd * 4); r += (uint64_t)nbnd * 4;
+    std::memcpy(D.nb, bytes + r, 56); r += 56;
+    const uint64_t nblk = ((uint64_t)D.d.text_len + 63) / 64;
+    const uint64_t rec = D.d.fmt == OCC_NARROW ? OCC_NARROW_U4 * 16 : OCC_WIDE_U4 * 16;
+    if (D.d.fmt > OCC_NARROW || D.nb[0] != nblk * rec || D.nb[2] != nblk * 16 || D.d.num_blocks != nblk ||
+        D.nb[5] != (uint64_t)nbnd * 4 || D.nb[6] != 32 || D.sc[0] != D.d.text_len || D.sc[7] != D.d.fmt ||
+        D.nb[1] != ((nblk + (1u << SB_BLOCK_SHIFT) - 1) >> SB_BLOCK_SHIFT) * 64 ||
+        (D.nb[4] != 0) != (D.d.lut_depth != 0) || D.nb[3] % 4 || D.nb[4] % 8)
+      return set_error(HFM_E_FORMAT, "device-layout sizes inconsistent with the text length");
+    for (int b = 0; b < 7; b++) {
+      if (!need(D.nb[b])) return set_error(HFM_E_FORMAT, "truncated device buffer");
+      D.at[b] = r; r += D.nb[b];
+    }
+  }
+  if (r != len) return set_error(HFM_E_FORMAT, "trailing bytes after the device layout");
+  if (kind == HFM_KIND_BIDIR && dirs[0].d.text_len != dirs[1].d.text_len)
+    return set_error(HFM_E_FORMAT, "forward and reverse text lengths differ");
+  int dev = opts ? opts->device : 0;
+  int ndev = 0;
+  CK(cudaGetDeviceCount(&ndev));
+  if (dev < 0 || dev >= ndev) return set_error(HFM_E_ARG, "device ordinal out of range");
+  CK(cudaSetDevice(dev));
+  std::unique_ptr<hfm_index> x(new hfm_index());
+  x->device = dev; x->kind = kind; x->flags = opts ? opts->flags : 0;
+  CK(cudaDeviceGetAttribute(&x->num_sms, cudaDevAttrMultiProcessorCount, dev));
+  CK(cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking));
+  for (auto& e : x->ev) CK(cudaEventCreate(&e));
+  for (auto& e : x->evk) CK(cudaEventCreate(&e));
+  CK(cudaEventCreateWithFlags(&x->ev_wait, cudaEventDisableTiming));
+  CK(cudaMallocHost((void**)&x->h_ctr, sizeof(Counters)));
+  RET(x->ctr.ensure(sizeof(Counters)));
+  FmDev* fs[2] = {&x->fwd, &x->rev};
+  for (uint32_t k = 0; k < hdr[3]; k++) {
+    Dir& D = dirs[k];
+    FmDev& f = *fs[k];
+    DevBuf* bufs[7] = {&f.occ, &f.sb, &f.ssa, &f.sa_vals, &f.lut, &f.bounds, &f.compat};
+    for (int b = 0; b < 7; b++) {
+      if (!D.nb[b]) continue;
+      RET(upload(*bufs[b], bytes + D.at[b], D.nb[b], x->stream));
+      f.nbytes[b] = D.nb[b];
+    }
+    f.d = D.d;
+    f.d.occ = f.occ.as<uint4>(); f.d.sb = f.sb.as<uint32_t>(); f.d.ssa = f.ssa.as<uint4>();
+    f.d.sa_vals = f.sa_vals.as<uint32_t>(); f.d.seq_bounds = f.bounds.as<uint32_t>();
+    f.d.lut = D.nb[4] ? f.lut.as<uint2>() : nullptr;
+    f.text_len = D.sc[0]; f.num_seqs = D.sc[1]; f.lookup_depth = D.sc[2]; f.tag = D.sc[3];
+    f.num_lanes = D.sc[4]; f.encoding = D.sc[5]; f.rate = D.sc[6]; f.fmt = D.sc[7];
+    f.seq_boundaries = D.bnd;
+  }
+  CK(cudaStreamSynchronize(x->stream));
   *out = x.release();
   return HFM_OK;
 }

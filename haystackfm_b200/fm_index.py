@@ -139,6 +139,29 @@ class _Handle:
             self.h = None
         self._src = None
 
+    def export_layout(self) -> bytes:
+        """hfm_index_export_layout: the device records of this index as one blob."""
+        out = L.u8p()
+        n = C.c_uint64()
+        L.check(L.lib().hfm_index_export_layout(self.h, C.byref(out), C.byref(n)))
+        try:
+            return _take_bytes(out, n.value)
+        finally:
+            L.lib().hfm_free(out)
+
+    @classmethod
+    def from_layout(cls, blob: bytes, device: int = 0, flags: int = 0) -> "_Handle":
+        """hfm_index_load_layout: a handle from a blob of export_layout, without the host
+        transform of the bincode records."""
+        o = cls.__new__(cls)
+        o._buf = np.frombuffer(blob, dtype=np.uint8)
+        h = C.c_void_p()
+        opts = L.HfmOpts(device, flags)
+        L.check(L.lib().hfm_index_load_layout(L.ptr(o._buf, L.u8p), len(blob), C.byref(opts), C.byref(h)))
+        o.h, o.device, o._src = h, device, None
+        o.kind = int(np.frombuffer(blob[8:12], dtype="<u4")[0])
+        return o
+
     def share(self) -> "_Handle":
         """hfm_index_share: another handle on this index (own stream and work buffers)."""
         o = _Handle.__new__(_Handle)

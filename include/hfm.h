@@ -133,6 +133,15 @@ int hfm_build_index_gpu(const uint8_t* codes, const uint64_t* seq_off, uint32_t 
  *      per-call uploads of src/gpu/locate.rs:69-111, src/gpu/mem_find.rs:56-102,
  *      src/gpu/mem_resolve.rs:44-85) ---------------------------------------- */
 int hfm_index_load(const uint8_t* bincode, size_t len, int kind, const hfm_opts* opts, hfm_index** out);
+/* Device-layout blob (no counterpart in the reference): hfm_index_export_layout writes the
+ * handle's device records — after the transform from the bincode records that
+ * hfm_index_load makes on the host — to one malloc'd block (*bytes_out, released with
+ * hfm_free); hfm_index_load_layout uploads such a block as it is, so a repeated load of a
+ * genome-scale index is a read and a copy.  Every length is checked against the text
+ * length and the blob size before any device work (HFM_E_FORMAT).  The blob is specific
+ * to this library's version and is not the reference's bincode. */
+int hfm_index_export_layout(hfm_index* idx, uint8_t** bytes_out, uint64_t* len_out);
+int hfm_index_load_layout(const uint8_t* bytes, uint64_t len, const hfm_opts* opts, hfm_index** out);
 void hfm_index_free(hfm_index* idx);
 int hfm_index_info_get(const hfm_index* idx, hfm_index_info* out);
 /* A second handle on the same device-resident index, with its own stream and work buffers

@@ -165,3 +165,28 @@ def test_graph_and_probe_arguments_rejected_without_a_gpu():
     assert b"span" in lib.hfm_last_error()
     assert lib.hfm_probe_gather(0, 1 << 20, 32, C.byref(gbs), None) == HFM_E_ARG
     assert lib.hfm_probe_gather(0, 1 << 30, 32, None, None) == HFM_E_ARG
+
+
+def test_malformed_layout_blob_rejected_before_device_work():
+    """hfm_index_load_layout checks magic, version, kind and every length against the blob
+    before it touches a device: all of these fail with HFM_E_FORMAT on a machine without a
+    GPU."""
+    import ctypes as C
+    from haystackfm_b200.errors import HFM_E_FORMAT
+    lib = L.lib()
+    h = C.c_void_p()
+
+    def load(blob):
+        buf = np.frombuffer(blob, dtype=np.uint8) if blob else np.zeros(1, np.uint8)
+        return lib.hfm_index_load_layout(L.ptr(buf, L.u8p), len(blob), None, C.byref(h))
+    hdr = np.array([0x444D4648, 1, 1, 2], dtype="<u4").tobytes()
+    assert load(b"") == HFM_E_FORMAT
+    assert load(b"HFMD") == HFM_E_FORMAT                                   # truncated header
+    assert load(np.array([0x12345678, 1, 1, 2], dtype="<u4").tobytes()) == HFM_E_FORMAT   # magic
+    assert load(np.array([0x444D4648, 9, 1, 2], dtype="<u4").tobytes()) == HFM_E_FORMAT   # version
+    assert load(np.array([0x444D4648, 1, 1, 1], dtype="<u4").tobytes()) == HFM_E_FORMAT   # bidir needs 2
+    assert load(hdr) == HFM_E_FORMAT                                       # no direction records
+    assert load(hdr + bytes(200)) == HFM_E_FORMAT                          # truncated direction
+    assert b"truncated" in lib.hfm_last_error()
+    assert load(hdr + bytes(400)) == HFM_E_FORMAT                          # sizes inconsistent
+    assert b"inconsistent" in lib.hfm_last_error()

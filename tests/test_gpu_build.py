@@ -69,3 +69,31 @@ def test_random_gather_probe_rates():
         assert 0 < gbs.value < 1e5 and ms.value > 0
         rates[span] = gbs.value
     assert rates[64] > rates[32] * 0.8 and rates[96] > rates[32] * 0.8
+
+
+def test_layout_blob_round_trip(oracle):
+    """The device-layout blob: a handle loaded from it answers exactly as the one loaded
+    from the bincode (and as the oracle), for both record formats, and exporting it again
+    gives the same blob."""
+    from haystackfm_b200.fm_index import BidirFmIndex, _Handle
+    for tag, ref in ((0, synth.iupac_reference(total=300_000, n_contigs=6, seed=101)),
+                     (1, synth.repeat_reference(total=300_000, n_contigs=3, seed=102))):
+        data = _build([al.DnaSequence(c) for c in ref.contigs], FmIndexConfig(sa_sample_rate=16, lookup_depth=8), tag,
+                      KIND_BIDIR)
+        idx = BidirFmIndex.from_bytes(data)
+        blob = idx.handle.export_layout()
+        h2 = _Handle.from_layout(blob)
+        assert h2.export_layout() == blob
+        reads = synth.sample_reads(ref, n_reads=500, seed=103)
+        flat, off = synth.pack_rows(reads)
+        bounds = idx.seq_boundaries()
+        want = oracle.OracleIndex(data, KIND_BIDIR).mems_packed(flat, off, 19, 0, bounds, 64, threads=8)
+        for hh in (idx.handle, h2):
+            got = hh.mems_packed(flat, off, 19, 0, bounds, 64)
+            for g, w in zip(got, want):
+                assert np.array_equal(g, w)
+        k32, o32 = synth.pack_rows(reads, 32)
+        a = idx.handle.locate_packed(k32, o32, 100)
+        b = h2.locate_packed(k32, o32, 100)
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
