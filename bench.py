@@ -285,6 +285,18 @@ def device_mems_tensors(torch, dev, dm, n, clone):
             view(dm.d_positions, 2 * dm.n_positions, "<i4"))
 
 
+def device_hits_tensors(torch, dev, dh):
+    """Views of a locate result's device arrays (counts, offsets, pairs) as torch tensors."""
+    from haystackfm_b200.fm_index import _DeviceArray
+    n = dh.nq
+
+    def view(ptr, k, ts):
+        if k == 0:
+            return torch.zeros(0, dtype=torch.int32, device=dev)
+        return torch.as_tensor(_DeviceArray(int(ptr), int(k), ts), device=dev)
+    return (view(dh.d_counts, n, "<i4"), view(dh.d_offsets, n + 1, "<i8"), view(dh.d_pairs, 2 * dh.total, "<i4"))
+
+
 def compare_outputs(got, want):
     """Byte comparison of (locate, mems) output tuples; -> list of differing arrays."""
     names = [("locate", ("counts", "offsets", "pairs")), ("mems", ("hit_offsets", "hits", "positions"))]
@@ -865,6 +877,7 @@ def main():
         learned_parity = {"reads_checked": n, "equal": eq, "mem_hits": int(dm_l.n_hits),
                           "mem_positions": int(dm_l.n_positions)}
         del snap, now
+        torch.cuda.empty_cache()      # the 24 GB snapshot back to the device, for the library's pools
     # the CUDA-graph-captured SMEM chain against the adaptive chain on the same batch
     # (host clock around each call: both include their waits for the device)
     graph_info = None
@@ -872,6 +885,9 @@ def main():
         g = C.c_void_p()
         L.check(lib.hfm_mems_graph_create(h.h, reads_d.data_ptr(), off_d.data_ptr(), n, n * 150, 19, 0,
                                           L.ptr(bounds, L.u32p), nb, 1024, int(n_pos * 1.25) + 4096, C.byref(g)))
+        # the locate of the 32-mers ahead of it in the same graph: one replay = one step
+        L.check(lib.hfm_mems_graph_add_locate(g, k32_d.data_ptr(), off32_d.data_ptr(), n, 1024, 0,
+                                              int(loc_total * 1.25) + 4096))
         rep = C.c_uint32()
         dmg = L.HfmDevMems()
 
@@ -887,6 +903,8 @@ def main():
             L.check(lib.hfm_mems_graph_launch(g, C.byref(dmg), C.byref(rep)))
 
         def adapt():
+            dh = L.HfmDevHits()
+            L.check(lib.hfm_locate_batch_device(h.h, k32_d.data_ptr(), off32_d.data_ptr(), n, 1024, C.byref(dh)))
             dm = L.HfmDevMems()
             L.check(lib.hfm_mems_batch_device(h.h, reads_d.data_ptr(), off_d.data_ptr(), n, 19, 0,
                                               L.ptr(bounds, L.u32p), nb, 1024, C.byref(dm)))
@@ -895,18 +913,30 @@ def main():
         g_ms = host_ms(glaunch, args.steps)
         replayed = int(rep.value)
         a_ms = host_ms(adapt, args.steps)
+        glaunch()
+        replayed = replayed and int(rep.value)
         snap = device_mems_tensors(torch, dev, dmg, n, clone=True)
+        lr = L.HfmDevHits()
+        L.check(lib.hfm_mems_graph_locate_result(g, C.byref(lr)))
+        lsnap = [x.clone() for x in device_hits_tensors(torch, dev, lr)]
+        dh_a = L.HfmDevHits()
+        L.check(lib.hfm_locate_batch_device(h.h, k32_d.data_ptr(), off32_d.data_ptr(), n, 1024, C.byref(dh_a)))
+        lnow = device_hits_tensors(torch, dev, dh_a)
+        leq = all(a.shape == b.shape and bool(torch.equal(a, b)) for a, b in zip(lsnap, lnow))
         dm_a = L.HfmDevMems()
         L.check(lib.hfm_mems_batch_device(h.h, reads_d.data_ptr(), off_d.data_ptr(), n, 19, 0, L.ptr(bounds, L.u32p),
                                           nb, 1024, C.byref(dm_a)))
         now = device_mems_tensors(torch, dev, dm_a, n, clone=False)
-        geq = all(a.shape == b.shape and bool(torch.equal(a, b)) for a, b in zip(snap, now))
-        del snap, now
+        geq = leq and all(a.shape == b.shape and bool(torch.equal(a, b)) for a, b in zip(snap, now))
+        del snap, now, lsnap, lnow
         lib.hfm_mems_graph_free(g)
+        torch.cuda.empty_cache()
         graph_info = {"graph_ms": round(g_ms, 3), "adaptive_ms": round(a_ms, 3), "speedup": round(a_ms / g_ms, 4),
                       "last_launch_replayed": replayed, "outputs_equal": geq,
-                      "what": "find_smems of the batch: one CUDA graph replay of the fixed-capacity chain "
-                              "(hfm_mems_graph_launch) vs hfm_mems_batch_device; host clock per call"}
+                      "what": "the headline step (locate of the 32-mers + find_smems of the batch): one CUDA graph "
+                              "replay of the fixed-capacity chains (hfm_mems_graph_add_locate + "
+                              "hfm_mems_graph_launch) vs hfm_locate_batch_device + hfm_mems_batch_device; host clock "
+                              "per call; every output array compared"}
     # kernel times (CUDA events around each launch, recorded by the library on its stream)
     k_mems_ms = statistics.mean(s2.ms_search_kernel for _, s2, *_ in per)
     k_res_mem_ms = statistics.mean(s2.ms_resolve_kernel for _, s2, *_ in per)

@@ -200,8 +200,13 @@ __global__ void __launch_bounds__(EXP_T) k_dedup_expand(const uint64_t* __restri
     if (p >= p1) return;
     uint64_t src;
     if (local) {
-      uint32_t hi = cnt - 1;
-      while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (s_off[mid] <= p) lo = mid; else hi = mid - 1; }
+      // still in the previous position's segment (the usual case for segments of more than
+      // EXP_T positions), else a binary search over the rest
+      if (lo + 1 < cnt && s_off[lo + 1] <= p) {
+        uint32_t hi = cnt - 1;
+        lo++;
+        while (lo < hi) { uint32_t mid = (lo + hi + 1) >> 1; if (s_off[mid] <= p) lo = mid; else hi = mid - 1; }
+      }
       src = s_src[lo] + (p - s_off[lo]);
     } else {
       uint32_t l = first, hi = nseg - 1;
