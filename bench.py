@@ -742,6 +742,17 @@ def main():
     off32_d = torch.arange(0, (n + 1) * 32, 32, dtype=torch.int64, device=dev)
     torch.cuda.synchronize()
     stream = torch.cuda.ExternalStream(h.stream(), device=dev)
+    memory = []
+
+    def mem_mark(label):
+        """Device memory after a phase: free, held by this handle, reserved by torch (GB)."""
+        free_b, _ = torch.cuda.mem_get_info(dev)
+        db = h.device_bytes()
+        memory.append({"after": label, "free_gb": round(free_b / 1e9, 1), "handle_work_gb": round(db["work"] / 1e9, 1),
+                       "handle_index_gb": round(db["index"] / 1e9, 2),
+                       "torch_reserved_gb": round(torch.cuda.memory_reserved(dev) / 1e9, 1)})
+        print("[bench] memory", json.dumps(memory[-1]), file=sys.stderr, flush=True)
+    mem_mark("index load")
 
     # learned cost model: trained on the logged work of a separate seeded read sample
     learned, learned_info, tuning_main = None, None, None
@@ -783,6 +794,7 @@ def main():
         if stats_out is not None:
             stats_out.append((s1, s2, dh.total, dm.n_hits, dm.n_positions, extra))
 
+    mem_mark("autotune + learned fit")
     # work counters (one untimed pass): algorithmic bytes per launch
     h.set_counters(True)
     cnt = []
@@ -816,6 +828,7 @@ def main():
     launches = sum(s1.search_launches + s1.resolve_launches + s1.other_launches + s2.search_launches +
                    s2.resolve_launches + s2.other_launches + p[5] for p in per for s1, s2 in [p[:2]])
 
+    mem_mark("timed steps")
     # the plain order, same loop (the learned path's fallback and judge)
     plain_info = None
     if learned is not None:
@@ -864,6 +877,7 @@ def main():
                         "value_speedup": round(lms / ms, 4),
                         "what": "locate + find_smems with the SMEM search as one thread per read over a grid of the "
                                 "batch, local-memory sets, count pass + host-read totals + write pass"}
+    mem_mark("plain launch")
     # learned order vs plain order on the whole batch: every output array byte for byte
     learned_parity = None
     if learned is not None:
@@ -878,6 +892,7 @@ def main():
                           "mem_positions": int(dm_l.n_positions)}
         del snap, now
         torch.cuda.empty_cache()      # the 24 GB snapshot back to the device, for the library's pools
+    mem_mark("learned vs plain comparison")
     # the CUDA-graph-captured SMEM chain against the adaptive chain on the same batch
     # (host clock around each call: both include their waits for the device)
     graph_info = None
@@ -937,6 +952,7 @@ def main():
                               "replay of the fixed-capacity chains (hfm_mems_graph_add_locate + "
                               "hfm_mems_graph_launch) vs hfm_locate_batch_device + hfm_mems_batch_device; host clock "
                               "per call; every output array compared"}
+    mem_mark("graph")
     # kernel times (CUDA events around each launch, recorded by the library on its stream)
     k_mems_ms = statistics.mean(s2.ms_search_kernel for _, s2, *_ in per)
     k_res_mem_ms = statistics.mean(s2.ms_resolve_kernel for _, s2, *_ in per)
@@ -999,6 +1015,7 @@ def main():
                 "kernels_ms": {k: v[0] for k, v in kern.items()},
                 "kernels_gbs": {k: (v[1] / (v[0] / 1000) / 1e9 if v[0] > 0 else None) for k, v in kern.items()}}
 
+    mem_mark("roofline")
     # end to end through the host-buffer C ABI (pinned reads in, every result out)
     reads_pin = torch.empty(n * 150, dtype=torch.uint8, pin_memory=True)
     reads_pin.numpy()[:] = reads.reshape(-1)
@@ -1133,7 +1150,7 @@ def main():
                     "distinct_rows_walked": int(rows_walked(c_mem) + rows_walked(c_loc)),
                     "autotuned": tuning_main},
             "parity": parity,
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "memory": memory,
             "plain": plain_info, "plain_launch": plain_launch, "graph": graph_info, "learned": learned_info,
             "serving": serving,
             "genome": genome,

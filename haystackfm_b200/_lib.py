@@ -95,6 +95,7 @@ SIGNATURES = {
     "hfm_build_index_gpu": (C.c_int, [u8p, u64p, C.c_uint32, C.POINTER(C.c_char_p), C.POINTER(HfmBuildOpts),
                                       C.c_int, C.c_int, C.POINTER(u8p), C.POINTER(C.c_size_t)]),
     "hfm_index_load": (C.c_int, [u8p, C.c_size_t, C.c_int, C.POINTER(HfmOpts), C.POINTER(C.c_void_p)]),
+    "hfm_index_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "hfm_index_export_layout": (C.c_int, [C.c_void_p, C.POINTER(u8p), C.POINTER(C.c_uint64)]),
     "hfm_index_load_layout": (C.c_int, [u8p, C.c_uint64, C.POINTER(HfmOpts), C.POINTER(C.c_void_p)]),
     "hfm_index_free": (None, [C.c_void_p]),

@@ -1621,6 +1621,27 @@ int hfm_index_load_layout(const uint8_t* bytes, uint64_t len, const hfm_opts* op
   return HFM_OK;
 }
 
+int hfm_index_device_bytes(const hfm_index* x, uint64_t* index_bytes, uint64_t* work_bytes) {
+  if (!x) return set_error(HFM_E_ARG, "NULL argument");
+  const DevBuf* idx_bufs[] = {&x->fwd.occ, &x->fwd.sb, &x->fwd.ssa, &x->fwd.sa_vals, &x->fwd.lut, &x->fwd.bounds,
+                              &x->fwd.compat, &x->rev.occ, &x->rev.sb, &x->rev.ssa, &x->rev.sa_vals, &x->rev.lut,
+                              &x->rev.bounds, &x->rev.compat};
+  const DevBuf* work_bufs[] = {
+      &x->q, &x->qoff, &x->counts, &x->nhits, &x->niv, &x->ivoff, &x->status, &x->ovf, &x->ivpool, &x->hitpool,
+      &x->seg_row, &x->seg_off, &x->pos_base, &x->seg_base, &x->scan_tmp, &x->out_pairs, &x->ref_bounds,
+      &x->hit_start, &x->hit_count, &x->hit_base, &x->hits, &x->npos_scan, &x->work, &x->cwork, &x->ctr,
+      &x->mivpool, &x->bswork, &x->memwork, &x->hkeys, &x->hslot, &x->hflags, &x->huid, &x->urow, &x->ulen,
+      &x->uoff, &x->uout, &x->blockmap, &x->blockmap2, &x->ovf2, &x->ovf3, &x->lflag, &x->lpos, &x->sids,
+      &x->lids, &x->ucount, &x->ubase, &x->uread, &x->uk, &x->ubits, &x->uexit, &x->ust, &x->ucoff, &x->ucnt,
+      &x->segpool, &x->fxe, &x->fxc, &x->fxx, &x->fxo, &x->fxn, &x->npos, &x->iota, &x->loc_pairs};
+  uint64_t a = 0, b = 0;
+  if (!x->shared_index) for (const DevBuf* d : idx_bufs) a += d->cap;
+  for (const DevBuf* d : work_bufs) b += d->cap;
+  if (index_bytes) *index_bytes = a;
+  if (work_bytes) *work_bytes = b;
+  return HFM_OK;
+}
+
 void hfm_index_free(hfm_index* x) {
   if (!x) return;
   cudaSetDevice(x->device);

@@ -139,6 +139,12 @@ class _Handle:
             self.h = None
         self._src = None
 
+    def device_bytes(self) -> dict:
+        """hfm_index_device_bytes: {"index": bytes of the layout, "work": work areas and results}."""
+        a, b = C.c_uint64(), C.c_uint64()
+        L.check(L.lib().hfm_index_device_bytes(self.h, C.byref(a), C.byref(b)))
+        return {"index": a.value, "work": b.value}
+
     def export_layout(self) -> bytes:
         """hfm_index_export_layout: the device records of this index as one blob."""
         out = L.u8p()

@@ -143,6 +143,10 @@ int hfm_index_load(const uint8_t* bincode, size_t len, int kind, const hfm_opts*
 int hfm_index_export_layout(hfm_index* idx, uint8_t** bytes_out, uint64_t* len_out);
 int hfm_index_load_layout(const uint8_t* bytes, uint64_t len, const hfm_opts* opts, hfm_index** out);
 void hfm_index_free(hfm_index* idx);
+/* Device bytes a handle holds: its index layout (0 for a share) and its grow-only work
+ * areas, pools and result arrays (reused across calls; freed with the handle).  For
+ * budgeting HBM between handles; no counterpart in the reference. */
+int hfm_index_device_bytes(const hfm_index* idx, uint64_t* index_bytes, uint64_t* work_bytes);
 int hfm_index_info_get(const hfm_index* idx, hfm_index_info* out);
 /* A second handle on the same device-resident index, with its own stream and work buffers
  * (no counterpart in the reference, whose process-wide context serialises every call,
