@@ -79,7 +79,7 @@ struct DevBuf {
     if (bytes <= cap) return HFM_OK;
     if (p) cudaFree(p);
     p = nullptr; cap = 0;
-    size_t want = std::max<size_t>(bytes + bytes / 4, 256);
+    size_t want = std::max<size_t>(bytes + std::min<size_t>(bytes / 4, 256ull << 20), 256);   // growth slack
     cudaError_t e = cudaMalloc(&p, want);
     if (e != cudaSuccess) {
       cudaGetLastError();
@@ -974,10 +974,11 @@ struct GraphTotals { uint64_t nh, npos, upos; uint32_t ovf, _pad; };
 // Totals of the chain: MemHits, and the position counts the resolve passes cover, both 0
 // (with ovf set) when a count exceeds the position capacity.
 __global__ void k_graph_totals(const uint64_t* __restrict__ hit_base, uint32_t nq, const uint64_t* __restrict__ pos_total,
-                               const uint64_t* __restrict__ u_total, uint64_t pos_cap, GraphTotals* __restrict__ t) {
+                               const uint64_t* __restrict__ u_total, uint64_t pos_cap, uint64_t upos_cap,
+                               GraphTotals* __restrict__ t) {
   if (blockIdx.x || threadIdx.x) return;
   const uint64_t np = *pos_total, nu = u_total ? *u_total : 0;
-  const bool over = np > pos_cap || nu > pos_cap;
+  const bool over = np > pos_cap || nu > upos_cap;
   t->nh = hit_base[nq];
   t->npos = over ? 0 : np;
   t->upos = over ? 0 : nu;
@@ -990,6 +991,7 @@ struct FixedChain {
   MemsParams P; uint32_t nb;   // ref bounds already in x->ref_bounds
   bool dedup;
   uint64_t pos_cap;
+  uint64_t upos_cap;           // distinct positions (rows walked once by the deduplicated resolve)
   GraphTotals* d_tot; GraphTotals* h_tot;     // device / pinned host
   uint64_t threads;            // resident threads of the persistent kernels
   uint32_t warp_cap = MEM_WARP_SET_CAP, warp_cands = 1024;   // warp tier: intervals per set, candidates
@@ -1007,7 +1009,7 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
     }
     return scan(x, in, stride, n, out, dummy);
   };
-  const uint64_t hcap = x->hit_cap, pcap = c.pos_cap;
+  const uint64_t hcap = x->hit_cap, pcap = c.pos_cap, upcap = std::min(c.upos_cap, c.pos_cap);
   if (hcap >= 0xFFFFFFFFull) return set_error(HFM_E_ARG, "MemHit capacity above 2^32");
   // work buffers
   RET(x->hit_start.ensure((size_t)nq * 8 + 8)); RET(x->hit_count.ensure((size_t)nq * 4 + 4));
@@ -1054,7 +1056,7 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
     RET(x->hkeys.ensure(hsize * 8)); RET(x->hslot.ensure(hcap * 4 + 4));
     RET(x->hflags.ensure(hsize * 4)); RET(x->huid.ensure((hsize + 1) * 8));
     RET(x->urow.ensure(hcap * 4 + 4)); RET(x->ulen.ensure(hcap * 4 + 4)); RET(x->uoff.ensure((hcap + 1) * 8));
-    RET(x->uout.ensure(pcap * 8 + 8));
+    RET(x->uout.ensure(upcap * 8 + 8));
     RET(x->blockmap2.ensure(eblocks * 4 + 4));
   }
   const MemsParams& P = c.P;
@@ -1178,12 +1180,13 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
     RET(SCAN(x->ulen.as<uint32_t>(), 1, hcap, x->uoff.as<uint64_t>()));     // uoff[hcap] = distinct positions
     if (launch) {
       k_graph_totals<<<1, 32, 0, x->stream>>>(x->hit_base.as<uint64_t>(), nq, seg_off + hcap,
-                                              x->uoff.as<uint64_t>() + hcap, pcap, c.d_tot);
+                                              x->uoff.as<uint64_t>() + hcap, pcap, upcap, c.d_tot);
       k_block_first<<<(unsigned)((hcap + 255) / 256), 256, 0, x->stream>>>(x->uoff.as<uint64_t>(), (uint32_t)hcap, RES_T,
-                                                                          x->blockmap.as<uint32_t>(), rblocks);
-      ResolveArgs A{x->urow.as<uint32_t>(), 1, x->uoff.as<uint64_t>(), (uint32_t)hcap, pcap, d_bounds, c.nb, guard,
+                                                                          x->blockmap.as<uint32_t>(),
+                                                                          (upcap + RES_T - 1) / RES_T);
+      ResolveArgs A{x->urow.as<uint32_t>(), 1, x->uoff.as<uint64_t>(), (uint32_t)hcap, upcap, d_bounds, c.nb, guard,
                     x->uout.as<uint32_t>(), &dc->walk_err, &dc->steps, x->blockmap.as<uint32_t>(), &c.d_tot->upos};
-      k_resolve<false><<<(unsigned)((pcap + RES_T - 1) / RES_T), RES_T, 0, x->stream>>>(Fw.d, A);
+      k_resolve<false><<<(unsigned)((upcap + RES_T - 1) / RES_T), RES_T, 0, x->stream>>>(Fw.d, A);
       k_block_first<<<(unsigned)((hcap + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)hcap, EXP_BLK,
                                                                           x->blockmap2.as<uint32_t>(), eblocks);
       k_dedup_expand<<<(unsigned)((pcap + EXP_BLK - 1) / EXP_BLK), EXP_T, 0, x->stream>>>(
@@ -1192,7 +1195,8 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
       CK(cudaGetLastError());
     }
   } else if (launch) {
-    k_graph_totals<<<1, 32, 0, x->stream>>>(x->hit_base.as<uint64_t>(), nq, seg_off + hcap, nullptr, pcap, c.d_tot);
+    k_graph_totals<<<1, 32, 0, x->stream>>>(x->hit_base.as<uint64_t>(), nq, seg_off + hcap, nullptr, pcap, pcap,
+                                            c.d_tot);
     k_block_first<<<(unsigned)((hcap + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)hcap, RES_T,
                                                                         x->blockmap.as<uint32_t>(), rblocks);
     ResolveArgs A{seg_row, 8, seg_off, (uint32_t)hcap, pcap, d_bounds, c.nb, guard, x->out_pairs.as<uint32_t>(),
@@ -1213,7 +1217,7 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
 // captured graph.
 struct FixedLocate {
   const uint8_t* d_q; const uint64_t* d_qoff; uint32_t nq; uint32_t max_hits;
-  uint64_t iv_cap, pos_cap;
+  uint64_t iv_cap, pos_cap, upos_cap;
   uint32_t warp_cap = BS_WARP_SET_CAP;
   bool dedup;
   uint64_t threads;
@@ -1233,7 +1237,7 @@ static int fixed_locate(hfm_index* x, FixedLocate& c, bool launch) {
     }
     return scan(x, in, stride, n, out, dummy);
   };
-  const uint64_t icap = c.iv_cap, pcap = c.pos_cap;
+  const uint64_t icap = c.iv_cap, pcap = c.pos_cap, upcap = std::min(c.upos_cap, c.pos_cap);
   if (icap >= 0xFFFFFFFFull) return set_error(HFM_E_ARG, "interval capacity above 2^32");
   RET(x->counts.ensure((size_t)nq * 4 + 4)); RET(x->nhits.ensure((size_t)nq * 8 + 8));
   RET(x->niv.ensure((size_t)nq * 4 + 4)); RET(x->ivoff.ensure((size_t)nq * 8 + 8));
@@ -1260,7 +1264,7 @@ static int fixed_locate(hfm_index* x, FixedLocate& c, bool launch) {
     RET(x->hkeys.ensure(hsize * 8)); RET(x->hslot.ensure(icap * 4 + 4));
     RET(x->hflags.ensure(hsize * 4)); RET(x->huid.ensure((hsize + 1) * 8));
     RET(x->urow.ensure(icap * 4 + 4)); RET(x->ulen.ensure(icap * 4 + 4)); RET(x->uoff.ensure((icap + 1) * 8));
-    RET(x->uout.ensure(pcap * 8 + 8));
+    RET(x->uout.ensure(upcap * 8 + 8));
     RET(x->blockmap2.ensure(eblocks * 4 + 4));
   }
   Counters* dc = c.ctr;
@@ -1317,12 +1321,13 @@ static int fixed_locate(hfm_index* x, FixedLocate& c, bool launch) {
     RET(SCAN(x->ulen.as<uint32_t>(), 1, icap, x->uoff.as<uint64_t>()));
     if (launch) {
       k_graph_totals<<<1, 32, 0, x->stream>>>(x->seg_base.as<uint64_t>(), nq, x->pos_base.as<uint64_t>() + nq,
-                                              x->uoff.as<uint64_t>() + icap, pcap, c.d_tot);
+                                              x->uoff.as<uint64_t>() + icap, pcap, upcap, c.d_tot);
       k_block_first<<<(unsigned)((icap + 255) / 256), 256, 0, x->stream>>>(x->uoff.as<uint64_t>(), (uint32_t)icap, RES_T,
-                                                                          x->blockmap.as<uint32_t>(), rblocks);
-      ResolveArgs A{x->urow.as<uint32_t>(), 1, x->uoff.as<uint64_t>(), (uint32_t)icap, pcap, d_bounds, nb, guard,
+                                                                          x->blockmap.as<uint32_t>(),
+                                                                          (upcap + RES_T - 1) / RES_T);
+      ResolveArgs A{x->urow.as<uint32_t>(), 1, x->uoff.as<uint64_t>(), (uint32_t)icap, upcap, d_bounds, nb, guard,
                     x->uout.as<uint32_t>(), &dc->walk_err, &dc->steps, x->blockmap.as<uint32_t>(), &c.d_tot->upos};
-      k_resolve<false><<<(unsigned)((pcap + RES_T - 1) / RES_T), RES_T, 0, x->stream>>>(F.d, A);
+      k_resolve<false><<<(unsigned)((upcap + RES_T - 1) / RES_T), RES_T, 0, x->stream>>>(F.d, A);
       k_block_first<<<(unsigned)((icap + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)icap, EXP_BLK,
                                                                           x->blockmap2.as<uint32_t>(), eblocks);
       k_dedup_expand<<<(unsigned)((pcap + EXP_BLK - 1) / EXP_BLK), EXP_T, 0, x->stream>>>(
@@ -1332,7 +1337,7 @@ static int fixed_locate(hfm_index* x, FixedLocate& c, bool launch) {
     }
   } else if (launch) {
     k_graph_totals<<<1, 32, 0, x->stream>>>(x->seg_base.as<uint64_t>(), nq, x->pos_base.as<uint64_t>() + nq, nullptr,
-                                            pcap, c.d_tot);
+                                            pcap, pcap, c.d_tot);
     k_block_first<<<(unsigned)((icap + 255) / 256), 256, 0, x->stream>>>(seg_off, (uint32_t)icap, RES_T,
                                                                         x->blockmap.as<uint32_t>(), rblocks);
     ResolveArgs A{seg_row, 1, seg_off, (uint32_t)icap, pcap, d_bounds, nb, guard, x->loc_pairs.as<uint32_t>(),
@@ -1956,6 +1961,7 @@ extern "C" int hfm_mems_graph_create(hfm_index* x, const uint8_t* d_q, const uin
   c.nb = nb;
   c.dedup = !(x->flags & HFM_FLAG_DEDUP_NEVER);
   c.pos_cap = std::max<uint64_t>(max_positions, 4096);
+  c.upos_cap = c.pos_cap / 16 + 4096;        // distinct positions: grown on a fallback
   c.d_tot = g->tot.as<GraphTotals>();
   c.h_tot = reinterpret_cast<GraphTotals*>(g->h_bases + 1);
   lk.unlock();
@@ -2029,11 +2035,15 @@ extern "C" int hfm_mems_graph_launch(hfm_graph* g, hfm_dev_mems* out, uint32_t* 
     h.d_pairs = x->loc_pairs.as<uint32_t>();
     g->loc_out = h;
     l.pos_cap = std::max<uint64_t>(l.pos_cap, h.total + h.total / 4 + 4096);
+    // distinct positions: what the adaptive run walked, at least twice the old capacity
+    l.upos_cap = std::max<uint64_t>(2 * l.upos_cap, x->stats.rows_unique + x->stats.rows_unique / 4 + 4096);
   }
   c.max_bases = std::max<uint64_t>(c.max_bases, g->h_bases[0] + g->h_bases[0] / 4);
   RET(mems_device(x, c.d_q, c.d_qoff, c.nq, c.P.min_len, c.P.mode, g->bounds.empty() ? nullptr : g->bounds.data(),
                   c.nb, c.P.max_hits, out));
   c.pos_cap = std::max<uint64_t>(c.pos_cap, out->n_positions + out->n_positions / 4 + 4096);
+  if (reason & HFM_GRAPH_POSITIONS)
+    c.upos_cap = std::max<uint64_t>(2 * c.upos_cap, x->stats.rows_unique + x->stats.rows_unique / 4 + 4096);
   if (replayed) *replayed = 0;
   return HFM_OK;
 }
@@ -2050,6 +2060,7 @@ extern "C" int hfm_mems_graph_add_locate(hfm_graph* g, const uint8_t* d_q, const
   l.d_q = d_q; l.d_qoff = d_qoff; l.nq = nq; l.max_hits = max_hits;
   l.iv_cap = std::max<uint64_t>(max_intervals, (uint64_t)nq * 2 + 4096);
   l.pos_cap = std::max<uint64_t>(max_positions, 4096);
+  l.upos_cap = l.pos_cap / 16 + 4096;
   l.dedup = !(x->flags & HFM_FLAG_DEDUP_NEVER);
   l.ctr = g->lctr.as<Counters>();
   l.d_tot = g->tot.as<GraphTotals>() + 1;
