@@ -2035,15 +2035,19 @@ extern "C" int hfm_mems_graph_launch(hfm_graph* g, hfm_dev_mems* out, uint32_t* 
     h.d_pairs = x->loc_pairs.as<uint32_t>();
     g->loc_out = h;
     l.pos_cap = std::max<uint64_t>(l.pos_cap, h.total + h.total / 4 + 4096);
-    // distinct positions: what the adaptive run walked, at least twice the old capacity
-    l.upos_cap = std::max<uint64_t>(2 * l.upos_cap, x->stats.rows_unique + x->stats.rows_unique / 4 + 4096);
+    // distinct positions: what the adaptive run walked (all its positions when it did not
+    // deduplicate: never fewer distinct than that), at least twice the old capacity
+    const uint64_t ru = x->stats.rows_unique ? x->stats.rows_unique : h.total;
+    l.upos_cap = std::max<uint64_t>(2 * l.upos_cap, ru + ru / 4 + 4096);
   }
   c.max_bases = std::max<uint64_t>(c.max_bases, g->h_bases[0] + g->h_bases[0] / 4);
   RET(mems_device(x, c.d_q, c.d_qoff, c.nq, c.P.min_len, c.P.mode, g->bounds.empty() ? nullptr : g->bounds.data(),
                   c.nb, c.P.max_hits, out));
   c.pos_cap = std::max<uint64_t>(c.pos_cap, out->n_positions + out->n_positions / 4 + 4096);
-  if (reason & HFM_GRAPH_POSITIONS)
-    c.upos_cap = std::max<uint64_t>(2 * c.upos_cap, x->stats.rows_unique + x->stats.rows_unique / 4 + 4096);
+  if (reason & HFM_GRAPH_POSITIONS) {
+    const uint64_t ru = x->stats.rows_unique ? x->stats.rows_unique : out->n_positions;
+    c.upos_cap = std::max<uint64_t>(2 * c.upos_cap, ru + ru / 4 + 4096);
+  }
   if (replayed) *replayed = 0;
   return HFM_OK;
 }
