@@ -139,7 +139,6 @@ SIGNATURES = {
     "hfm_last_stats": (C.c_int, [C.c_void_p, C.POINTER(HfmStats)]),
     "hfm_set_counters": (C.c_int, [C.c_void_p, C.c_int]),
     "hfm_set_timeout": (C.c_int, [C.c_void_p, C.c_uint32]),
-    "hfm_set_turns": (C.c_int, [C.c_void_p, C.c_int]),
     "hfm_mems_graph_create": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint32,
                                         C.c_uint32, u32p, C.c_uint32, C.c_uint32, C.c_uint64,
                                         C.POINTER(C.c_void_p)]),

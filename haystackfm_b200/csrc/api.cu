@@ -136,7 +136,6 @@ struct hfm_index {
   uint64_t seg_cap = 0;                            // segment candidate pool capacity (Cand)
   Counters* h_ctr = nullptr;        // pinned
   uint32_t timeout_ms = 0;          // host-side deadline of every wait on the stream (0: none)
-  bool turns = false;               // host-buffer calls take per-device turns (hfm_set_turns)
   std::vector<void*> orphans;       // result blocks of calls that timed out (freed once the stream drains)
   bool shared_index = false;        // fwd / rev device buffers belong to another handle
   cudaEvent_t ev_wait = nullptr;
@@ -1428,7 +1427,7 @@ static int make_shadow(hfm_index* x, hfm_index** out) {
   sh->device = x->device; sh->kind = x->kind; sh->flags = x->flags; sh->num_sms = x->num_sms;
   sh->seg_len = x->seg_len; sh->mems_variant = x->mems_variant; sh->count_work = x->count_work;
   sh->queue_chunk = x->queue_chunk; sh->threads_per_read = x->threads_per_read;
-  sh->timeout_ms = x->timeout_ms; sh->turns = x->turns;
+  sh->timeout_ms = x->timeout_ms;
   sh->shared_index = true;
   for (int k = 0; k < 2; k++) {
     const FmDev& src = k ? x->rev : x->fwd;
@@ -1769,13 +1768,6 @@ int hfm_mems_reserve(hfm_index* x, uint32_t nq, uint64_t intervals, uint64_t hit
   return HFM_OK;
 }
 
-int hfm_set_turns(hfm_index* x, int enable) {
-  if (!x) return set_error(HFM_E_ARG, "NULL argument");
-  std::lock_guard<std::mutex> lk(x->mu);
-  x->turns = enable != 0;
-  return HFM_OK;
-}
-
 int hfm_set_timeout(hfm_index* x, uint32_t ms) {
   if (!x) return set_error(HFM_E_ARG, "NULL argument");
   std::lock_guard<std::mutex> lk(x->mu);
@@ -1827,33 +1819,13 @@ int hfm_count_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint3
   return wait_stream(x);
 }
 
-// Turns of the host-buffer entry points on one device (handles with hfm_set_turns): the
-// device work of one call at a time, so a search runs at the whole GPU's speed instead of
-// sharing it with another handle's, and one large result copy at a time, so a copy runs
-// at the host link's full rate; a handle's next search then overlaps another's copy.
-// Copies below TURN_COPY_MIN (a locate's pairs, offsets) take no turn.
-struct DeviceTurns { std::mutex compute, copy; };
-static DeviceTurns& device_turns(int device) {
-  static DeviceTurns t[64];
-  return t[(unsigned)device & 63];
-}
-static constexpr size_t TURN_COPY_MIN = 64ull << 20;
-
-static std::unique_lock<std::mutex> take_turn(hfm_index* x, bool copy, size_t bytes = 0) {
-  if (!x->turns || (copy && bytes < TURN_COPY_MIN)) return std::unique_lock<std::mutex>();
-  DeviceTurns& t = device_turns(x->device);
-  return std::unique_lock<std::mutex>(copy ? t.copy : t.compute);
-}
-
 int hfm_locate_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32_t nq, uint32_t cap, hfm_hits** out) {
   if (!x || !out) return set_error(HFM_E_ARG, "NULL argument");
   *out = nullptr;
   Guard g(x);
-  std::unique_lock<std::mutex> turn = take_turn(x, false);
   RET(stage_queries(x, q, q_off, nq));
   hfm_dev_hits d{};
   RET(locate_device(x, x->q.as<uint8_t>(), x->qoff.as<uint64_t>(), nq, cap, &d));
-  if (turn.owns_lock()) turn.unlock();
   // one malloc block: struct | offsets | counts | pairs
   size_t bytes = sizeof(hfm_hits) + ((size_t)nq + 1) * 8 + (size_t)nq * 4 + 4 + (size_t)d.total * 8;
   uint8_t* blk = (uint8_t*)host_result_alloc(bytes);
@@ -1863,7 +1835,6 @@ int hfm_locate_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint
   h->offsets = (uint64_t*)(blk + sizeof(hfm_hits));
   h->pairs = (uint32_t*)(h->offsets + nq + 1);
   h->counts = h->pairs + d.total * 2;
-  std::unique_lock<std::mutex> copy_turn = take_turn(x, true, bytes);
   CK(cudaMemcpyAsync(h->offsets, d.d_offsets, ((size_t)nq + 1) * 8, cudaMemcpyDeviceToHost, x->stream));
   if (d.total) CK(cudaMemcpyAsync(h->pairs, d.d_pairs, (size_t)d.total * 8, cudaMemcpyDeviceToHost, x->stream));
   if (nq) CK(cudaMemcpyAsync(h->counts, d.d_counts, (size_t)nq * 4, cudaMemcpyDeviceToHost, x->stream));
@@ -1882,11 +1853,9 @@ int hfm_mems_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32
   if (!x || !out || (nb && !ref_bounds)) return set_error(HFM_E_ARG, "NULL argument");
   *out = nullptr;
   Guard g(x);
-  std::unique_lock<std::mutex> turn = take_turn(x, false);
   RET(stage_queries(x, q, q_off, nq));
   hfm_dev_mems d{};
   RET(mems_device(x, x->q.as<uint8_t>(), x->qoff.as<uint64_t>(), nq, min_len, mode, ref_bounds, nb, cap, &d));
-  if (turn.owns_lock()) turn.unlock();
   size_t bytes = sizeof(hfm_mem_out) + ((size_t)nq + 1) * 8 + (size_t)d.n_hits * sizeof(hfm_mem_hit) +
                  (size_t)d.n_positions * 8 + 8;
   uint8_t* blk = (uint8_t*)host_result_alloc(bytes);
@@ -1896,7 +1865,6 @@ int hfm_mems_batch(hfm_index* x, const uint8_t* q, const uint64_t* q_off, uint32
   m->hit_offsets = (uint64_t*)(blk + sizeof(hfm_mem_out));
   m->hits = (hfm_mem_hit*)(m->hit_offsets + nq + 1);
   m->positions = (uint32_t*)(m->hits + d.n_hits);
-  std::unique_lock<std::mutex> copy_turn = take_turn(x, true, bytes);
   CK(cudaMemcpyAsync(m->hit_offsets, d.d_hit_offsets, ((size_t)nq + 1) * 8, cudaMemcpyDeviceToHost, x->stream));
   if (d.n_hits) CK(cudaMemcpyAsync(m->hits, d.d_hits, (size_t)d.n_hits * sizeof(hfm_mem_hit), cudaMemcpyDeviceToHost, x->stream));
   if (d.n_positions) CK(cudaMemcpyAsync(m->positions, d.d_positions, (size_t)d.n_positions * 8, cudaMemcpyDeviceToHost, x->stream));

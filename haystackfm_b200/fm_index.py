@@ -139,10 +139,6 @@ class _Handle:
             self.h = None
         self._src = None
 
-    def set_turns(self, enable: bool = True) -> None:
-        """hfm_set_turns: host-buffer calls of this handle take per-device turns."""
-        L.check(L.lib().hfm_set_turns(self.h, 1 if enable else 0))
-
     def device_bytes(self) -> dict:
         """hfm_index_device_bytes: {"index": bytes of the layout, "work": work areas and results}."""
         a, b = C.c_uint64(), C.c_uint64()

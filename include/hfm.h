@@ -355,14 +355,6 @@ int hfm_set_counters(hfm_index* idx, int enable);  /* per-read work counters on/
  * counts_out included) until the next call on the handle, which first drains the abandoned
  * work; the handle stays usable. */
 int hfm_set_timeout(hfm_index* idx, uint32_t ms);
-/* Per-device turns for the host-buffer calls of this handle (no counterpart in the
- * reference; default off; a share made afterwards inherits it).  With several handles on
- * one GPU driven from several host threads (hfm_index_share), enable it on each: the device
- * work of hfm_locate_batch / hfm_mems_batch then runs one call at a time at the whole GPU's
- * speed, and result copies of 64 MiB or more run one at a time at the host link's full
- * rate, so one handle's search overlaps another's copy instead of two searches and two
- * copies sharing the GPU and the link.  Results do not change. */
-int hfm_set_turns(hfm_index* idx, int enable);
 
 /* Tunable parameters of the SMEM/MEM search and their autotuner (no counterpart in the
  * reference, whose shaders run a fixed workgroup_size(64), shaders/mem_find.wgsl:364-372).

@@ -146,7 +146,6 @@ def test_oracle_doubling_sort_equals_comparison_sort(oracle):
 
 def test_null_handle_timeout_rejected():
     assert L.lib().hfm_set_timeout(None, 5) == HFM_E_ARG
-    assert L.lib().hfm_set_turns(None, 1) == HFM_E_ARG
 
 
 def test_graph_and_probe_arguments_rejected_without_a_gpu():

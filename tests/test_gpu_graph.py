@@ -222,36 +222,3 @@ def test_graph_with_locate_chain(oracle):
         assert lib.hfm_mems_graph_add_locate(g, lq_d.data_ptr(), lo_d.data_ptr(), lq, 256, 0, 0) != 0
     finally:
         lib.hfm_mems_graph_free(g)
-
-
-def test_turns_keep_results_under_concurrency(oracle):
-    """Shares with per-device turns (hfm_set_turns), driven from three host threads through
-    the host-buffer calls, return the oracle's bytes for locate and find_smems."""
-    import threading
-    ref = synth.iupac_reference(total=1_000_000, n_contigs=10, n_run_mean=60, seed=111)
-    data = _build([al.DnaSequence(c) for c in ref.contigs], FmIndexConfig(sa_sample_rate=32, lookup_depth=10), 0,
-                  KIND_BIDIR)
-    idx = BidirFmIndex.from_bytes(data)
-    bounds = idx.seq_boundaries()
-    reads = synth.sample_reads(ref, n_reads=4000, seed=112)
-    flat, off = synth.pack_rows(reads)
-    k32, o32 = synth.pack_rows(reads, 32)
-    o = oracle.OracleIndex(data, KIND_BIDIR)
-    want_m = o.mems_packed(flat, off, 19, 0, bounds, 256, threads=8)
-    want_l = o.locate_packed(k32, o32, 256, threads=8)
-    idx.handle.set_turns(True)
-    shares = [idx.handle.share() for _ in range(3)]
-    got = [None] * 3
-
-    def run(k):
-        got[k] = [(shares[k].locate_packed(k32, o32, 256), shares[k].mems_packed(flat, off, 19, 0, bounds, 256))
-                  for _ in range(3)]
-    ts = [threading.Thread(target=run, args=(k,)) for k in range(3)]
-    for t in ts:
-        t.start()
-    for t in ts:
-        t.join()
-    for k in range(3):
-        for loc, mem in got[k]:
-            _same(loc, want_l)
-            _same(mem, want_m)
