@@ -360,6 +360,33 @@ def profile_step(args):
                       "locate_positions": dh.total}), flush=True)
 
 
+def ingest_bench(reads):
+    """The workload's reads as FASTQ text (307 bytes a record), parsed and encoded by
+    hfm_parse_reads on every host core, best of three: -> rate and a byte comparison of
+    the packed batch with the reads."""
+    from haystackfm_b200 import io as hio
+    n, m = reads.shape
+    sym = np.frombuffer(b"$ACGTNRYSWKMBDHV", dtype=np.uint8)
+    rec = np.empty((n, m * 2 + 7), dtype=np.uint8)
+    rec[:, 0:3] = np.frombuffer(b"@r\n", dtype=np.uint8)
+    rec[:, 3:3 + m] = sym[reads]
+    rec[:, 3 + m:6 + m] = np.frombuffer(b"\n+\n", dtype=np.uint8)
+    rec[:, 6 + m:6 + 2 * m] = ord("I")
+    rec[:, 6 + 2 * m] = ord("\n")
+    text = rec.tobytes()
+    best = None
+    for _ in range(3):
+        t0 = time.perf_counter()
+        flat, off = hio.parse_reads(text, "fastq")
+        dt = time.perf_counter() - t0
+        best = dt if best is None else min(best, dt)
+    equal = len(off) == n + 1 and bool(np.array_equal(flat, reads.reshape(-1)))
+    return {"format": "FASTQ", "bytes": len(text), "reads": n, "s": round(best, 3),
+            "reads_per_s": round(n / best), "gb_per_s": round(len(text) / best / 1e9, 2),
+            "threads": os.cpu_count(), "equal": equal,
+            "path": "hfm_parse_reads (text -> packed codes + offsets), the input of hfm_locate_batch / hfm_mems_batch"}
+
+
 def serving_latency(h, lib, L, kp, rp, bounds, n, n_batches, seed=17):
     """Batch latency through the host-buffer C ABI: batches of log-uniform size 1..100,000
     reads (mean ~8.7k) taken from the workload's reads, each a locate of the first 32-mer
@@ -1151,6 +1178,7 @@ def main():
                     "autotuned": tuning_main},
             "parity": parity,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "memory": memory,
+            "ingest": ingest_bench(reads) if rank == 0 else None,
             "plain": plain_info, "plain_launch": plain_launch, "graph": graph_info, "learned": learned_info,
             "serving": serving,
             "genome": genome,

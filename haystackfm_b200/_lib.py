@@ -39,6 +39,10 @@ class HfmHits(C.Structure):
                 ("counts", u32p), ("pairs", u32p)]
 
 
+class HfmReads(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("n_codes", C.c_uint64), ("offsets", u64p), ("codes", u8p)]
+
+
 class HfmMemHit(C.Structure):
     _fields_ = [("query_start", C.c_uint32), ("query_end", C.c_uint32), ("match_count", C.c_uint32),
                 ("truncated", C.c_uint32), ("fwd_lo", C.c_uint32), ("n_pos", C.c_uint32),
@@ -95,6 +99,7 @@ SIGNATURES = {
     "hfm_build_index_gpu": (C.c_int, [u8p, u64p, C.c_uint32, C.POINTER(C.c_char_p), C.POINTER(HfmBuildOpts),
                                       C.c_int, C.c_int, C.POINTER(u8p), C.POINTER(C.c_size_t)]),
     "hfm_index_load": (C.c_int, [u8p, C.c_size_t, C.c_int, C.POINTER(HfmOpts), C.POINTER(C.c_void_p)]),
+    "hfm_parse_reads": (C.c_int, [C.c_char_p, C.c_uint64, C.c_uint32, C.c_uint32, C.POINTER(C.POINTER(HfmReads))]),
     "hfm_index_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "hfm_index_export_layout": (C.c_int, [C.c_void_p, C.POINTER(u8p), C.POINTER(C.c_uint64)]),
     "hfm_index_load_layout": (C.c_int, [u8p, C.c_uint64, C.POINTER(HfmOpts), C.POINTER(C.c_void_p)]),

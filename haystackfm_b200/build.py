@@ -14,7 +14,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libhfm.so")
-SOURCES = ["api.cu", "mlp.cu", "bincode.cpp", "index_build.cpp", "index_gpu.cu", "probe.cu"]
+SOURCES = ["api.cu", "mlp.cu", "bincode.cpp", "index_build.cpp", "index_gpu.cu", "probe.cu", "ingest.cpp"]
 HEADERS = ["dev_index.cuh", "search.cuh", "resolve.cuh", "hfm_internal.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

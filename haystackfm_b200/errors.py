@@ -10,10 +10,11 @@ HFM_E_ARG = -4
 HFM_E_TIMEOUT = -5
 HFM_E_OVERFLOW = -6
 HFM_E_WALK = -7
+HFM_E_CHAR = -8
 
 STATUS_NAMES = {
     HFM_E_CUDA: "E_CUDA", HFM_E_OOM: "E_OOM", HFM_E_FORMAT: "E_FORMAT", HFM_E_ARG: "E_ARG",
-    HFM_E_TIMEOUT: "E_TIMEOUT", HFM_E_OVERFLOW: "E_OVERFLOW", HFM_E_WALK: "E_WALK",
+    HFM_E_TIMEOUT: "E_TIMEOUT", HFM_E_OVERFLOW: "E_OVERFLOW", HFM_E_WALK: "E_WALK", HFM_E_CHAR: "E_CHAR",
 }
 
 
@@ -42,6 +43,8 @@ class FmIndexError(Exception):
     def from_status(cls, status: int, message: str):
         if status == HFM_E_FORMAT:
             return cls("DeserializeError", f"deserialization failed: {message}", status)
+        if status == HFM_E_CHAR:
+            return cls("InvalidCharacter", message, status)
         if status == HFM_E_ARG and message.startswith("empty"):
             return cls("EmptySequence", message, status)
         return cls("GpuError", f"GPU error: {STATUS_NAMES.get(status, status)}: {message}", status)

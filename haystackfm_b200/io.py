@@ -73,6 +73,26 @@ def encode_reads(reads: Iterable[str]) -> Tuple[np.ndarray, np.ndarray]:
     return flat, off
 
 
+def parse_reads(text, fmt: str = "auto", threads: int = 0) -> Tuple[np.ndarray, np.ndarray]:
+    """hfm_parse_reads: FASTA / FASTQ / one-read-per-line text (str or bytes) -> the packed
+    (flat u8 codes, u64 offsets[n+1]) batch, parsed and encoded natively on the host's
+    threads.  Same reads as parse_fasta / parse_fastq + encode_reads; a character outside
+    the alphabet raises FmIndexError("InvalidCharacter")."""
+    import ctypes as C
+    from . import _lib as L
+    raw = text.encode("ascii") if isinstance(text, str) else bytes(text)
+    f = {"auto": 0, "fasta": 1, "fastq": 2}[fmt]
+    res = C.POINTER(L.HfmReads)()
+    L.check(L.lib().hfm_parse_reads(raw, len(raw), f, threads, C.byref(res)))
+    try:
+        r = res.contents
+        off = np.ctypeslib.as_array(r.offsets, shape=(r.n + 1,)).copy()
+        flat = np.ctypeslib.as_array(r.codes, shape=(r.n_codes,)).copy() if r.n_codes else np.zeros(1, np.uint8)
+    finally:
+        L.lib().hfm_free(res)
+    return flat, off
+
+
 def batches(n: int, batch: int):
     """[start, end) ranges covering n reads in batches of at most `batch`."""
     for a in range(0, n, batch):

@@ -31,6 +31,8 @@ extern "C" {
 #define HFM_E_TIMEOUT (-5)  /* the handle's deadline (hfm_set_timeout) passed while waiting    */
 #define HFM_E_OVERFLOW (-6) /* a per-read work set outgrew the largest fallback capacity     */
 #define HFM_E_WALK (-7)     /* an LF walk exceeded sample_rate steps (index inconsistent)   */
+#define HFM_E_CHAR (-8)     /* a read holds a character outside the alphabet, or no read was
+                               found (FmIndexError::InvalidCharacter)                        */
 
 #define HFM_KIND_FM 0       /* FmIndex bytes        (src/fm_index/serialize.rs:13-52)       */
 #define HFM_KIND_BIDIR 1    /* BidirFmIndex bytes   (src/fm_index/bidir_index.rs:183-210)   */
@@ -340,8 +342,33 @@ int hfm_mlp_schedule(hfm_mlp* m, const float* d_y, uint32_t nq, float warp_min_h
  * (CUDA events), *ms_out (may be NULL) = one launch. */
 int hfm_probe_gather(int device, uint64_t buffer_bytes, uint32_t span, float* gbs_out, float* ms_out);
 
+/* ---- read ingest (host) ---------------------------------------------------- */
+/* Text of reads -> the packed batch every query entry point takes (codes 1..15 of
+ * src/alphabet.rs:54-94, either case, U as T; offsets[n + 1] with offsets[0] = 0).
+ * format: HFM_READS_FASTA follows the reference's sequence reader (src/wasm/js_api.rs:18-68):
+ * `>` lines start a record whose non-blank lines are concatenated, blank lines are skipped,
+ * and lines before any header are one read each (no read at all: HFM_E_CHAR).
+ * HFM_READS_FASTQ: four-line records (`@name`, sequence, `+...`, quality), blank lines
+ * between records skipped, a malformed record is HFM_E_FORMAT with its line number.
+ * HFM_READS_AUTO: FASTQ when the first non-blank character is `@`, else FASTA.  Lines
+ * end at \n, \r\n or \r; white space around a line is ignored.  A character outside
+ * the alphabet (`$` included) is HFM_E_CHAR, naming the character, its read and position.
+ * threads: host threads for the encoding (0 = all).  *out is one block released with
+ * hfm_free.  No counterpart in the reference's GPU path (which takes encoded
+ * DnaSequence values); it replaces the caller-side parse + encode loop. */
+#define HFM_READS_AUTO 0u
+#define HFM_READS_FASTA 1u
+#define HFM_READS_FASTQ 2u
+typedef struct hfm_reads {
+  uint64_t n;          /* reads                       */
+  uint64_t n_codes;    /* total codes (offsets[n])    */
+  uint64_t* offsets;   /* n + 1 entries               */
+  uint8_t* codes;
+} hfm_reads;
+int hfm_parse_reads(const char* text, uint64_t len, uint32_t format, uint32_t threads, hfm_reads** out);
+
 /* ---- misc ----------------------------------------------------------------- */
-void hfm_free(void* p);                    /* frees hfm_hits*, hfm_mem_out*, build bytes */
+void hfm_free(void* p);                    /* frees hfm_hits*, hfm_mem_out*, hfm_reads*, build bytes */
 const char* hfm_last_error(void);          /* thread-local message of the last failure   */
 void* hfm_index_stream(hfm_index* idx);    /* the handle's cudaStream_t (for event timing) */
 int hfm_last_stats(const hfm_index* idx, hfm_stats* out);

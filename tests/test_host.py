@@ -9,6 +9,7 @@ import numpy as np
 import pytest
 import torch.multiprocessing as mp
 
+from haystackfm_b200 import _lib as L
 from haystackfm_b200 import alphabet as al
 from haystackfm_b200 import io as hio
 from haystackfm_b200.errors import FmIndexError
@@ -86,3 +87,58 @@ def test_sharded_run_gloo_world2(oracle, tmp_path):
     mp.spawn(_worker, args=(2, _free_port(), data, queries, str(tmp_path)), nprocs=2, join=True)
     assert list(np.load(tmp_path / "res.npy")) == want
     assert float(np.load(tmp_path / "t.npy")[0]) == 2.0
+
+
+def _py_packed_fasta(text):
+    seqs = hio.parse_fasta(text)
+    flat, off = L.pack_queries([s.as_slice() for s in seqs])
+    return flat, off
+
+
+def test_native_read_parser_matches_python_readers():
+    """hfm_parse_reads gives the packed batch of parse_fasta / parse_fastq + encode_reads:
+    multi-line and header-less FASTA, blank lines, CRLF, lower case and U, FASTQ with blank
+    lines between records, and automatic format detection."""
+    fasta = ">r1 x\r\nACGT\r\nac\r\n\r\n>empty\n>r2\n  NNRYu  \n"
+    for fmt in ("auto", "fasta"):
+        f, o = hio.parse_reads(fasta, fmt)
+        pf, po = _py_packed_fasta(fasta)
+        assert np.array_equal(o, po) and np.array_equal(f[:int(o[-1])], pf[:int(po[-1])])
+    plain = "ACGT\n\nTTGA\nn\n"
+    f, o = hio.parse_reads(plain)
+    pf, po = _py_packed_fasta(plain)
+    assert np.array_equal(o, po) and np.array_equal(f[:int(o[-1])], pf[:int(po[-1])])
+    fastq = "@r1\nACGTN\n+\nIIIII\n\n@r2 d\nggry\n+r2\nIIII\n@r3\n\n+\n\n"
+    for fmt in ("auto", "fastq"):
+        f, o = hio.parse_reads(fastq, fmt)
+        pf, po = hio.encode_reads([r for _, r in hio.parse_fastq(fastq)])
+        assert np.array_equal(o, po) and np.array_equal(f[:int(o[-1])], pf[:int(po[-1])])
+    f, o = hio.parse_reads("", "fastq")
+    assert list(o) == [0]
+
+
+def test_native_read_parser_large_batch_and_errors():
+    """A FASTQ batch large enough for the threaded encoding equals the Python encoding;
+    bad characters, '$', malformed records and empty FASTA input fail with the reference's
+    error kinds and the read and position in the message."""
+    rng = np.random.default_rng(5)
+    reads = ["".join(rng.choice(list("ACGTNRYacgtu"), int(rng.integers(50, 300)))) for _ in range(60_000)]
+    text = "".join(f"@q{i}\n{r}\n+\n{'I' * len(r)}\n" for i, r in enumerate(reads))
+    f, o = hio.parse_reads(text, "auto", threads=4)
+    pf, po = hio.encode_reads(reads)
+    assert np.array_equal(o, po) and np.array_equal(f, pf)
+    f, o = hio.parse_reads(text.replace("\n", "\r\n"), "fastq", threads=3)    # stretches cut inside CRLF text
+    assert np.array_equal(o, po) and np.array_equal(f, pf)
+    bad = text[:-1] + "\n@bad\nACGXT\n+\nIIIII\n"
+    with pytest.raises(FmIndexError) as e:
+        hio.parse_reads(bad, threads=4)
+    assert e.value.kind == "InvalidCharacter" and "'X' at position 3 of read 60000" in str(e.value)
+    with pytest.raises(FmIndexError) as e:
+        hio.parse_reads(">a\nAC$T\n")
+    assert e.value.kind == "InvalidCharacter" and "'$' at position 2 of read 0" in str(e.value)
+    with pytest.raises(FmIndexError) as e:
+        hio.parse_reads("@r1\nACGT\nIIII\n", "fastq")
+    assert e.value.kind == "DeserializeError" and "line 1" in str(e.value)
+    with pytest.raises(FmIndexError) as e:
+        hio.parse_reads("\n \n>only-header\n")
+    assert e.value.kind == "InvalidCharacter"
