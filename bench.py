@@ -856,7 +856,7 @@ def main():
                    s2.resolve_launches + s2.other_launches + p[5] for p in per for s1, s2 in [p[:2]])
 
     mem_mark("timed steps")
-    # the plain order, same loop (the learned path's fallback and judge)
+    # the plain order, same loop (the learned path's fallback and its yardstick)
     plain_info = None
     if learned is not None:
         for _ in range(args.warmup):

@@ -8,7 +8,7 @@ trained on the GPU by the library's own forward / backward kernels (hfm_mlp_*). 
 predicted cost (costliest first, warp-uniform runs of similar cost) and sends reads
 predicted to report many MemHits straight to the warp-per-read kernel.  The schedule only
 reorders work: results are byte-identical to the plain path for any model, which is its
-fallback and its judge.
+fallback and its yardstick.
 
 Device arrays are torch CUDA tensors (plumbing only; every kernel is the library's).
 """
@@ -195,7 +195,7 @@ class LearnedSmem:
             holdout: float = 0.1, calibrate: bool = True):
         """Log the exact kernel's work on the training reads, train on the first
         (1 - holdout) of them (MSE of standardised targets; per-epoch losses are in those
-        units), and judge the model on the rest: the learned order is used
+        units), and evaluate the model on the rest: the learned order is used
         only when its predicted Occ touches rank the held-out reads' true touches with
         Spearman >= min_spearman and (calibrate) the learned order runs the held-out reads
         at least 2% faster than the plain order; otherwise run() keeps the plain order."""
