@@ -104,6 +104,8 @@ extern "C" int hfm_parse_reads(const char* text, uint64_t len, uint32_t format, 
   if (len < (8u << 20)) nt = 1;
   std::vector<Line> rl;
   split_lines_parallel(text, len, nt, rl);
+  for (const Line& r : rl)
+    if (r.b - r.a > 0xFFFFFFFFull) return set_error(HFM_E_ARG, "a line longer than 4 GiB");
   if (format == HFM_READS_AUTO) {                 // the first non-blank character decides
     format = HFM_READS_FASTA;
     for (const Line& r : rl) {
