@@ -70,12 +70,13 @@ class HfmSched(C.Structure):
 
 class HfmTuning(C.Structure):
     _fields_ = [("mems_variant", C.c_uint32), ("seg_len", C.c_uint32), ("queue_chunk", C.c_uint32),
-                ("threads_per_read", C.c_uint32)]
+                ("threads_per_read", C.c_uint32), ("read_order", C.c_uint32)]
 
 
 # hfm_autotune_mems candidates {variant, seg_len, queue_chunk, threads_per_read}, in order
-TUNE_CANDIDATES = [(3, 512, 1, 1), (3, 256, 1, 1), (3, 1024, 1, 1), (2, 512, 1, 1), (3, 512, 4, 1), (3, 512, 16, 1),
-                   (3, 512, 1, 4), (3, 512, 1, 8), (3, 512, 1, 32)]
+TUNE_CANDIDATES = [(3, 512, 1, 1, 0), (3, 256, 1, 1, 0), (3, 1024, 1, 1, 0), (2, 512, 1, 1, 0), (3, 512, 4, 1, 0),
+                   (3, 512, 16, 1, 0), (3, 512, 1, 4, 0), (3, 512, 1, 8, 0), (3, 512, 1, 32, 0), (3, 512, 1, 1, 1),
+                   (3, 1024, 1, 1, 1)]
 
 
 class HfmStats(C.Structure):

@@ -8,6 +8,7 @@
 // src/fm_index/bidir_index.rs:410-411).
 
 #include <cuda_runtime.h>
+#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <chrono>
@@ -123,11 +124,12 @@ struct hfm_index {
       scan_tmp, out_pairs, ref_bounds, hit_start, hit_count, hit_base, hits, npos_scan, work, cwork, ctr,
       mivpool, bswork, memwork, hkeys, hslot, hflags, huid, urow, ulen, uoff, uout, blockmap, blockmap2, ovf2, ovf3,
       lflag, lpos, sids, lids, ucount, ubase, uread, uk, ubits, uexit, ust, ucoff, ucnt, segpool, fxe, fxc, fxx,
-      fxo, fxn, npos, loc_pairs;
+      fxo, fxn, npos, loc_pairs, okeys, oids, otemp;
   uint32_t flags = 0;
   uint32_t seg_len = 512;  // SMEM reads longer than 2 * seg_len take the segmented sweep
   uint32_t queue_chunk = 1;       // reads a per-thread kernel takes from its queue per atomic
   uint32_t threads_per_read = 1;  // 32: every read on the warp-per-read kernel
+  uint32_t read_order = 0;        // 1: SMEM queue in the order of the reads' first 16 codes
   DevBuf iota;                    // 0..nq-1 (the order of a batch sent whole to the warp kernel)
   int mems_variant = 3;   // SMEM fast-kernel variant (see mems_device): 2 local 32-entry
                           // candidate lists; 3 global 1024-entry lists
@@ -555,6 +557,44 @@ static int locate_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qof
   return HFM_OK;
 }
 
+// Sort key of a read for the prefix queue order: its first 16 codes, 4 bits each, the first
+// code in the top bits; a shorter read is padded with code 0, which no read holds.
+__global__ void k_prefix_keys(const uint8_t* __restrict__ q, const uint64_t* __restrict__ qoff, uint32_t n,
+                              unsigned long long* __restrict__ keys, uint32_t* __restrict__ ids) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t o = qoff[i], len = qoff[i + 1] - o;
+  unsigned long long k = 0;
+#pragma unroll
+  for (uint32_t j = 0; j < 16; j++) k = (k << 4) | (j < len ? (unsigned long long)(q[o + j] & 15u) : 0ull);
+  keys[i] = k;
+  ids[i] = i;
+}
+
+// The queue order of read_order = 1: reads sorted by their first 16 codes (radix sort of
+// key / index pairs on the handle's stream).  Reads that share a prefix then sit in one
+// warp and carry the same reference windows (on an IUPAC text, the N-run windows that a
+// read's first bases select), so their interval sets have alike sizes and their Occ
+// records are fetched once for the warp.  Any order gives the same results.
+static int prefix_order(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, const uint32_t*& order,
+                        uint32_t& launches) {
+  RET(x->okeys.ensure((size_t)nq * 16 + 16));
+  RET(x->oids.ensure((size_t)nq * 8 + 8));
+  unsigned long long* k_in = x->okeys.as<unsigned long long>();
+  unsigned long long* k_out = k_in + nq;
+  uint32_t* i_in = x->oids.as<uint32_t>();
+  uint32_t* i_out = i_in + nq;
+  size_t temp = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, temp, k_in, k_out, i_in, i_out, (int)nq, 0, 64, x->stream));
+  RET(x->otemp.ensure(temp + 16));
+  k_prefix_keys<<<(nq + 255) / 256, 256, 0, x->stream>>>(d_q, d_qoff, nq, k_in, i_in);
+  CK(cudaGetLastError());
+  CK(cub::DeviceRadixSort::SortPairs(x->otemp.p, temp, k_in, k_out, i_in, i_out, (int)nq, 0, 64, x->stream));
+  launches += nq > 8192 ? 11 : 2;     // keys, then a histogram, a scan and 8 one-sweep passes (one tile when small)
+  order = i_out;
+  return HFM_OK;
+}
+
 static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, uint32_t min_len,
                        uint32_t mode, const uint32_t* h_bounds, uint32_t nb, uint32_t cap, hfm_dev_mems* out,
                        const hfm_sched* sc = nullptr) {
@@ -562,6 +602,7 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   if (mode > 1) return set_error(HFM_E_ARG, "mode must be 0 (SMEM) or 1 (MEM)");
   const uint32_t* order = sc ? sc->d_order : nullptr;
   uint32_t n_warp = sc ? sc->n_warp : 0;
+  bool own_order = false;                      // an order made here: a permutation by construction
   if (!sc && x->threads_per_read > 1 && x->mems_variant != MEMS_PLAIN && nq) {
     // every read on the lane-group kernels (a warp or 4, 8, 16 lanes per read): the
     // identity order, all of it routed
@@ -576,7 +617,11 @@ static int mems_device(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff,
   if (n_warp && !order) return set_error(HFM_E_ARG, "sched.n_warp needs sched.d_order");
   begin_stats(x);
   uint32_t launches = 0, other = 0;
-  if (order && nq) {
+  if (!order && x->read_order == 1 && x->threads_per_read == 1 && x->mems_variant != MEMS_PLAIN && nq > 1) {
+    RET(prefix_order(x, d_q, d_qoff, nq, order, other));
+    own_order = true;
+  }
+  if (order && nq && !own_order) {
     // the order must be a permutation of 0..nq-1: every read is processed exactly once
     RET(x->hflags.ensure((size_t)nq * 4));
     CK(cudaMemsetAsync(x->hflags.p, 0, (size_t)nq * 4, x->stream));
@@ -1426,7 +1471,7 @@ static int make_shadow(hfm_index* x, hfm_index** out) {
   std::unique_ptr<hfm_index> sh(new hfm_index());
   sh->device = x->device; sh->kind = x->kind; sh->flags = x->flags; sh->num_sms = x->num_sms;
   sh->seg_len = x->seg_len; sh->mems_variant = x->mems_variant; sh->count_work = x->count_work;
-  sh->queue_chunk = x->queue_chunk; sh->threads_per_read = x->threads_per_read;
+  sh->queue_chunk = x->queue_chunk; sh->threads_per_read = x->threads_per_read; sh->read_order = x->read_order;
   sh->timeout_ms = x->timeout_ms;
   sh->shared_index = true;
   for (int k = 0; k < 2; k++) {
@@ -1638,7 +1683,8 @@ int hfm_index_device_bytes(const hfm_index* x, uint64_t* index_bytes, uint64_t* 
       &x->mivpool, &x->bswork, &x->memwork, &x->hkeys, &x->hslot, &x->hflags, &x->huid, &x->urow, &x->ulen,
       &x->uoff, &x->uout, &x->blockmap, &x->blockmap2, &x->ovf2, &x->ovf3, &x->lflag, &x->lpos, &x->sids,
       &x->lids, &x->ucount, &x->ubase, &x->uread, &x->uk, &x->ubits, &x->uexit, &x->ust, &x->ucoff, &x->ucnt,
-      &x->segpool, &x->fxe, &x->fxc, &x->fxx, &x->fxo, &x->fxn, &x->npos, &x->iota, &x->loc_pairs};
+      &x->segpool, &x->fxe, &x->fxc, &x->fxx, &x->fxo, &x->fxn, &x->npos, &x->iota, &x->loc_pairs,
+      &x->okeys, &x->oids, &x->otemp};
   uint64_t a = 0, b = 0;
   if (!x->shared_index) for (const DevBuf* d : idx_bufs) a += d->cap;
   for (const DevBuf* d : work_bufs) b += d->cap;
@@ -1664,7 +1710,8 @@ void hfm_index_free(hfm_index* x) {
                     &x->hkeys, &x->hslot, &x->hflags, &x->huid, &x->urow, &x->ulen, &x->uoff, &x->uout,
                     &x->blockmap, &x->blockmap2, &x->ovf2, &x->ovf3, &x->lflag, &x->lpos, &x->sids, &x->lids,
                     &x->ucount, &x->ubase, &x->uread, &x->uk, &x->ubits, &x->uexit, &x->ust, &x->ucoff, &x->ucnt,
-                    &x->segpool, &x->fxe, &x->fxc, &x->fxx, &x->fxo, &x->fxn, &x->npos, &x->iota, &x->loc_pairs})
+                    &x->segpool, &x->fxe, &x->fxc, &x->fxx, &x->fxo, &x->fxn, &x->npos, &x->iota, &x->loc_pairs,
+                    &x->okeys, &x->oids, &x->otemp})
     b->release();
   for (auto& e : x->ev) if (e) cudaEventDestroy(e);
   for (auto& e : x->evk) if (e) cudaEventDestroy(e);
@@ -1697,6 +1744,7 @@ int hfm_get_tuning(const hfm_index* x, hfm_tuning* t) {
   t->seg_len = x->seg_len;
   t->queue_chunk = x->queue_chunk;
   t->threads_per_read = x->threads_per_read;
+  t->read_order = x->read_order;
   return HFM_OK;
 }
 
@@ -1708,11 +1756,13 @@ int hfm_set_tuning(hfm_index* x, const hfm_tuning* t) {
   if (t->threads_per_read != 1 && t->threads_per_read != 4 && t->threads_per_read != 8 && t->threads_per_read != 16 &&
       t->threads_per_read != 32)
     return set_error(HFM_E_ARG, "threads_per_read must be 1, 4, 8, 16 or 32");
+  if (t->read_order > 1) return set_error(HFM_E_ARG, "read_order must be 0 or 1");
   std::lock_guard<std::mutex> lk(x->mu);
   x->mems_variant = (int)t->mems_variant;
   x->seg_len = t->seg_len;
   x->queue_chunk = t->queue_chunk;
   x->threads_per_read = t->threads_per_read;
+  x->read_order = t->read_order;
   return HFM_OK;
 }
 
@@ -1724,13 +1774,13 @@ int hfm_autotune_mems(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, 
   reps = std::max(1u, reps);
   Guard g(x);
   // HFM_TUNE_CANDIDATES settings, in the order include/hfm.h lists them
-  const hfm_tuning cands[HFM_TUNE_CANDIDATES] = {{3, 512, 1, 1}, {3, 256, 1, 1}, {3, 1024, 1, 1}, {2, 512, 1, 1},
-                                                 {3, 512, 4, 1}, {3, 512, 16, 1}, {3, 512, 1, 4},  {3, 512, 1, 8},
-                                                 {3, 512, 1, 32}};
-  const hfm_tuning saved{(uint32_t)x->mems_variant, x->seg_len, x->queue_chunk, x->threads_per_read};
+  const hfm_tuning cands[HFM_TUNE_CANDIDATES] = {
+      {3, 512, 1, 1, 0}, {3, 256, 1, 1, 0},  {3, 1024, 1, 1, 0}, {2, 512, 1, 1, 0},  {3, 512, 4, 1, 0}, {3, 512, 16, 1, 0},
+      {3, 512, 1, 4, 0}, {3, 512, 1, 8, 0},  {3, 512, 1, 32, 0}, {3, 512, 1, 1, 1}, {3, 1024, 1, 1, 1}};
+  const hfm_tuning saved{(uint32_t)x->mems_variant, x->seg_len, x->queue_chunk, x->threads_per_read, x->read_order};
   auto apply = [&](const hfm_tuning& t) {
     x->mems_variant = (int)t.mems_variant; x->seg_len = t.seg_len;
-    x->queue_chunk = t.queue_chunk; x->threads_per_read = t.threads_per_read;
+    x->queue_chunk = t.queue_chunk; x->threads_per_read = t.threads_per_read; x->read_order = t.read_order;
   };
   float best_ms = 0.f;
   int best_k = -1;

@@ -270,12 +270,14 @@ class _Handle:
         t = L.HfmTuning()
         L.check(L.lib().hfm_get_tuning(self.h, C.byref(t)))
         return {"mems_variant": t.mems_variant, "seg_len": t.seg_len, "queue_chunk": t.queue_chunk,
-                "threads_per_read": t.threads_per_read}
+                "threads_per_read": t.threads_per_read, "read_order": t.read_order}
 
-    def set_tuning(self, mems_variant: int, seg_len: int, queue_chunk: int = None, threads_per_read: int = None):
+    def set_tuning(self, mems_variant: int, seg_len: int, queue_chunk: int = None, threads_per_read: int = None,
+                   read_order: int = None):
         cur = self.tuning()
         t = L.HfmTuning(mems_variant, seg_len, cur["queue_chunk"] if queue_chunk is None else queue_chunk,
-                        cur["threads_per_read"] if threads_per_read is None else threads_per_read)
+                        cur["threads_per_read"] if threads_per_read is None else threads_per_read,
+                        cur["read_order"] if read_order is None else read_order)
         L.check(L.lib().hfm_set_tuning(self.h, C.byref(t)))
 
     def autotune_mems(self, q_d, off_d, nq: int, min_len: int, mode: int, ref_bounds, max_hits: int, reps: int = 2):
@@ -287,9 +289,9 @@ class _Handle:
                                           L.ptr(rb, L.u32p) if len(rb) else None, len(rb), max_hits, reps,
                                           C.byref(best), times.ctypes.data_as(C.POINTER(C.c_float))))
         return {"mems_variant": best.mems_variant, "seg_len": best.seg_len, "queue_chunk": best.queue_chunk,
-                "threads_per_read": best.threads_per_read,
-                "candidates_ms": {f"v{v}/seg{sl}/chunk{ch}/tpr{tp}": round(float(t), 3)
-                                  for (v, sl, ch, tp), t in zip(L.TUNE_CANDIDATES, times)}}
+                "threads_per_read": best.threads_per_read, "read_order": best.read_order,
+                "candidates_ms": {f"v{v}/seg{sl}/chunk{ch}/tpr{tp}/order{od}": round(float(t), 3)
+                                  for (v, sl, ch, tp, od), t in zip(L.TUNE_CANDIDATES, times)}}
 
 
 class _DeviceArray:

@@ -397,22 +397,27 @@ int hfm_set_timeout(hfm_index* idx, uint32_t ms);
  *                     (multiple of 32 in 64..4096, default 512).
  *   queue_chunk       reads a per-thread kernel takes from its device work queue per atomic
  *                     (1..64, default 1).
+ *   read_order        0 (default): the SMEM queue in the caller's read order (or the order of
+ *                     hfm_mems_batch_device_sched); 1: reads queued in the order of their first
+ *                     16 codes (a device radix sort; per-thread kernels only), so that reads
+ *                     sharing a prefix — and the reference windows it selects — share a warp.
  *   threads_per_read  1 (default): a thread per read; 4, 8 or 16: every read on a group of
  *                     that many lanes (sub-warp kernel, the fast pass's set capacities; a
  *                     read that outgrows them goes on to the warp tier); 32: every read on
  *                     the warp-per-read kernel (the lanes of a group share each interval set).
  * hfm_autotune_mems times the search of a sample batch under each of the HFM_TUNE_CANDIDATES
- * settings {variant, seg_len, chunk, threads}: {3,512,1,1}, {3,256,1,1}, {3,1024,1,1},
- * {2,512,1,1}, {3,512,4,1}, {3,512,16,1}, {3,512,1,4}, {3,512,1,8}, {3,512,1,32} — best of
- * `reps` runs after a warm-up run, by CUDA events on the handle's stream; it keeps the
- * fastest on the handle, writes it to *best, and the candidates' times to
- * times_ms[HFM_TUNE_CANDIDATES] when non-NULL. */
-#define HFM_TUNE_CANDIDATES 9
+ * settings {variant, seg_len, chunk, threads, order}: {3,512,1,1,0}, {3,256,1,1,0},
+ * {3,1024,1,1,0}, {2,512,1,1,0}, {3,512,4,1,0}, {3,512,16,1,0}, {3,512,1,4,0}, {3,512,1,8,0},
+ * {3,512,1,32,0}, {3,512,1,1,1}, {3,1024,1,1,1} — best of `reps` runs after a warm-up run,
+ * by CUDA events on the handle's stream; it keeps the fastest on the handle, writes it to
+ * *best, and the candidates' times to times_ms[HFM_TUNE_CANDIDATES] when non-NULL. */
+#define HFM_TUNE_CANDIDATES 11
 typedef struct hfm_tuning {
   uint32_t mems_variant;
   uint32_t seg_len;
   uint32_t queue_chunk;
   uint32_t threads_per_read;
+  uint32_t read_order;
 } hfm_tuning;
 int hfm_get_tuning(const hfm_index* idx, hfm_tuning* out);
 int hfm_set_tuning(hfm_index* idx, const hfm_tuning* t);

@@ -123,18 +123,21 @@ def test_autotune_keeps_results(oracle):
     q = torch.from_numpy(flat).cuda()
     o = torch.from_numpy(off.view(np.int64)).cuda()
     res = h.autotune_mems(q, o, len(off) - 1, 19, 0, bounds, 128, reps=1)
-    chosen = (res["mems_variant"], res["seg_len"], res["queue_chunk"], res["threads_per_read"])
+    chosen = (res["mems_variant"], res["seg_len"], res["queue_chunk"], res["threads_per_read"], res["read_order"])
     assert chosen in L.TUNE_CANDIDATES
     assert h.tuning() == {"mems_variant": chosen[0], "seg_len": chosen[1], "queue_chunk": chosen[2],
-                          "threads_per_read": chosen[3]}
+                          "threads_per_read": chosen[3], "read_order": chosen[4]}
     assert len(res["candidates_ms"]) == len(L.TUNE_CANDIDATES) and all(v > 0 for v in res["candidates_ms"].values())
-    for v, sl, ch, tp in [(3, 64, 1, 1), (3, 4096, 1, 1), (2, 512, 1, 1), (4, 512, 1, 1), (3, 512, 7, 1),
-                          (3, 256, 64, 1), (3, 512, 1, 32), (2, 512, 3, 32), (3, 512, 1, 4), (3, 512, 1, 8),
-                          (3, 512, 1, 16), (2, 512, 3, 4)]:
-        h.set_tuning(v, sl, ch, tp)
+    for v, sl, ch, tp, od in [(3, 64, 1, 1, 0), (3, 4096, 1, 1, 0), (2, 512, 1, 1, 0), (4, 512, 1, 1, 0),
+                              (3, 512, 7, 1, 0), (3, 256, 64, 1, 0), (3, 512, 1, 32, 0), (2, 512, 3, 32, 0),
+                              (3, 512, 1, 4, 0), (3, 512, 1, 8, 0), (3, 512, 1, 16, 0), (2, 512, 3, 4, 0),
+                              (3, 512, 1, 1, 1), (3, 64, 1, 1, 1), (2, 512, 5, 1, 1), (4, 512, 1, 1, 1),
+                              (3, 512, 1, 8, 1)]:
+        h.set_tuning(v, sl, ch, tp, od)
         _same(h.mems_packed(flat, off, 19, 0, bounds, 128), want)
         _same(h.mems_sched_packed(flat, off, 19, 0, bounds, 128), want)
-    for bad in [(5, 512, 1, 1), (3, 100, 1, 1), (3, 512, 0, 1), (3, 512, 65, 1), (3, 512, 1, 2), (3, 512, 1, 12)]:
+    for bad in [(5, 512, 1, 1, 0), (3, 100, 1, 1, 0), (3, 512, 0, 1, 0), (3, 512, 65, 1, 0), (3, 512, 1, 2, 0),
+                (3, 512, 1, 12, 0), (3, 512, 1, 1, 2)]:
         with pytest.raises(FmIndexError):
             h.set_tuning(*bad)
 
@@ -187,3 +190,33 @@ def test_sub_warp_groups_bit_exact(oracle, tpr):
         _same(h.mems_packed(sf, so, 15, 1, bounds, 16), o.mems_packed(sf, so, 15, 1, bounds, 16, threads=8))
     finally:
         h.set_tuning(saved["mems_variant"], saved["seg_len"], saved["queue_chunk"], saved["threads_per_read"])
+
+
+def test_prefix_read_order_bit_exact(oracle):
+    """read_order = 1 (reads queued by their first 16 codes, a device radix sort) gives the
+    bytes of the caller's order, on a batch large enough for the multi-pass sort, in SMEM
+    and MEM mode; a subsample equals the oracle's."""
+    ref = synth.iupac_reference(total=2_000_000, n_contigs=20, n_run_mean=60, seed=121)
+    reads = synth.sample_reads(ref, n_reads=30_000, seed=122)
+    flat, off = synth.pack_rows(reads)
+    b = _build([al.DnaSequence(c) for c in ref.contigs], FmIndexConfig(sa_sample_rate=32, lookup_depth=10), 0,
+               KIND_BIDIR)
+    idx = BidirFmIndex.from_bytes(b)
+    h = idx.handle
+    bounds = idx.seq_boundaries()
+    saved = h.tuning()
+    try:
+        h.set_tuning(3, 512, 1, 1, 0)
+        want = h.mems_packed(flat, off, 19, 0, bounds, 64)
+        want_mem = h.mems_packed(flat[:150 * 3000], off[:3001], 17, 1, bounds, 8)
+        h.set_tuning(3, 512, 1, 1, 1)
+        assert h.tuning()["read_order"] == 1
+        for _ in range(2):
+            _same(h.mems_packed(flat, off, 19, 0, bounds, 64), want)
+        _same(h.mems_packed(flat[:150 * 3000], off[:3001], 17, 1, bounds, 8), want_mem)
+        sf, so = flat[:150 * 2000], off[:2001]
+        _same(h.mems_packed(sf, so, 19, 0, bounds, 64),
+              oracle.OracleIndex(b, KIND_BIDIR).mems_packed(sf, so, 19, 0, bounds, 64, threads=8))
+    finally:
+        h.set_tuning(saved["mems_variant"], saved["seg_len"], saved["queue_chunk"], saved["threads_per_read"],
+                     saved["read_order"])
