@@ -654,7 +654,8 @@ def genome_workloads(args, device, torch):
     # learned: train on the logged work of the 2M reads, evaluate on held-out reads
     ls = LearnedSmem(h, device, seed=1)
     t0 = time.time()
-    losses, _, _ = ls.fit(r3_q, r3_o, n3, 19, 0, bounds, 1024, epochs=args.train_epochs, batch=8192, lr=1e-3)
+    losses, _, _ = ls.fit(r3_q, r3_o, n3, 19, 0, bounds, 1024, epochs=args.train_epochs, batch=8192, lr=1e-3,
+                          calibrate_all=True)
     learned = {"train_reads": n3, "epochs": args.train_epochs, "fit_s": round(time.time() - t0, 1),
                "train_mse": [round(float(v), 4) for v in losses],
                "holdout_error": ls.holdout_error.as_dict() if ls.holdout_error else None,
@@ -792,7 +793,7 @@ def main():
         learned = LearnedSmem(h, local, seed=1)
         t0 = time.perf_counter()
         losses, _, _ = learned.fit(tr_d, tr_off, args.train_reads, 19, 0, bounds, 1024, epochs=args.train_epochs,
-                                   batch=8192, lr=1e-3)
+                                   batch=8192, lr=1e-3, calibrate_all=True)
         torch.cuda.synchronize()
         fit_s = time.perf_counter() - t0
         del tr_d, tr_off

@@ -192,7 +192,7 @@ class LearnedSmem:
         return log[:4 * nq].view(nq, 4)
 
     def fit(self, q_d, off_d, nq, min_len, mode, bounds, max_hits, epochs=4, batch=8192, lr=1e-3, seed=0,
-            holdout: float = 0.1, calibrate: bool = True):
+            holdout: float = 0.1, calibrate: bool = True, calibrate_all: bool = False):
         """Log the exact kernel's work on the training reads, train on the first
         (1 - holdout) of them (MSE of standardised targets; per-epoch losses are in those
         units), and evaluate the model on the rest: the learned order is used
@@ -225,7 +225,11 @@ class LearnedSmem:
             self.holdout_error = prediction_error(self.model.forward(x[ntr:].contiguous()), t[ntr:])
             self.enabled = self.holdout_error.spearman_touches >= self.min_spearman
             if self.enabled and calibrate:
-                self.calibrate(q_d, off_d, ntr, nq, min_len, mode, bounds, max_hits)
+                # the order's effect depends on the batch size (how many reads share a warp's
+                # prefix, how long the queue's tail is): calibrate_all times it on every
+                # training read, a batch the size of the one it will run on
+                a = 0 if calibrate_all else ntr
+                self.calibrate(q_d, off_d, a, nq, min_len, mode, bounds, max_hits)
         return losses, x, t
 
     def calibrate(self, q_d, off_d, a, b, min_len, mode, bounds, max_hits, reps=2):
