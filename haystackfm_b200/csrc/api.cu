@@ -577,7 +577,7 @@ __global__ void k_prefix_keys(const uint8_t* __restrict__ q, const uint64_t* __r
 // read's first bases select), so their interval sets have alike sizes and their Occ
 // records are fetched once for the warp.  Any order gives the same results.
 static int prefix_order(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff, uint32_t nq, const uint32_t*& order,
-                        uint32_t& launches) {
+                        uint32_t& launches, bool launch = true) {
   RET(x->okeys.ensure((size_t)nq * 16 + 16));
   RET(x->oids.ensure((size_t)nq * 8 + 8));
   unsigned long long* k_in = x->okeys.as<unsigned long long>();
@@ -587,6 +587,8 @@ static int prefix_order(hfm_index* x, const uint8_t* d_q, const uint64_t* d_qoff
   size_t temp = 0;
   CK(cub::DeviceRadixSort::SortPairs(nullptr, temp, k_in, k_out, i_in, i_out, (int)nq, 0, 64, x->stream));
   RET(x->otemp.ensure(temp + 16));
+  order = i_out;
+  if (!launch) return HFM_OK;                  // sizing pass of a graph capture
   k_prefix_keys<<<(nq + 255) / 256, 256, 0, x->stream>>>(d_q, d_qoff, nq, k_in, i_in);
   CK(cudaGetLastError());
   CK(cub::DeviceRadixSort::SortPairs(x->otemp.p, temp, k_in, k_out, i_in, i_out, (int)nq, 0, 64, x->stream));
@@ -1112,16 +1114,19 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
   const uint16_t* cfw = Fw.compat.as<uint16_t>();
   const uint16_t* crv = Rv.compat.as<uint16_t>();
   if (launch) CK(cudaMemsetAsync(x->ctr.p, 0, sizeof(Counters), x->stream));
+  // the prefix queue order (read_order 1), inside the captured work like the rest
+  const uint32_t* ord = nullptr;
+  if (x->read_order == 1 && x->threads_per_read == 1 && nq > 1) RET(prefix_order(x, c.d_q, c.d_qoff, nq, ord, dummy, launch));
   // search: long reads cut into segments, every read through the segment queue
   if (seg) {
     if (launch) {
-      k_long_flags<<<(nq + 255) / 256, 256, 0, x->stream>>>(nullptr, nq, c.d_qoff, 2 * x->seg_len, x->lflag.as<uint32_t>());
+      k_long_flags<<<(nq + 255) / 256, 256, 0, x->stream>>>(ord, nq, c.d_qoff, 2 * x->seg_len, x->lflag.as<uint32_t>());
       CK(cudaGetLastError());
     }
     RET(SCAN(x->lflag.as<uint32_t>(), 1, nq, x->lpos.as<uint64_t>()));
     if (launch) {
       CK(cudaMemsetAsync(x->ucount.p, 0, (size_t)nq * 4, x->stream));
-      k_split_ids<<<(nq + 255) / 256, 256, 0, x->stream>>>(nullptr, nq, x->lflag.as<uint32_t>(), x->lpos.as<uint64_t>(),
+      k_split_ids<<<(nq + 255) / 256, 256, 0, x->stream>>>(ord, nq, x->lflag.as<uint32_t>(), x->lpos.as<uint64_t>(),
                                                            x->sids.as<uint32_t>(), x->lids.as<uint32_t>(),
                                                            x->ucount.as<uint32_t>(), c.d_qoff, x->seg_len);
       CK(cudaGetLastError());
@@ -1154,7 +1159,7 @@ static int fixed_chain(hfm_index* x, FixedChain& c, bool launch) {
       CK(cudaGetLastError());
     }
   } else if (launch) {
-    MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), FAST_CAND_CAP, &dc->queue, nullptr, nq,
+    MemsWork W{x->memwork.as<BIv>(), MEM_SET_CAP, x->cwork.as<Cand>(), FAST_CAND_CAP, &dc->queue, ord, nq,
                &dc->still_ovf, 0u, nullptr, nullptr};
     W.chunk = x->queue_chunk;
     WITH_FMT(fmt, {

@@ -222,3 +222,26 @@ def test_graph_with_locate_chain(oracle):
         assert lib.hfm_mems_graph_add_locate(g, lq_d.data_ptr(), lo_d.data_ptr(), lq, 256, 0, 0) != 0
     finally:
         lib.hfm_mems_graph_free(g)
+
+
+def test_graph_with_prefix_order(oracle):
+    """A handle tuned to the prefix queue order (read_order 1): the captured chain sorts the
+    reads inside the graph and its replays give the adaptive chain's bytes."""
+    ref = synth.iupac_reference(total=2_000_000, n_contigs=20, n_run_mean=60, seed=131)
+    h, lib, bounds, bp, batches, nq, q_d, o_d, load, adaptive, want0, cap_bases = _case(ref, 0, 133, oracle)
+    h.set_tuning(3, 512, 1, 1, 1)
+    g = C.c_void_p()
+    L.check(lib.hfm_mems_graph_create(h.h, q_d.data_ptr(), o_d.data_ptr(), nq, cap_bases, 19, 0, bp, len(bounds), 64,
+                                      2 * len(want0[2]) + 4096, C.byref(g)))
+    try:
+        rep = C.c_uint32()
+        for b in (0, 1, 2, 1):
+            load(batches[b])
+            want = adaptive()
+            dm = L.HfmDevMems()
+            L.check(lib.hfm_mems_graph_launch(g, C.byref(dm), C.byref(rep)))
+            _same(_host(dm, nq, 0), want)
+        assert rep.value == 1
+    finally:
+        lib.hfm_mems_graph_free(g)
+        h.set_tuning(3, 512, 1, 1, 0)
