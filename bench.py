@@ -74,6 +74,8 @@ def parse():
     ap.add_argument("--no-serving", action="store_true", help="skip the batch-latency measurement")
     ap.add_argument("--serving-batches", type=int, default=1000)
     ap.add_argument("--serving-workers", type=int, default=3)
+    ap.add_argument("--read-order", type=int, default=1,
+                    help="read_order of the profile modes (1: the autotuner's choice on the IUPAC workload)")
     ap.add_argument("--profile-step", action="store_true",
                     help="only the W + K headline steps (the launch-list command)")
     ap.add_argument("--profile-smem", action="store_true",
@@ -317,6 +319,7 @@ def profile_smem(args):
     _, data, reads, _, _ = workload(args)
     idx = BidirFmIndex.from_bytes(data)
     h, lib, n = idx.handle, L.lib(), args.reads
+    h.set_tuning(3, 512, 1, 1, args.read_order)
     rd = torch.from_numpy(reads.reshape(-1)).cuda()
     off = torch.arange(0, (n + 1) * 150, 150, dtype=torch.int64, device="cuda")
     dm = L.HfmDevMems()
@@ -339,6 +342,7 @@ def profile_step(args):
     _, data, reads, _, _ = workload(args)
     idx = BidirFmIndex.from_bytes(data)
     h, lib, n = idx.handle, L.lib(), args.reads
+    h.set_tuning(3, 512, 1, 1, args.read_order)
     bounds = np.ascontiguousarray(idx.seq_boundaries(), dtype=np.uint32)
     rd = torch.from_numpy(reads.reshape(-1)).cuda()
     off = torch.arange(0, (n + 1) * 150, 150, dtype=torch.int64, device="cuda")
